@@ -1,0 +1,279 @@
+"""Pin the CPU oracle to RainMD's golden vectors and known-answer tests.
+
+Each test restates one of the reference's own checks (test/physics.test.js,
+tools/check-against-openmm.mjs, tools/check-force-gradients.mjs) against the committed
+OpenMM 8.4 Reference dumps, with the reference's bars.
+"""
+import math
+
+import numpy as np
+import pytest
+
+import oracle
+from goldens import system_for
+
+
+def test_erfc_known_values():
+    # physics.test.js:19-35 (SciPy values)
+    cases = [(0.0, 1.0), (0.5, 0.47950012218695348), (1.0, 0.15729920705028516),
+             (2.0, 0.0046777349810472662), (2.628261, 0.00020166438881469927)]
+    for x, expected in cases:
+        assert abs(oracle.erfc(x) - expected) / max(expected, 1e-300) < 1e-13
+    assert abs(oracle.erf(0.5) + oracle.erfc(0.5) - 1) < 1e-15
+    assert abs(oracle.erfc(-1) - (2 - oracle.erfc(1))) < 1e-15
+
+
+def test_alpha_rule():
+    # physics.test.js:37-41
+    assert abs(oracle.alpha_from_tolerance(1.0, 0.0005) - 2.628261) < 1e-6
+    assert abs(oracle.alpha_from_tolerance(0.9, 0.0005) - 2.92029) < 1e-5
+
+
+@pytest.mark.parametrize("order", [4, 5])
+def test_bspline_partition_of_unity(order):
+    # physics.test.js:43-51, generalised to the order the engine runs (4 or 5)
+    for index in range(33):
+        w, d = oracle.bspline(index / 32, order)
+        assert abs(w.sum() - 1) < 1e-14
+        assert abs(d.sum()) < 1e-14
+
+
+def test_nyquist_modulus_patched():
+    # physics.test.js:53-61
+    m = oracle.bspline_moduli(24, 5)
+    assert (m > 1e-6).all()
+    assert abs(m[12] - 0.5 * (m[11] + m[13])) < 1e-9
+
+
+def test_grid_sizes_are_smooth():
+    box = np.diag([2.719, 2.972, 2.540]).reshape(-1)
+    grid = oracle.grid_size_for(box, 2.6282608939112584, 0.0005)
+    for g in grid:
+        r = g
+        for p in (2, 3, 5):
+            while r % p == 0:
+                r //= p
+        assert r == 1
+
+
+def test_counter_noise_moments_and_reproducibility():
+    # physics.test.js:71-86
+    values = np.array([oracle.gaussian_triple(99, atom, 3) for atom in range(4000)]).ravel()
+    assert abs(values.mean()) < 0.05
+    assert abs((values ** 2).mean() - 1) < 0.05
+    assert np.array_equal(oracle.gaussian_triple(99, 7, 3), oracle.gaussian_triple(99, 7, 3))
+
+
+def test_uniform_is_exact_in_f32():
+    # random.js:34-56: the 9-bit shift makes (state>>9)+0.5 exact in f32
+    for a in range(2000):
+        u = oracle.uniform_at(0x1234, a, 5, 1)
+        assert float(np.float32(u)) == u
+        assert 0 < u < 1
+
+
+def test_vacuum_per_term_vs_openmm():
+    # physics.test.js:88-102: LJ 1e-9, Coulomb and total 1e-7
+    s, pos, raw = system_for("ala-vac", constraints="none", rigid_water=False, cutoff=0)
+    e, _ = oracle.Oracle(s).potential(pos, method="NoCutoff")
+
+    def close(ours, theirs, tol):
+        return abs(ours - theirs) / max(abs(theirs), 1) <= tol
+
+    assert close(e["lennardJones"], float(raw["ala-vac-nocutoff:energy.ljOnly"]), 1e-9)
+    assert close(e["coulomb"], float(raw["ala-vac-nocutoff:energy.coulombOnly"]), 1e-7)
+    assert close(e["total"], float(raw["ala-vac-nocutoff:energy.total"]), 1e-7)
+
+
+@pytest.mark.parametrize("dump,constraints", [("ala-wat-pme", "HBonds"), ("ala-wat-pme-free", "none")])
+def test_pme_energy_and_forces_vs_openmm(dump, constraints):
+    # physics.test.js:104-130: total < 1e-7 relative, worst force < 1e-6 of rms
+    s, pos, raw = system_for("ala-wat", constraints=constraints, rigid_water=constraints != "none")
+    o = oracle.Oracle(s)
+    e, f = o.potential(pos, method="PME", alpha=float(raw[f"{dump}:pme.alpha"]),
+                       grid=[24, 24, 24], order=5)
+    ref = float(raw[f"{dump}:energy.total"])
+    assert abs(e["total"] - ref) / abs(ref) < 1e-7
+    F = raw[f"{dump}:forces.total"].reshape(-1)
+    rms = np.sqrt(np.mean(F ** 2))
+    assert np.max(np.abs(f - F)) / rms < 1e-6
+    # per force group (check-against-openmm.mjs)
+    assert abs(e["harmonicBond"] - float(raw[f"{dump}:group.HarmonicBondForce"])) < 1e-8
+    assert abs(e["harmonicAngle"] - float(raw[f"{dump}:group.HarmonicAngleForce"])) < 1e-8
+    assert abs(e["periodicTorsion"] - float(raw[f"{dump}:group.PeriodicTorsionForce"])) < 1e-8
+
+
+def test_sheared_box_vs_openmm():
+    # ala-oct: a truncated octahedron, the only sheared fixture
+    s, pos, raw = system_for("ala-oct")
+    assert max(abs(s["boxVectors"][i]) for i in (3, 6, 7)) > 0.5
+    e, f = oracle.Oracle(s).potential(pos, method="PME", alpha=float(raw["ala-oct-pme:pme.alpha"]),
+                                      grid=[24, 24, 24], order=5)
+    ref = float(raw["ala-oct-pme:energy.total"])
+    # OpenMM is the outlier on direct space for this box: the reference measured its
+    # LJ off by 0.082 kJ/mol and its direct Coulomb by 2.115 kJ/mol, grid-independent,
+    # while an independent sum agrees with the reference's own code to machine
+    # precision (tools/check-against-openmm.mjs:41-50). The oracle reproduces exactly
+    # that documented offset, and nothing more.
+    assert abs((e["total"] - ref) - (-(0.082 + 2.115))) < 0.01
+
+
+def test_restraint_vs_openmm():
+    s, _, raw = system_for("ala-wat")
+    pos = raw["ala-wat-restraint-500:positions"].reshape(-1)
+    atoms = raw["ala-wat-restraint-500:restraint.atoms"]
+    _, ref_pos, _ = system_for("ala-wat")[0], system_for("ala-wat")[1], None
+    reference = system_for("ala-wat")[1].reshape(-1, 3)[atoms].reshape(-1)
+    restraint = {"atoms": atoms, "reference": reference,
+                 "force": float(raw["ala-wat-restraint-500:restraint.force"])}
+    e, _ = oracle.Oracle(s).potential(pos, method="PME", alpha=float(raw["ala-wat-restraint-500:pme.alpha"]),
+                                      grid=[24, 24, 24], order=5, restraint=restraint)
+    assert abs(e["positionRestraint"] - float(raw["ala-wat-restraint-500:group.CustomExternalForce"])) < 1e-6
+    ref = float(raw["ala-wat-restraint-500:energy.total"])
+    assert abs(e["total"] - ref) / abs(ref) < 1e-6
+
+
+def test_dispersion_vs_openmm():
+    # physics.test.js:521-539
+    s, pos, raw = system_for("ala-wat")
+    b = s["boxVectors"]
+    volume = b[0] * b[4] * b[8]
+    o = oracle.Oracle(s)
+    energy = o.dispersion(volume, 1.0)
+    assert abs(energy - -41.537158) / 41.537158 < 1e-6
+    assert abs(o.dispersion(volume * 1.05, 1.0) / energy - 1 / 1.05) < 1e-12
+
+
+@pytest.mark.parametrize("scale", ["0.97", "1.00", "1.02"])
+def test_barostat_forced_scale_vs_openmm(scale):
+    # check-barostat.mjs arms: molecule-centroid scaling plus a box scale
+    s, pos, raw = system_for("ala-wat")
+    o = oracle.Oracle(s)
+    factor = float(scale)
+    scaled = o.scale_molecules(pos, factor)
+    s2 = dict(s)
+    s2["boxVectors"] = s["boxVectors"] * factor
+    o2 = oracle.Oracle(s2)
+    e, _ = o2.potential(scaled, method="PME", alpha=float(raw[f"ala-wat-scale-{scale}:pme.alpha"]),
+                        grid=[24, 24, 24], order=5)
+    b = s2["boxVectors"]
+    total = e["total"] + o2.dispersion(b[0] * b[4] * b[8], 1.0)
+    ref = float(raw[f"ala-wat-scale-{scale}:energy.total"])
+    assert abs(total - ref) / abs(ref) < 1e-7
+
+
+def test_metropolis_weight_entropy_term():
+    # physics.test.js:541-556
+    expand = oracle.metropolis_weight(0, 0.1, 1.01, 0, 2.478, 393)
+    assert expand < 0
+    assert oracle.metropolis_weight(0, 0.1, 1.01, 0, 2.478, 0) == 0
+    assert oracle.metropolis_weight(0, 0.1, 1.01, 100, 2.478, 393) > expand
+
+
+def test_shake_restores_lengths():
+    # physics.test.js:132-158
+    s, pos, _ = system_for("ala-wat")
+    perturbed = pos + np.sin(np.arange(pos.size) * 12.9898) * 0.004
+    out, iterations = oracle.Oracle(s).constrain_positions(perturbed, pos, 1e-8)
+    assert iterations > 0
+    c = s["constraints"]
+    p = out.reshape(-1, 3)
+    lengths = np.linalg.norm(p[c["atomA"]] - p[c["atomB"]], axis=1)
+    assert np.max(np.abs(lengths - c["distance"]) / c["distance"]) < 1e-7
+
+
+def test_force_gradients_central_difference():
+    # tools/check-force-gradients.mjs: bar 1e-5 of rms, on bonded and nonbonded terms
+    s, pos, _ = system_for("ala-wat")
+    o = oracle.Oracle(s)
+    alpha, grid = 2.6282608939112584, [24, 24, 24]
+    _, f = o.potential(pos, method="PME", alpha=alpha, grid=grid, order=5)
+    rms = np.sqrt(np.mean(f ** 2))
+    h = 1e-6
+    rng = np.random.default_rng(3)
+    for index in rng.choice(pos.size, 6, replace=False):
+        plus = pos.copy()
+        plus[index] += h
+        minus = pos.copy()
+        minus[index] -= h
+        ep, _ = o.potential(plus, method="PME", alpha=alpha, grid=grid, order=5)
+        em, _ = o.potential(minus, method="PME", alpha=alpha, grid=grid, order=5)
+        numeric = -(ep["total"] - em["total"]) / (2 * h)
+        assert abs(numeric - f[index]) / rms < 1e-5
+
+
+def exact_ewald(system, positions, alpha, nmax):
+    """physics.test.js:391-519: the textbook k-space sum, sharing no code with PME."""
+    b = np.asarray(system["boxVectors"]).reshape(3, 3)
+    recip = np.linalg.inv(b)
+    volume = abs(b[0, 0] * b[1, 1] * b[2, 2])
+    q = system["topology"]["charges"]
+    p = positions.reshape(-1, 3)
+    r = np.arange(-nmax, nmax + 1)
+    n = np.array(np.meshgrid(r, r, r, indexing="ij")).reshape(3, -1).T
+    n = n[np.any(n != 0, axis=1)]
+    m = n @ recip.T  # row form: m_i = sum_d n_d recip[i][d]
+    m2 = (m ** 2).sum(axis=1)
+    weight = np.exp(-(math.pi ** 2 / alpha ** 2) * m2) / m2
+    keep = weight >= 1e-18
+    m, weight = m[keep], weight[keep]
+    phase = 2 * math.pi * (m @ p.T)
+    re = (np.cos(phase) * q).sum(axis=1)
+    im = (np.sin(phase) * q).sum(axis=1)
+    return (1 / (2 * math.pi * volume)) * 138.935456 * float((weight * (re ** 2 + im ** 2)).sum())
+
+
+@pytest.mark.parametrize("name", ["ala-wat", "ala-oct"])
+def test_pme_vs_exact_lattice_sum(name):
+    # physics.test.js:391-519: 48^3, order 5, bar 1e-5
+    s, pos, _ = system_for(name)
+    o = oracle.Oracle(s)
+    alpha = 2.6282608939112584
+    pme, _ = o.reciprocal(pos, alpha, [48, 48, 48], 5)
+    exact = exact_ewald(s, pos, alpha, 8)
+    assert abs(pme - exact) / abs(exact) < 1e-5
+
+
+def symmetric_exclusions(system):
+    """The both-direction sorted exclusion CSR (cells.js:191-227), for the f32 list."""
+    n = system["topology"]["atomCount"]
+    ex = system["exceptions"]
+    a = np.concatenate([ex["atomA"], ex["atomB"]])
+    b = np.concatenate([ex["atomB"], ex["atomA"]])
+    order = np.lexsort((b, a))
+    start = np.zeros(n + 1, np.int32)
+    np.add.at(start, a + 1, 1)
+    return np.cumsum(start).astype(np.int32), b[order].astype(np.int32)
+
+
+def test_cell_and_neighbour_lists_f32_equal_enumeration():
+    # check-nonbonded.mjs:240-262: the list is the O(N^2) set within rc+skin, no
+    # missing, spurious or duplicated pairs (pairs within 1e-6 of the boundary aside)
+    s, pos, _ = system_for("ala-wat")
+    box = s["boxVectors"]
+    lc = 1.1
+    counts = [max(1, int(abs(box[4 * d]) // lc)) for d in range(3)]
+    P = oracle.pack_params(box, 1.0, lc, 2.6282608939112584)
+    p32 = pos.astype(np.float32)
+    coa, cs, ca = oracle.cell_list_f32(p32, P, counts)
+    assert cs[-1] == s["topology"]["atomCount"]
+    for c in range(len(cs) - 1):
+        assert np.all(np.diff(ca[cs[c]:cs[c + 1]]) > 0)
+    es, ep = symmetric_exclusions(s)
+    nb, nc, req = oracle.neighbour_list_f32(p32, P, counts, cs, ca, es, ep, 800)
+    assert req <= 800
+    n = s["topology"]["atomCount"]
+    p = pos.reshape(-1, 3)
+    excluded = set(zip(s["exceptions"]["atomA"].tolist(), s["exceptions"]["atomB"].tolist()))
+    d = p[:, None, :] - p[None, :, :]
+    L = np.array([box[0], box[4], box[8]])
+    d -= np.floor(d / L + 0.5) * L
+    r2 = (d ** 2).sum(-1)
+    for i in range(0, n, 7):
+        listed = nb[i, :nc[i]]
+        assert len(set(listed.tolist())) == len(listed)
+        expect = {j for j in np.nonzero(r2[i] <= lc * lc)[0].tolist()
+                  if j != i and (min(i, j), max(i, j)) not in excluded}
+        got = set(listed.tolist())
+        boundary = {j for j in expect ^ got if abs(math.sqrt(r2[i, j]) - lc) < 1e-6}
+        assert (expect ^ got) <= boundary
