@@ -1,0 +1,281 @@
+/*
+ * rmd.h — C ABI of the B200 RainMD step engine.
+ *
+ * Every entry point replaces one member of RainMD's `class GpuSimulation`
+ * (webgpu/simulation.js:82-1341); the comment on each names the member and its line.
+ * A Node N-API addon binds these 1:1; Python binds them with ctypes
+ * (rainmd_b200/_lib.py).
+ *
+ * Conventions
+ *   - Units are RainMD's (shared/units.js): nm, ps, kJ/mol, amu, elementary charge, K, bar.
+ *   - Inputs are caller-owned host arrays, copied at the call; outputs are written into
+ *     caller-owned host buffers. No pointer is retained after a call returns.
+ *   - Every call returns an rmd_status (0 = ok). rmd_last_error() gives the message of the
+ *     last failure on that handle; the N-API shim maps codes to RainMD's error classes.
+ *   - A handle holds one or more independent systems advanced together ("batch"); system
+ *     index 0 is the only one for a handle made by rmd_create. Calls on one handle must not
+ *     overlap; different handles are independent.
+ */
+#ifndef RMD_H
+#define RMD_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  RMD_OK = 0,
+  RMD_ERR_INVALID = 1,            /* refused input: RangeError/Error from buildSystem, pmeParameters */
+  RMD_ERR_NEIGHBOUR_OVERFLOW = 2, /* NeighbourOverflowError (webgpu/kernels/neighbours.js:172-183) */
+  RMD_ERR_NON_FINITE = 3,         /* NonFiniteStateError (shared/finite.js:63-95) */
+  RMD_ERR_BUDGET = 4,             /* GpuBudgetError (webgpu/runtime/allocator.js:141-154) */
+  RMD_ERR_STOPPED = 5,            /* SimulationStopped (webgpu/runtime/yield.js:44-50) */
+  RMD_ERR_CUDA = 6,               /* device or driver failure */
+  RMD_ERR_CONSTRAINTS = 7         /* constraint solver hit its iteration cap */
+} rmd_status;
+
+typedef struct rmd_sim rmd_sim;
+
+/* The `system` object of shared/topology/system.js:205-235 (the output of buildSystem),
+ * flattened. Index arrays are 0-based. */
+typedef struct {
+  int32_t atom_count;
+  const double *charges;        /* [N] e */
+  const double *masses;         /* [N] amu; <= 0 marks a massless site */
+  const int32_t *atom_types;    /* [N] */
+  int32_t type_count;
+  const double *lj_a;           /* [T*T] kJ/mol nm^12, A/r^12 - B/r^6 */
+  const double *lj_b;           /* [T*T] kJ/mol nm^6 */
+  const int32_t *exclusion_start;    /* [N+1] AMBER one-sided exclusion CSR (topology.exclusions) */
+  const int32_t *exclusion_partners; /* [exclusion_start[N]] */
+  int32_t bond_count;           /* harmonic (unconstrained) bonds: 1/2 k (r - r0)^2 */
+  const int32_t *bond_atoms;    /* [2*B] */
+  const double *bond_k, *bond_r0;
+  int32_t angle_count;          /* 1/2 k (theta - theta0)^2 */
+  const int32_t *angle_atoms;   /* [3*A] */
+  const double *angle_k, *angle_theta0;
+  int32_t torsion_count;        /* k (1 + cos(n phi - phase)) */
+  const int32_t *torsion_atoms; /* [4*D] */
+  const double *torsion_k, *torsion_periodicity, *torsion_phase;
+  int32_t constraint_count;
+  const int32_t *constraint_atoms; /* [2*C] */
+  const double *constraint_distance;
+  int32_t exception_count;      /* every excluded pair; 1-4 pairs carry scaled parameters */
+  const int32_t *exception_atoms;  /* [2*E] */
+  const double *exception_charge_product, *exception_lj_a, *exception_lj_b;
+  int32_t molecule_count;
+  const int32_t *molecule_of_atom; /* [N] */
+  const double *box_vectors;    /* [9] reduced, row-major (a, b, c); NULL = not periodic */
+  int32_t degrees_of_freedom;
+  double cutoff;                /* nm */
+} rmd_system;
+
+/* Constructor options of GpuSimulation (webgpu/simulation.js:93-188). A field set to its
+ * "derive" value takes the reference's default. rmd_default_options() fills them. */
+typedef struct {
+  double timestep;              /* ps, default 0.002 */
+  double temperature;           /* K, default 298 */
+  double friction;              /* 1/ps, default 1.0 */
+  uint32_t seed;                /* default 0 */
+  double tolerance;             /* constraint tolerance, default 1e-5 (floored as clusters.js:136) */
+  int32_t max_constraint_iterations; /* default 150 */
+  int32_t rebuild_interval;     /* default 20 */
+  int32_t adaptive_rebuild;     /* default 1 */
+  double pressure;              /* bar; <= -1e30 (RMD_NO_PRESSURE) = NVT */
+  int32_t barostat_interval;    /* steps, default 25 */
+  int32_t dispersion_correction;/* default 1 */
+  double restraint_force;       /* kJ/mol/nm^2 in k*d^2, default 0 */
+  int32_t restraint_count;
+  const int32_t *restraint_atoms;      /* [R] */
+  const double *restraint_reference;   /* [3N] positions to restrain towards (only restrained atoms read) */
+  double skin;                  /* nm; <= 0 derives it (cells.js:67 skinFor) */
+  double neighbour_slack;       /* default 2.0 */
+  int32_t max_neighbours;       /* <= 0 derives it */
+  double ewald_tolerance;       /* default 5e-4 */
+  double alpha;                 /* 1/nm; <= 0 derives it */
+  int32_t grid[3];              /* <= 0 derives it */
+  /* B200 engine options (no counterpart in the reference) */
+  int32_t pme_order;            /* B-spline order, 4 or 5; default 5 (the reference's PME_ORDER) */
+  int32_t water_solver;         /* 0 = SHAKE/RATTLE per cluster (reference); 1 = SETTLE for rigid 3-site water */
+  int32_t learned_barostat;     /* 0 = exact Metropolis test; 1 = two-stage delayed acceptance with the MLP */
+} rmd_options;
+
+#define RMD_NO_PRESSURE (-1.0e300)
+
+/* energy() — webgpu/simulation.js:1073-1230 */
+typedef struct {
+  int64_t step;
+  double time;                  /* ps */
+  double bonded, harmonic_bond, harmonic_angle, periodic_torsion;
+  double lennard_jones, dispersion;
+  double coulomb_direct, coulomb_reciprocal, coulomb_self, coulomb;
+  double position_restraint;
+  int32_t restrained_atoms;
+  double potential, kinetic, total;
+  double temperature, kinetic_for_temperature;
+  int32_t kinetic_sampled_before_closing_kick; /* kineticSampledAt */
+  double volume;
+  double box_vectors[9];
+} rmd_energy_report;
+
+/* attemptVolumeChange() — webgpu/simulation.js:995-1070 */
+typedef struct {
+  int32_t attempted;            /* 0: no barostat on this handle (the reference returns null) */
+  int32_t accepted;
+  int32_t refused;              /* cutoff would not fit the proposed box */
+  int32_t screened;             /* learned barostat: rejected at stage 1 without an exact evaluation */
+  double weight, delta_volume, length_scale;
+  double old_potential, new_potential;
+  double volume, volume_scale, acceptance_rate;
+} rmd_volume_move;
+
+/* minimise() — webgpu/simulation.js:880-979 */
+typedef struct {
+  int32_t iterations, rejected, stalled, converged;
+  double potential, max_force, max_step;
+} rmd_minimise_result;
+
+/* diagnostics() — webgpu/simulation.js:1264-1334 */
+typedef struct {
+  int32_t max_shake_iterations;
+  int32_t shake_hit_iteration_cap, rattle_hit_iteration_cap;
+  double worst_stalled_residual;
+  int32_t neighbour_required, neighbour_capacity, worst_neighbour_required, neighbour_growths;
+  double skin, worst_displacement, worst_skin_ratio;
+  int32_t skin_violations;
+  int64_t steps_with_stale_list;
+  int32_t rebuild_interval, requested_rebuild_interval, rebuild_shrinks, rebuild_growths;
+  double worst_skin_usage;
+  int32_t adaptive_rebuild;
+  double volume;
+  int32_t barostat_attempts, barostat_accepted, barostat_refused, barostat_screened,
+      barostat_exact_evaluations;
+  double volume_scale;
+  double constraint_tolerance, requested_tolerance, tolerance_floor;
+  int32_t cell_counts[3];
+  int32_t pme_grid[3];
+  double pme_alpha;
+  int32_t pme_order;
+  int32_t cluster_count, settle_count;
+  int64_t device_bytes;
+} rmd_diagnostics_report;
+
+/* Fills `options` with the reference's defaults. */
+void rmd_default_options(rmd_options *options);
+
+/* new GpuSimulation(device, system, options) — simulation.js:83-190 */
+rmd_status rmd_create(const rmd_system *system, const rmd_options *options, rmd_sim **out);
+
+/* A batch of independent systems of uneven size advanced together: every kernel launch
+ * covers all of them, and a block of steps is one CUDA graph. No reference counterpart
+ * (the reference runs one GpuSimulation per system); every other call takes a
+ * `system_index` into it through the *_at variants below. */
+rmd_status rmd_create_batch(int32_t count, const rmd_system *systems, const rmd_options *options,
+                            rmd_sim **out);
+int32_t rmd_system_count(const rmd_sim *sim);
+
+/* setState(positions, velocities, {step, suppliedNoise}) — simulation.js:357-369.
+ * velocities may be NULL (zero). Applies to system 0. */
+rmd_status rmd_set_state(rmd_sim *sim, const double *positions, const double *velocities,
+                         int64_t step, int32_t supplied_noise);
+rmd_status rmd_set_state_at(rmd_sim *sim, int32_t system_index, const double *positions,
+                            const double *velocities, int64_t step, int32_t supplied_noise);
+
+/* setNoise(noise) — simulation.js:371; f32 [3N] standard normals for the thermostat. */
+rmd_status rmd_set_noise(rmd_sim *sim, const float *noise);
+rmd_status rmd_set_noise_at(rmd_sim *sim, int32_t system_index, const float *noise);
+
+/* initialise() — simulation.js:412-443: one force evaluation with a fresh neighbour list,
+ * growing the list capacity if the measured requirement exceeds it. All systems. */
+rmd_status rmd_initialise(rmd_sim *sim);
+
+/* run(count, {blockSize, stopSignal}) — simulation.js:456-527. All systems advance
+ * `count` steps in blocks of `block_size` (<= 0: the rebuild interval). `stop_flag`, if
+ * not NULL, is polled between blocks (a nonzero value stops with RMD_ERR_STOPPED).
+ * `step_out` (may be NULL) receives system 0's step afterwards. */
+rmd_status rmd_run(rmd_sim *sim, int64_t count, int32_t block_size, const volatile int32_t *stop_flag,
+                   int64_t *step_out);
+
+/* minimise({maxIterations, forceTolerance, maxStep, maxDisplacement}) — simulation.js:880-979 */
+rmd_status rmd_minimise(rmd_sim *sim, int32_t max_iterations, double force_tolerance,
+                        double max_step, double max_displacement, rmd_minimise_result *out);
+
+/* attemptVolumeChange() — simulation.js:995-1070. One Monte Carlo volume move on every
+ * system of the handle; `out` describes system 0. */
+rmd_status rmd_attempt_volume_change(rmd_sim *sim, rmd_volume_move *out);
+rmd_status rmd_last_volume_move_at(rmd_sim *sim, int32_t system_index, rmd_volume_move *out);
+
+/* scaleVolume(s) — simulation.js:801-811: scale molecular centroids and the box of
+ * system 0 by a length factor and return the potential energy there. */
+rmd_status rmd_scale_volume(rmd_sim *sim, double length_scale, double *potential_out);
+
+/* energy() — simulation.js:1073-1230 */
+rmd_status rmd_energy(rmd_sim *sim, rmd_energy_report *out);
+rmd_status rmd_energy_at(rmd_sim *sim, int32_t system_index, rmd_energy_report *out);
+
+/* readPositions() — simulation.js:1239 (f32 [3N]) */
+rmd_status rmd_read_positions(rmd_sim *sim, float *positions);
+
+/* readState() — simulation.js:1244-1261. Any output pointer may be NULL. */
+rmd_status rmd_read_state(rmd_sim *sim, float *positions, float *velocities, float *forces,
+                          double box_vectors[9], double *volume);
+rmd_status rmd_read_state_at(rmd_sim *sim, int32_t system_index, float *positions,
+                             float *velocities, float *forces, double box_vectors[9],
+                             double *volume);
+
+/* diagnostics() — simulation.js:1264-1334 */
+rmd_status rmd_diagnostics(rmd_sim *sim, rmd_diagnostics_report *out);
+rmd_status rmd_diagnostics_at(rmd_sim *sim, int32_t system_index, rmd_diagnostics_report *out);
+
+/* release() — simulation.js:1336-1340 */
+void rmd_destroy(rmd_sim *sim);
+
+/* The message of the last failed call on `sim` (or of the last failed create when NULL). */
+const char *rmd_last_error(const rmd_sim *sim);
+
+/* --- Inspection entry points used by the parity tests (no reference counterpart; they
+ * expose the device's index structures and the grid so they can be compared with the
+ * reference's own intermediate buffers: cellStart/cellAtoms, neighbours, the spread grid). */
+
+/* The cell list of system `system_index` after the last rebuild: counts[3], cell_start
+ * [cells+1] and cell_atoms [N] (local atom indices). Pass NULL to query sizes only. */
+rmd_status rmd_debug_cells(rmd_sim *sim, int32_t system_index, int32_t counts[3],
+                           int32_t *cell_start, int32_t *cell_atoms);
+/* The neighbour list: capacity, then per-atom count [N] and rows [N*capacity]. */
+rmd_status rmd_debug_neighbours(rmd_sim *sim, int32_t system_index, int32_t *capacity,
+                                int32_t *counts, int32_t *rows, int32_t *required);
+/* Evaluate forces and energies at the current positions, with a fresh list, and return
+ * the per-term breakdown (same fields as rmd_energy) and forces (f64 from fixed point). */
+rmd_status rmd_debug_evaluate(rmd_sim *sim, int32_t system_index, rmd_energy_report *energy,
+                              double *forces);
+/* The real spread charge grid (K^3, z fastest) of the last evaluation. */
+rmd_status rmd_debug_charge_grid(rmd_sim *sim, int32_t system_index, double *grid);
+/* A forward+inverse 3D transform check: runs the engine's R2C/C2R FFT on `data`
+ * (real K^3) and returns the unnormalised round trip and the forward half spectrum
+ * ([Kx*Ky*(Kz/2+1)] complex, interleaved) of system `system_index`'s grid size. */
+rmd_status rmd_debug_fft(rmd_sim *sim, int32_t system_index, const double *data,
+                         double *half_spectrum, double *round_trip);
+
+/* Average device time of one launch of a kernel group on the engine's own stream, by CUDA
+ * events over `reps` back-to-back launches: 0 nonbonded (no energy), 1 the seven PME
+ * kernels, 2 the fused integrator, 3 bonded, 4 the five list-rebuild kernels, 5 nonbonded
+ * with energies. For roofline measurement; no reference counterpart. */
+rmd_status rmd_debug_time_kernel(rmd_sim *sim, int32_t which, int32_t reps, double *ms_per_launch);
+/* run() with every block's CUDA graph bracketed by CUDA events on the engine's stream;
+ * `device_ms` receives the summed device time of the blocks (host bookkeeping between
+ * blocks excluded). With `flush_l2`, a 256 MB buffer is written before each block, outside
+ * the timed interval, so no block starts with the previous one's data in L2. */
+rmd_status rmd_bench_run(rmd_sim *sim, int64_t count, int32_t block_size, int32_t flush_l2,
+                         double *device_ms);
+/* Kernels this handle has launched so far (graph replays included). */
+int64_t rmd_debug_kernel_launches(const rmd_sim *sim);
+/* Lanes per atom of the nonbonded kernel (8, 16 or 32), the autotuner's knob. */
+rmd_status rmd_debug_set_nonbonded_lanes(rmd_sim *sim, int32_t lanes);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RMD_H */

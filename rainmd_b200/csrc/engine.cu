@@ -1,0 +1,1971 @@
+// Host engine and C ABI (include/rmd.h) of the B200 RainMD step engine.
+//
+// Mirrors RainMD's `class GpuSimulation` (webgpu/simulation.js:82-1341): host set-up of the
+// device arrays, step blocks, the adaptive rebuild and skin check, capacity growth, the
+// barostat, energy and state readback. The host-side derivations are restated from the
+// reference's shared/ modules and cited where they appear. The step itself is a CUDA graph
+// per block of steps: one replay launches every kernel of every step of every system.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <numeric>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/rmd.h"
+#include "common.cuh"
+#include "kernels.h"
+
+namespace rmd {
+
+struct Error : std::runtime_error {
+  rmd_status code;
+  Error(rmd_status c, const std::string &m) : std::runtime_error(m), code(c) {}
+};
+
+#define CUDA_OK(expr)                                                                       \
+  do {                                                                                      \
+    cudaError_t e_ = (expr);                                                                \
+    if (e_ != cudaSuccess)                                                                  \
+      throw ::rmd::Error(RMD_ERR_CUDA, std::string(#expr) + ": " + cudaGetErrorString(e_));        \
+  } while (0)
+
+template <class T>
+struct DevArray {
+  T *p = nullptr;
+  size_t n = 0;
+  void alloc(size_t count) {
+    release();
+    n = count;
+    if (count) CUDA_OK(cudaMalloc(&p, sizeof(T) * count));
+  }
+  void upload(const std::vector<T> &v) {
+    alloc(v.size());
+    if (!v.empty()) CUDA_OK(cudaMemcpy(p, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice));
+  }
+  void zero() {
+    if (n) CUDA_OK(cudaMemset(p, 0, sizeof(T) * n));
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  size_t bytes() const { return sizeof(T) * n; }
+};
+
+// -------------------------------------------------------------- host-side derivations
+static double alpha_from_tolerance(double cutoff, double tol) {  // parameters.js:43-49
+  return std::sqrt(-std::log(2.0 * tol)) / cutoff;
+}
+static bool transformable(int v) {  // parameters.js:68-74
+  int r = v;
+  for (int p : {2, 3, 5})
+    while (r % p == 0) r /= p;
+  return r == 1;
+}
+static void bspline_host(double u, int order, double *w) {  // parameters.js:121-149 (weights)
+  std::vector<double> dw(order);
+  for (int k = 0; k < order; ++k) w[k] = 0;
+  w[0] = 1 - u;
+  w[1] = u;
+  for (int k = 3; k < order; ++k) {
+    double div = 1.0 / (k - 1);
+    w[k - 1] = div * u * w[k - 2];
+    for (int j = 1; j < k - 1; ++j) w[k - j - 1] = div * ((u + j) * w[k - j - 2] + (k - j - u) * w[k - j - 1]);
+    w[0] = div * (1 - u) * w[0];
+  }
+  double div = 1.0 / (order - 1);
+  w[order - 1] = div * u * w[order - 2];
+  for (int j = 1; j < order - 1; ++j)
+    w[order - j - 1] = div * ((u + j) * w[order - j - 2] + (order - j - u) * w[order - j - 1]);
+  w[0] = div * (1 - u) * w[0];
+}
+static std::vector<double> bspline_moduli(int K, int order) {  // parameters.js:164-215
+  std::vector<double> w(order), raw(K), out(K);
+  bspline_host(0.0, order, w.data());
+  for (int m = 0; m < K; ++m) {
+    double re = 0, im = 0;
+    for (int k = 0; k < order; ++k) {
+      double a = 2.0 * M_PI * m * k / K;
+      re += w[k] * std::cos(a);
+      im += w[k] * std::sin(a);
+    }
+    raw[m] = re * re + im * im;
+  }
+  for (int m = 0; m < K; ++m) {
+    out[m] = raw[m] < 1e-7 ? 0.5 * (raw[(m - 1 + K) % K] + raw[(m + 1) % K]) : raw[m];
+    if (!(out[m] > 0))
+      throw Error(RMD_ERR_INVALID, "B-spline modulus " + std::to_string(m) + " of " + std::to_string(K) +
+                                       " is still zero after the neighbour substitution: the grid is "
+                                       "too small for this interpolation order");
+  }
+  return out;
+}
+
+struct Cluster {
+  std::vector<int> atoms;             // global, ascending
+  std::vector<std::pair<int, int>> c;  // local index pairs
+  std::vector<float> d;
+};
+
+// Per-system host state.
+struct HostSystem {
+  int n = 0, atom_start = 0;
+  rmd_options opt{};
+  std::vector<double> charges, masses;
+  std::vector<int> types;
+  int type_count = 0;
+  std::vector<double> lj_a, lj_b;
+  std::vector<double> box;  // 9
+  double cutoff = 1.0, skin = 0.1, list_cutoff = 1.1, alpha = 0;
+  int grid[3] = {0, 0, 0}, order = 5;
+  int counts[3] = {1, 1, 1};
+  int capacity = 32;
+  double estimated_neighbours = 0;
+  int dof = 0, n_molecules = 0;
+  double q2 = 0, qsum = 0, disp_a = 0, disp_b = 0;
+  double tolerance = 1e-5, tol_floor = 0, requested_tol = 1e-5;
+  double min_constraint = 0;
+  std::vector<double> restraint_reference;  // 3 per restrained atom
+  std::vector<int> restraint_atoms;
+  int64_t step = 0;
+  // adaptive rebuild (simulation.js:105-118, 544-623)
+  int rebuild_interval = 20, requested_rebuild = 20;
+  bool adaptive = true;
+  int calm_blocks = 0, rebuild_growths = 0, rebuild_shrinks = 0, skin_violations = 0;
+  int64_t steps_with_stale = 0;
+  int64_t steps_since_rebuild = 1LL << 40;
+  double worst_displacement = 0, worst_skin_ratio = 0, worst_skin_usage = 0;
+  int worst_required = 0, neighbour_growths = 0, last_required = 0;
+  bool kinetic_sampled_in_step = false;
+  int64_t kinetic_sampled_at = -1;
+  int n_clusters = 0, n_settle = 0;
+  int barostat_interval = 25;
+  int64_t steps_since_barostat = 0;
+  bool has_pressure = false;
+  rmd_volume_move last_move{};
+};
+
+static const double LIGHT_ANCHOR_SKIN = 0.40;  // cells.js:67-91
+
+struct Engine {
+  std::vector<HostSystem> hs;
+  int S = 0, N = 0;
+  cudaStream_t stream = nullptr;
+  std::string last_error;
+  int nb_lanes = 32;
+  int pme_order = 5;
+  bool pme_on = true;
+
+  // device arrays
+  DevArray<float4> posq, vel, origin, saved_posq;
+  DevArray<int> atom_type, sys_of_atom, sys_atom_start;
+  DevArray<float> masses, noise;
+  DevArray<unsigned long long> force, saved_force;
+  DevArray<double> e_lj, e_coul, ke_post, ke_early, e_term, e_pme;
+  DevArray<float2> lj;
+  DevArray<int> excl_start, excl_partners, exc_start, exc_partner;
+  DevArray<float4> exc_param;
+  DevArray<int> cell_of_atom, cell_count, cell_start, cell_atoms, cell_sys;
+  int n_cells_total = 0;
+  DevArray<int> nbr, nbr_count, required;
+  DevArray<int2> bond_atoms;
+  DevArray<float2> bond_param, angle_param;
+  DevArray<int4> angle_atoms, tor_atoms;
+  DevArray<float4> tor_param, rest_param;
+  DevArray<int> rest_atom;
+  int n_bonds = 0, n_angles = 0, n_tors = 0, n_rest = 0;
+  std::vector<int> term_start;  // per system: bonds, angles, torsions, restraints offsets (4*S+4)
+  DevArray<unsigned long long> fixed_grid;
+  DevArray<float2> half, twiddles;
+  DevArray<float> real_grid, moduli;
+  DevArray<FftPlan> fft_plans;
+  DevArray<FftTask> tasks_z, tasks_y, tasks_x;
+  std::vector<int> task_x_start;  // per system range of x tasks
+  DevArray<DevSys> sys;
+  DevArray<DevSysD> sysd;
+  std::vector<DevSys> h_sys;
+  std::vector<DevSysD> h_sysd;
+  DevArray<DevInteg> integ;
+  DevArray<long long> step_base;
+  DevArray<unsigned> disp;
+  DevArray<int> diag;
+  DevArray<double> energies, saved_energies, baro, seg_out, fixed_scales;
+  DevArray<Segment> segments;
+  int n_segments = 0;
+  DevArray<int> free_atoms, cl_atom_start, cl_atoms, cl_con_start;
+  DevArray<int2> cl_con_pair;
+  DevArray<float> cl_con_dist;
+  DevArray<int3> settle_atoms;
+  DevArray<DevSettle> settle_param;
+  int n_free = 0, n_clusters = 0, n_settle = 0;
+  DevArray<int> mol_start, mol_atoms;
+  int n_molecules_total = 0;
+  bool any_pressure = false;
+  bool supplied_noise_any = false;
+
+  std::map<std::string, cudaGraphExec_t> graphs;
+  std::map<std::string, long long> graph_launches;  // kernels recorded in each graph
+  long long recorded = 0;                            // kernels recorded by record_* calls
+  long long kernel_launches = 0;                     // kernels launched so far (graphs and direct)
+
+  ~Engine() {
+    for (auto &kv : graphs) cudaGraphExecDestroy(kv.second);
+    if (stream) cudaStreamDestroy(stream);
+  }
+
+  // ---------------------------------------------------------------- construction
+  void build(int count, const rmd_system *systems, const rmd_options *options);
+  void plan_system(HostSystem &h, const rmd_system &s);
+  void upload_all(const std::vector<const rmd_system *> &src);
+  void allocate_neighbours();
+  LaunchCtx ctx() const;
+  IntegrateArgs iargs(int step_offset) const;
+  BaroArgs bargs() const;
+
+  // ---------------------------------------------------------------- operations
+  void record_forces(bool rebuild, bool energy);
+  void record_barostat();
+  void evaluate(bool rebuild, bool energy);
+  void set_state(int s, const double *pos, const double *vel, int64_t step, int supplied);
+  void initialise();
+  int check_capacity();  // returns max required; grows if needed
+  void run(int64_t count, int block, const volatile int32_t *stop);
+  void run_block(int n, bool barostat, bool energy_last);
+  // timing hooks for run(): events around each block's graph, optional L2 flush between
+  cudaEvent_t ev_a = nullptr, ev_b = nullptr;
+  bool timing = false, flush = false;
+  double timed_ms = 0.0;
+  DevArray<unsigned char> flush_buffer;
+  void check_block(int steps);
+  void energy(int s, rmd_energy_report *out);
+  void sync() { CUDA_OK(cudaStreamSynchronize(stream)); }
+  void update_box_from_host(int s);
+  void attempt_volume_change();
+  double scale_volume(int s, double ls);
+  std::vector<float> max_forces();
+  void minimise(int max_iterations, double force_tolerance, double max_step, double cap,
+                rmd_minimise_result *out);
+  std::vector<double> read_energies();
+};
+
+// ------------------------------------------------------------------------ set-up
+void Engine::plan_system(HostSystem &h, const rmd_system &s) {
+  const rmd_options &o = h.opt;
+  h.n = s.atom_count;
+  if (h.n <= 0) throw Error(RMD_ERR_INVALID, "atom_count must be positive");
+  if (s.box_vectors == nullptr)
+    throw Error(RMD_ERR_INVALID,
+                "the device path needs a periodic box: a cell list cannot be built without one "
+                "(cells.js:109-115); a non-periodic system uses the all-pairs host path");
+  h.box.assign(s.box_vectors, s.box_vectors + 9);
+  for (int k : {1, 2, 5})
+    if (h.box[k] != 0.0) throw Error(RMD_ERR_INVALID, "box vectors must be reduced upper-triangular (a along x, b in xy)");
+  h.cutoff = s.cutoff;
+  const double widths[3] = {std::fabs(h.box[0]), std::fabs(h.box[4]), std::fabs(h.box[8])};
+  const double smallest = std::min(widths[0], std::min(widths[1], widths[2]));
+  if (!(h.cutoff > 0) || h.cutoff > 0.5 * smallest) {  // system.js:70-89
+    char msg[256];
+    snprintf(msg, sizeof msg, "a %g nm cutoff does not fit in a box whose smallest width is %.4f nm: "
+             "the cutoff must be at most half of it", h.cutoff, smallest);
+    throw Error(RMD_ERR_INVALID, msg);
+  }
+  h.charges.assign(s.charges, s.charges + h.n);
+  h.masses.assign(s.masses, s.masses + h.n);
+  h.types.assign(s.atom_types, s.atom_types + h.n);
+  h.type_count = s.type_count;
+  h.lj_a.assign(s.lj_a, s.lj_a + (size_t)h.type_count * h.type_count);
+  h.lj_b.assign(s.lj_b, s.lj_b + (size_t)h.type_count * h.type_count);
+  h.dof = s.degrees_of_freedom;
+  h.n_molecules = s.molecule_count;
+
+  // skinFor (cells.js:67-91), unless given.
+  if (o.skin > 0) {
+    h.skin = o.skin;
+  } else {
+    double lightest = INFINITY;
+    for (double m : h.masses)
+      if (m > 0 && m < lightest) lightest = m;
+    if (!std::isfinite(lightest)) lightest = 1.008;
+    const double speed = std::sqrt((o.temperature / 298.0) * (1.008 / lightest));
+    const double scaled = LIGHT_ANCHOR_SKIN * (o.timestep / 0.002) * speed;
+    const double room = 0.5 * smallest - h.cutoff;
+    h.skin = std::max(0.1, std::min(scaled, room > 0 ? room * 0.9 : 0.1));
+  }
+  h.list_cutoff = h.cutoff + h.skin;
+  // planCellList (cells.js:101-171)
+  for (int d = 0; d < 3; ++d) h.counts[d] = std::max(1, (int)std::floor(widths[d] / h.list_cutoff));
+  const double volume = widths[0] * widths[1] * widths[2];
+  const double density = h.n / volume;
+  h.estimated_neighbours = density * (4.0 / 3.0) * M_PI * std::pow(h.list_cutoff, 3);
+  const double slack = o.neighbour_slack > 0 ? o.neighbour_slack : 2.0;
+  h.capacity = o.max_neighbours > 0 ? o.max_neighbours
+                                    : std::max(32, (int)std::ceil(h.estimated_neighbours * slack));
+  // pmeParameters (parameters.js:227-252)
+  const double tol = o.ewald_tolerance > 0 ? o.ewald_tolerance : 5e-4;
+  h.alpha = o.alpha > 0 ? o.alpha : alpha_from_tolerance(h.cutoff, tol);
+  h.order = o.pme_order == 4 ? 4 : 5;
+  for (int d = 0; d < 3; ++d) {
+    if (o.grid[d] > 0) {
+      h.grid[d] = o.grid[d];
+    } else {
+      const double len = std::sqrt(h.box[3 * d] * h.box[3 * d] + h.box[3 * d + 1] * h.box[3 * d + 1] +
+                                   h.box[3 * d + 2] * h.box[3 * d + 2]);
+      int c = std::max(2, (int)std::ceil(2.0 * h.alpha * len / (3.0 * std::pow(tol, 0.2))));
+      while (!transformable(c)) ++c;
+      h.grid[d] = c;
+    }
+    if (!transformable(h.grid[d]))
+      throw Error(RMD_ERR_INVALID, "PME grid size " + std::to_string(h.grid[d]) +
+                                       " is not a product of 2, 3 and 5, which is what the FFT can transform");
+    if (h.grid[d] < h.order)
+      throw Error(RMD_ERR_INVALID, "PME grid size smaller than the interpolation order; the box is too "
+                                   "small for this cutoff");
+    if (h.grid[d] > 2048) throw Error(RMD_ERR_INVALID, "PME grid sizes above 2048 are not supported");
+  }
+  h.q2 = 0;
+  h.qsum = 0;
+  for (double q : h.charges) {
+    h.q2 += q * q;
+    h.qsum += q;
+  }
+  // dispersionCoefficients (dispersion.js:37-64)
+  {
+    const int T = h.type_count;
+    std::vector<double> cnt(T, 0.0);
+    for (int t : h.types) cnt[t] += 1.0;
+    double oa = 0, ob = 0, da = 0, db = 0;
+    for (int i = 0; i < T; ++i) {
+      for (int j = 0; j < T; ++j) {
+        oa += cnt[i] * cnt[j] * h.lj_a[T * i + j];
+        ob += cnt[i] * cnt[j] * h.lj_b[T * i + j];
+      }
+      da += cnt[i] * h.lj_a[T * i + i];
+      db += cnt[i] * h.lj_b[T * i + i];
+    }
+    const double sc = (double)h.n / (h.n + 1);
+    h.disp_a = (oa + da) * sc;
+    h.disp_b = (ob + db) * sc;
+  }
+  h.requested_rebuild = o.rebuild_interval > 0 ? o.rebuild_interval : 20;
+  h.adaptive = o.adaptive_rebuild != 0;
+  h.rebuild_interval = h.adaptive ? std::min(h.requested_rebuild, 4) : h.requested_rebuild;
+  h.has_pressure = o.pressure > -1e299;
+  h.barostat_interval = o.barostat_interval > 0 ? o.barostat_interval : 25;
+  h.requested_tol = o.tolerance > 0 ? o.tolerance : 1e-5;
+  h.tolerance = h.requested_tol;
+  h.min_constraint = INFINITY;
+  for (int k = 0; k < s.constraint_count; ++k) h.min_constraint = std::min(h.min_constraint, s.constraint_distance[k]);
+  if (o.restraint_force > 0 && o.restraint_count > 0) {
+    h.restraint_atoms.assign(o.restraint_atoms, o.restraint_atoms + o.restraint_count);
+    for (int a : h.restraint_atoms) {
+      if (a < 0 || a >= h.n) throw Error(RMD_ERR_INVALID, "restraint atom out of range");
+      for (int c = 0; c < 3; ++c) h.restraint_reference.push_back(o.restraint_reference[3 * a + c]);
+    }
+  }
+}
+
+static void fft_axis_plan(int n, FftAxis &ax, int tw_base) {
+  ax.n = n;
+  ax.nstages = 0;
+  ax.tw_base = tw_base;
+  int r = n;
+  while (r % 4 == 0) { ax.radix[ax.nstages++] = 4; r /= 4; }
+  while (r % 2 == 0) { ax.radix[ax.nstages++] = 2; r /= 2; }
+  while (r % 3 == 0) { ax.radix[ax.nstages++] = 3; r /= 3; }
+  while (r % 5 == 0) { ax.radix[ax.nstages++] = 5; r /= 5; }
+}
+
+constexpr int FFT_SMEM_HOST = 2048;
+
+void Engine::build(int count, const rmd_system *systems, const rmd_options *options) {
+  S = count;
+  hs.resize(S);
+  std::vector<const rmd_system *> src(S);
+  N = 0;
+  for (int s = 0; s < S; ++s) {
+    hs[s].opt = options[s];
+    src[s] = &systems[s];
+    plan_system(hs[s], systems[s]);
+    hs[s].atom_start = N;
+    N += hs[s].n;
+  }
+  pme_order = hs[0].order;
+  for (auto &h : hs)
+    if (h.order != pme_order) throw Error(RMD_ERR_INVALID, "every system of a batch must use the same PME order");
+  CUDA_OK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+  upload_all(src);
+}
+
+void Engine::upload_all(const std::vector<const rmd_system *> &src) {
+  // ---- atoms
+  std::vector<float4> h_posq(N), h_vel(N);
+  std::vector<int> h_type(N), h_sys_of(N), h_sys_start(S);
+  std::vector<float> h_mass(N);
+  std::vector<float2> h_lj;
+  std::vector<int> lj_base(S);
+  for (int s = 0; s < S; ++s) {
+    const HostSystem &h = hs[s];
+    h_sys_start[s] = h.atom_start;
+    lj_base[s] = (int)h_lj.size();
+    for (int k = 0; k < h.type_count * h.type_count; ++k) h_lj.push_back(make_float2((float)h.lj_a[k], (float)h.lj_b[k]));
+    for (int i = 0; i < h.n; ++i) {
+      const int g = h.atom_start + i;
+      h_posq[g] = make_float4(0, 0, 0, (float)h.charges[i]);
+      h_vel[g] = make_float4(0, 0, 0, h.masses[i] > 0 ? (float)(1.0 / h.masses[i]) : 0.f);
+      h_type[g] = h.types[i];
+      h_sys_of[g] = s;
+      h_mass[g] = (float)h.masses[i];
+    }
+  }
+  posq.upload(h_posq);
+  vel.upload(h_vel);
+  origin.upload(h_posq);
+  saved_posq.upload(h_posq);
+  atom_type.upload(h_type);
+  sys_of_atom.upload(h_sys_of);
+  sys_atom_start.upload(h_sys_start);
+  masses.upload(h_mass);
+  lj.upload(h_lj);
+  noise.alloc(3 * (size_t)N);
+  noise.zero();
+  force.alloc(3 * (size_t)N);
+  force.zero();
+  saved_force.alloc(3 * (size_t)N);
+  saved_force.zero();
+  for (auto *a : {&e_lj, &e_coul, &ke_post, &ke_early}) {
+    a->alloc(N);
+    a->zero();
+  }
+
+  // ---- exclusions (buildExclusionGather, cells.js:191-227) and exceptions
+  //      (buildExceptionGather, cells.js:237-271), global atom indices
+  std::vector<int> ex_start(N + 1, 0), ex_part, xs(N + 1, 0), xp;
+  std::vector<float4> xparam;
+  {
+    std::vector<std::vector<int>> ex(N);
+    std::vector<std::vector<std::pair<int, float4>>> xc(N);
+    for (int s = 0; s < S; ++s) {
+      const rmd_system &r = *src[s];
+      const int base = hs[s].atom_start;
+      for (int a = 0; a < r.atom_count; ++a)
+        for (int c = r.exclusion_start[a]; c < r.exclusion_start[a + 1]; ++c) {
+          const int b = r.exclusion_partners[c];
+          if (b < 0 || b >= r.atom_count) throw Error(RMD_ERR_INVALID, "exclusion partner out of range");
+          ex[base + a].push_back(base + b);
+          ex[base + b].push_back(base + a);
+        }
+      for (int k = 0; k < r.exception_count; ++k) {
+        const int a = r.exception_atoms[2 * k], b = r.exception_atoms[2 * k + 1];
+        if (a < 0 || b < 0 || a >= r.atom_count || b >= r.atom_count)
+          throw Error(RMD_ERR_INVALID, "exception atom out of range");
+        const float qa = (float)r.charges[a], qb = (float)r.charges[b];
+        (void)qa; (void)qb;
+        const float full_ab = (float)(r.charges[a] * r.charges[b]);
+        float4 p = make_float4((float)r.exception_charge_product[k], (float)r.exception_lj_a[k],
+                               (float)r.exception_lj_b[k], full_ab);
+        xc[base + a].push_back({base + b, p});
+        xc[base + b].push_back({base + a, p});
+      }
+    }
+    for (int i = 0; i < N; ++i) {
+      std::sort(ex[i].begin(), ex[i].end());
+      ex_start[i + 1] = ex_start[i] + (int)ex[i].size();
+      ex_part.insert(ex_part.end(), ex[i].begin(), ex[i].end());
+      xs[i + 1] = xs[i] + (int)xc[i].size();
+      for (auto &pr : xc[i]) {
+        xp.push_back(pr.first);
+        xparam.push_back(pr.second);
+      }
+    }
+  }
+  if (ex_part.empty()) ex_part.push_back(0);
+  if (xp.empty()) {
+    xp.push_back(0);
+    xparam.push_back(make_float4(0, 0, 0, 0));
+  }
+  excl_start.upload(ex_start);
+  excl_partners.upload(ex_part);
+  exc_start.upload(xs);
+  exc_partner.upload(xp);
+  exc_param.upload(xparam);
+
+  // ---- bonded terms and restraints, per system in order
+  std::vector<int2> hb;
+  std::vector<float2> hbp, hap;
+  std::vector<int4> ha, ht;
+  std::vector<float4> htp, hrp;
+  std::vector<int> hra;
+  std::vector<int> bstart(S + 1), astart(S + 1), tstart(S + 1), rstart(S + 1);
+  for (int s = 0; s < S; ++s) {
+    const rmd_system &r = *src[s];
+    const int base = hs[s].atom_start;
+    bstart[s] = (int)hb.size();
+    for (int k = 0; k < r.bond_count; ++k) {
+      hb.push_back(make_int2(base + r.bond_atoms[2 * k], base + r.bond_atoms[2 * k + 1]));
+      hbp.push_back(make_float2((float)r.bond_k[k], (float)r.bond_r0[k]));
+    }
+    astart[s] = (int)ha.size();
+    for (int k = 0; k < r.angle_count; ++k) {
+      ha.push_back(make_int4(base + r.angle_atoms[3 * k], base + r.angle_atoms[3 * k + 1],
+                             base + r.angle_atoms[3 * k + 2], 0));
+      hap.push_back(make_float2((float)r.angle_k[k], (float)r.angle_theta0[k]));
+    }
+    tstart[s] = (int)ht.size();
+    for (int k = 0; k < r.torsion_count; ++k) {
+      ht.push_back(make_int4(base + r.torsion_atoms[4 * k], base + r.torsion_atoms[4 * k + 1],
+                             base + r.torsion_atoms[4 * k + 2], base + r.torsion_atoms[4 * k + 3]));
+      htp.push_back(make_float4((float)r.torsion_k[k], (float)r.torsion_periodicity[k],
+                                (float)r.torsion_phase[k], 0.f));
+    }
+    rstart[s] = (int)hra.size();
+    const HostSystem &h = hs[s];
+    for (size_t k = 0; k < h.restraint_atoms.size(); ++k) {
+      hra.push_back(base + h.restraint_atoms[k]);
+      hrp.push_back(make_float4((float)h.restraint_reference[3 * k], (float)h.restraint_reference[3 * k + 1],
+                                (float)h.restraint_reference[3 * k + 2], (float)h.opt.restraint_force));
+    }
+  }
+  bstart[S] = (int)hb.size();
+  astart[S] = (int)ha.size();
+  tstart[S] = (int)ht.size();
+  rstart[S] = (int)hra.size();
+  n_bonds = (int)hb.size();
+  n_angles = (int)ha.size();
+  n_tors = (int)ht.size();
+  n_rest = (int)hra.size();
+  bond_atoms.upload(hb);
+  bond_param.upload(hbp);
+  angle_atoms.upload(ha);
+  angle_param.upload(hap);
+  tor_atoms.upload(ht);
+  tor_param.upload(htp);
+  rest_atom.upload(hra);
+  rest_param.upload(hrp);
+  e_term.alloc(std::max(1, n_bonds + n_angles + n_tors + n_rest));
+  e_term.zero();
+
+  // ---- constraint clusters (buildConstraintClusters, clusters.js:20-57) and SETTLE waters
+  std::vector<int> h_free, h_cl_as, h_cl_atoms, h_cl_cs;
+  std::vector<int2> h_pairs;
+  std::vector<float> h_dist;
+  std::vector<int3> h_settle;
+  std::vector<DevSettle> h_settle_p;
+  h_cl_as.push_back(0);
+  h_cl_cs.push_back(0);
+  for (int s = 0; s < S; ++s) {
+    const rmd_system &r = *src[s];
+    HostSystem &h = hs[s];
+    const int base = h.atom_start;
+    std::vector<int> parent(h.n);
+    std::iota(parent.begin(), parent.end(), 0);
+    auto find = [&](int x) {
+      int root = x;
+      while (parent[root] != root) root = parent[root];
+      while (parent[x] != root) {
+        int nx = parent[x];
+        parent[x] = root;
+        x = nx;
+      }
+      return root;
+    };
+    for (int k = 0; k < r.constraint_count; ++k) {
+      const int a = r.constraint_atoms[2 * k], b = r.constraint_atoms[2 * k + 1];
+      if (a < 0 || b < 0 || a >= h.n || b >= h.n) throw Error(RMD_ERR_INVALID, "constraint atom out of range");
+      const int ra = find(a), rb = find(b);
+      if (ra != rb) parent[rb] = ra;
+    }
+    std::map<int, std::vector<int>> by_root;  // root -> constraint indices, in order
+    std::vector<int> root_order;
+    for (int k = 0; k < r.constraint_count; ++k) {
+      const int root = find(r.constraint_atoms[2 * k]);
+      if (!by_root.count(root)) root_order.push_back(root);
+      by_root[root].push_back(k);
+    }
+    std::vector<char> in_cluster(h.n, 0);
+    h.n_clusters = 0;
+    h.n_settle = 0;
+    for (int root : root_order) {
+      const auto &members = by_root[root];
+      std::vector<int> atoms;
+      for (int k : members) {
+        atoms.push_back(r.constraint_atoms[2 * k]);
+        atoms.push_back(r.constraint_atoms[2 * k + 1]);
+      }
+      std::sort(atoms.begin(), atoms.end());
+      atoms.erase(std::unique(atoms.begin(), atoms.end()), atoms.end());
+      for (int a : atoms) in_cluster[a] = 1;
+      // SETTLE candidate: a 3-atom triangle, apex the heaviest, equal light masses and
+      // equal apex distances (findWaterClusters, constraints.js:36-85).
+      if (h.opt.water_solver == 1 && members.size() == 3 && atoms.size() == 3) {
+        int apex = atoms[0];
+        for (int a : atoms)
+          if (h.masses[a] > h.masses[apex]) apex = a;
+        std::vector<int> light;
+        for (int a : atoms)
+          if (a != apex) light.push_back(a);
+        auto length = [&](int p, int q) {
+          for (int k : members) {
+            const int a = r.constraint_atoms[2 * k], b = r.constraint_atoms[2 * k + 1];
+            if ((a == p && b == q) || (a == q && b == p)) return r.constraint_distance[k];
+          }
+          return -1.0;
+        };
+        const double d1 = length(apex, light[0]), d2 = length(apex, light[1]), d3 = length(light[0], light[1]);
+        const double mo = h.masses[apex], mh = h.masses[light[0]];
+        if (d1 > 0 && d2 > 0 && d3 > 0 && std::fabs(d1 - d2) < 1e-9 * d1 &&
+            std::fabs(h.masses[light[1]] - mh) < 1e-9 * mh && mo > 0 && mh > 0) {
+          DevSettle w;
+          w.m_o = (float)mo;
+          w.m_h = (float)mh;
+          const double rc = 0.5 * d3, height = std::sqrt(d1 * d1 - rc * rc);
+          const double wt = mo + 2 * mh;
+          w.ra = (float)(2.0 * mh * height / wt);
+          w.rb = (float)(height - 2.0 * mh * height / wt);
+          w.rc = (float)rc;
+          w.d_oh = (float)d1;
+          w.d_hh = (float)d3;
+          w.pad = 0.f;
+          h_settle.push_back(make_int3(base + apex, base + light[0], base + light[1]));
+          h_settle_p.push_back(w);
+          h.n_settle++;
+          continue;
+        }
+      }
+      if ((int)atoms.size() > MAX_CLUSTER_ATOMS || (int)members.size() > MAX_CLUSTER_CONSTRAINTS)
+        throw Error(RMD_ERR_INVALID, "a constraint cluster of " + std::to_string(atoms.size()) + " atoms and " +
+                                         std::to_string(members.size()) +
+                                         " constraints exceeds the per-thread solver limit (8 atoms, 12 "
+                                         "constraints); use HBonds constraints");
+      for (int a : atoms) h_cl_atoms.push_back(base + a);
+      h_cl_as.push_back((int)h_cl_atoms.size());
+      for (int k : members) {
+        const int a = r.constraint_atoms[2 * k], b = r.constraint_atoms[2 * k + 1];
+        const int la = (int)(std::lower_bound(atoms.begin(), atoms.end(), a) - atoms.begin());
+        const int lb = (int)(std::lower_bound(atoms.begin(), atoms.end(), b) - atoms.begin());
+        h_pairs.push_back(make_int2(la, lb));
+        h_dist.push_back((float)r.constraint_distance[k]);
+      }
+      h_cl_cs.push_back((int)h_pairs.size());
+      h.n_clusters++;
+    }
+    for (int a = 0; a < h.n; ++a)
+      if (!in_cluster[a]) h_free.push_back(base + a);
+  }
+  // units in order: free atoms, SHAKE clusters, SETTLE waters
+  n_free = (int)h_free.size();
+  n_clusters = (int)h_cl_as.size() - 1;
+  n_settle = (int)h_settle.size();
+  if (h_free.empty()) h_free.push_back(0);
+  if (h_cl_atoms.empty()) h_cl_atoms.push_back(0);
+  if (h_pairs.empty()) {
+    h_pairs.push_back(make_int2(0, 0));
+    h_dist.push_back(0.f);
+  }
+  if (h_settle.empty()) {
+    h_settle.push_back(make_int3(0, 0, 0));
+    h_settle_p.push_back(DevSettle{});
+  }
+  free_atoms.upload(h_free);
+  cl_atom_start.upload(h_cl_as);
+  cl_atoms.upload(h_cl_atoms);
+  cl_con_start.upload(h_cl_cs);
+  cl_con_pair.upload(h_pairs);
+  cl_con_dist.upload(h_dist);
+  settle_atoms.upload(h_settle);
+  settle_param.upload(h_settle_p);
+
+  // ---- molecules (global CSR over all systems)
+  {
+    std::vector<int> ms(1, 0), ma;
+    for (int s = 0; s < S; ++s) {
+      const rmd_system &r = *src[s];
+      const int base = hs[s].atom_start;
+      std::vector<std::vector<int>> mol(r.molecule_count);
+      for (int a = 0; a < r.atom_count; ++a) {
+        const int m = r.molecule_of_atom[a];
+        if (m < 0 || m >= r.molecule_count) throw Error(RMD_ERR_INVALID, "molecule index out of range");
+        mol[m].push_back(base + a);
+      }
+      for (auto &m : mol) {
+        ma.insert(ma.end(), m.begin(), m.end());
+        ms.push_back((int)ma.size());
+      }
+    }
+    n_molecules_total = (int)ms.size() - 1;
+    if (ma.empty()) ma.push_back(0);
+    mol_start.upload(ms);
+    mol_atoms.upload(ma);
+  }
+
+  // ---- cells
+  std::vector<int> h_cell_sys;
+  h_sys.resize(S);
+  h_sysd.resize(S);
+  int cell_base = 0, cell_start_base = 0;
+  for (int s = 0; s < S; ++s) {
+    HostSystem &h = hs[s];
+    DevSys &d = h_sys[s];
+    DevSysD &dd = h_sysd[s];
+    memset(&d, 0, sizeof d);
+    memset(&dd, 0, sizeof dd);
+    d.cutoff = (float)h.cutoff;
+    d.cutoff2 = d.cutoff * d.cutoff;
+    d.list_cutoff = (float)h.list_cutoff;
+    d.list_cutoff2 = d.list_cutoff * d.list_cutoff;
+    d.alpha = (float)h.alpha;
+    d.atom_start = h.atom_start;
+    d.atom_count = h.n;
+    d.type_count = h.type_count;
+    d.lj_base = lj_base[s];
+    const int cells = h.counts[0] * h.counts[1] * h.counts[2];
+    for (int k = 0; k < 3; ++k) {
+      d.cell_counts[k] = h.counts[k];
+      dd.max_counts[k] = h.counts[k];
+    }
+    d.cell_base = cell_base;
+    d.cell_start_base = cell_start_base;
+    d.cell_capacity = cells;
+    for (int c = 0; c < cells; ++c) h_cell_sys.push_back(s);
+    cell_base += cells;
+    cell_start_base += cells + 1;
+    d.order = h.order;
+    d.molecule_count = h.n_molecules;
+    dd.q2_sum = h.q2;
+    dd.q_sum = h.qsum;
+    dd.disp_a = h.disp_a;
+    dd.disp_b = h.disp_b;
+    dd.cutoff = h.cutoff;
+    dd.alpha = h.alpha;
+    dd.list_cutoff = h.list_cutoff;
+    dd.dispersion_on = h.opt.dispersion_correction != 0;
+    for (int k = 0; k < 9; ++k) dd.box[k] = h.box[k];
+  }
+  n_cells_total = cell_base;
+  cell_sys.upload(h_cell_sys);
+  cell_count.alloc(n_cells_total);
+  cell_count.zero();
+  cell_start.alloc(cell_start_base);
+  cell_start.zero();
+  cell_atoms.alloc(N);
+  cell_of_atom.alloc(N);
+  required.alloc(S);
+  required.zero();
+
+  // ---- PME grids, moduli, twiddles, FFT plans and task tables
+  {
+    long long gbase = 0, hbase = 0;
+    std::vector<float> h_mod;
+    std::vector<float2> h_tw;
+    std::vector<FftPlan> h_plans(S);
+    std::vector<FftTask> tz, ty, tx;
+    task_x_start.assign(S + 1, 0);
+    for (int s = 0; s < S; ++s) {
+      HostSystem &h = hs[s];
+      DevSys &d = h_sys[s];
+      const int nx = h.grid[0], ny = h.grid[1], nz = h.grid[2], nzh = nz / 2 + 1;
+      for (int k = 0; k < 3; ++k) d.grid[k] = h.grid[k];
+      d.grid_base = gbase;
+      d.half_base = hbase;
+      d.moduli_base = (int)h_mod.size();
+      gbase += (long long)nx * ny * nz;
+      hbase += (long long)nx * ny * nzh;
+      for (int ax = 0; ax < 3; ++ax) {
+        for (double m : bspline_moduli(h.grid[ax], h.order)) h_mod.push_back((float)m);
+        fft_axis_plan(h.grid[ax], h_plans[s].axis[ax], (int)h_tw.size());
+        for (int k = 0; k < h.grid[ax]; ++k) {
+          const double a = -2.0 * M_PI * k / h.grid[ax];
+          h_tw.push_back(make_float2((float)std::cos(a), (float)std::sin(a)));
+        }
+      }
+      // z pass: pairs of real lines
+      const int lines = nx * ny, pairs = (lines + 1) / 2;
+      const int mz = std::max(1, std::min(64, FFT_SMEM_HOST / nz));
+      for (int p = 0; p < pairs; p += mz) tz.push_back(FftTask{s, 0, p, std::min(mz, pairs - p)});
+      const int my = std::max(1, std::min(nzh, FFT_SMEM_HOST / ny));
+      for (int x = 0; x < nx; ++x)
+        for (int k = 0; k < nzh; k += my) ty.push_back(FftTask{s, x, k, std::min(my, nzh - k)});
+      task_x_start[s] = (int)tx.size();
+      const int mx = std::max(1, std::min(nzh, FFT_SMEM_HOST / nx));
+      for (int y = 0; y < ny; ++y)
+        for (int k = 0; k < nzh; k += mx) tx.push_back(FftTask{s, y, k, std::min(mx, nzh - k)});
+    }
+    task_x_start[S] = (int)tx.size();
+    fixed_grid.alloc(gbase);
+    fixed_grid.zero();
+    half.alloc(hbase);
+    real_grid.alloc(gbase);
+    real_grid.zero();
+    moduli.upload(h_mod);
+    twiddles.upload(h_tw);
+    fft_plans.upload(h_plans);
+    tasks_z.upload(tz);
+    tasks_y.upload(ty);
+    tasks_x.upload(tx);
+    e_pme.alloc(tx.size());
+    e_pme.zero();
+  }
+
+  // ---- per-system device state
+  sysd.upload(h_sysd);
+  sys.upload(h_sys);
+  launch_update_box(sys.p, sysd.p, S, stream);
+  CUDA_OK(cudaStreamSynchronize(stream));
+  CUDA_OK(cudaMemcpy(h_sys.data(), sys.p, sizeof(DevSys) * S, cudaMemcpyDeviceToHost));
+  allocate_neighbours();
+
+  std::vector<DevInteg> h_integ(S);
+  for (int s = 0; s < S; ++s) {
+    const rmd_options &o = hs[s].opt;
+    const double decay = std::exp(-o.friction * o.timestep);
+    h_integ[s] = DevInteg{(float)(0.5 * o.timestep), (float)decay,
+                          (float)std::sqrt(std::max(0.0, 1.0 - decay * decay)),
+                          (float)(BOLTZMANN * o.temperature), (float)hs[s].tolerance, o.seed,
+                          o.max_constraint_iterations > 0 ? o.max_constraint_iterations : 150, 0};
+  }
+  integ.upload(h_integ);
+  step_base.alloc(S);
+  step_base.zero();
+  disp.alloc(2 * S);
+  disp.zero();
+  diag.alloc(4 * S);
+  diag.zero();
+  energies.alloc((size_t)S * N_ENERGY);
+  energies.zero();
+  saved_energies.alloc((size_t)S * N_ENERGY);
+  saved_energies.zero();
+  fixed_scales.alloc(S);
+  {
+    std::vector<double> hb(S * (size_t)N_BARO, 0.0);
+    for (int s = 0; s < S; ++s) {
+      const HostSystem &h = hs[s];
+      double *b = hb.data() + (size_t)s * N_BARO;
+      any_pressure = any_pressure || h.has_pressure;
+      b[B_ACTIVE] = h.has_pressure ? 1.0 : 0.0;
+      b[B_PRESSURE] = h.has_pressure ? h.opt.pressure * BAR_TO_KJ_PER_MOL_NM3 : 0.0;
+      b[B_KT] = BOLTZMANN * h.opt.temperature;
+      b[B_NMOL] = h.n_molecules;
+      b[B_SEED] = (double)h.opt.seed;
+    }
+    std::vector<double> tmp = hb;
+    baro.upload(tmp);
+  }
+  // ---- energy segments
+  {
+    std::vector<Segment> seg;
+    for (int s = 0; s < S; ++s) {
+      const HostSystem &h = hs[s];
+      const long long a0 = h.atom_start, a1 = h.atom_start + h.n;
+      seg.push_back(Segment{s, E_BOND, e_term.p, bstart[s], bstart[s + 1], nullptr});
+      seg.push_back(Segment{s, E_ANGLE, e_term.p, n_bonds + astart[s], n_bonds + astart[s + 1], nullptr});
+      seg.push_back(Segment{s, E_TORSION, e_term.p, n_bonds + n_angles + tstart[s],
+                            n_bonds + n_angles + tstart[s + 1], nullptr});
+      seg.push_back(Segment{s, E_RESTRAINT, e_term.p, n_bonds + n_angles + n_tors + rstart[s],
+                            n_bonds + n_angles + n_tors + rstart[s + 1], nullptr});
+      seg.push_back(Segment{s, E_LJ, e_lj.p, a0, a1, nullptr});
+      seg.push_back(Segment{s, E_COUL_DIRECT, e_coul.p, a0, a1, nullptr});
+      seg.push_back(Segment{s, E_RECIP, e_pme.p, task_x_start[s], task_x_start[s + 1], nullptr});
+      seg.push_back(Segment{s, E_KINETIC, ke_post.p, a0, a1, nullptr});
+      seg.push_back(Segment{s, E_KINETIC_EARLY, ke_early.p, a0, a1, nullptr});
+    }
+    n_segments = (int)seg.size();
+    segments.upload(seg);
+    seg_out.alloc(n_segments);
+  }
+}
+
+void Engine::allocate_neighbours() {
+  long long total = 0;
+  for (int s = 0; s < S; ++s) {
+    h_sys[s].nbr_base = total;
+    h_sys[s].nbr_capacity = hs[s].capacity;
+    total += (long long)hs[s].n * hs[s].capacity;
+  }
+  nbr.alloc(total);
+  nbr.zero();
+  nbr_count.alloc(N);
+  nbr_count.zero();
+  // push only the neighbour fields (the box may have been changed on the device)
+  std::vector<DevSys> cur(S);
+  CUDA_OK(cudaMemcpy(cur.data(), sys.p, sizeof(DevSys) * S, cudaMemcpyDeviceToHost));
+  for (int s = 0; s < S; ++s) {
+    cur[s].nbr_base = h_sys[s].nbr_base;
+    cur[s].nbr_capacity = h_sys[s].nbr_capacity;
+  }
+  CUDA_OK(cudaMemcpy(sys.p, cur.data(), sizeof(DevSys) * S, cudaMemcpyHostToDevice));
+  h_sys = cur;
+  for (auto &kv : graphs) cudaGraphExecDestroy(kv.second);
+  graphs.clear();
+}
+
+LaunchCtx Engine::ctx() const {
+  LaunchCtx c{};
+  c.n_atoms = N;
+  c.n_systems = S;
+  c.posq = posq.p;
+  c.atom_type = atom_type.p;
+  c.sys_of_atom = sys_of_atom.p;
+  c.sys = sys.p;
+  c.sysd = sysd.p;
+  c.cell_of_atom = cell_of_atom.p;
+  c.cell_count = cell_count.p;
+  c.cell_start = cell_start.p;
+  c.cell_atoms = cell_atoms.p;
+  c.cell_sys = cell_sys.p;
+  c.n_cells_total = n_cells_total;
+  c.excl_start = excl_start.p;
+  c.excl_partners = excl_partners.p;
+  c.nbr = nbr.p;
+  c.nbr_count = nbr_count.p;
+  c.required = required.p;
+  c.origin = origin.p;
+  c.lj = lj.p;
+  c.exc_start = exc_start.p;
+  c.exc_partner = exc_partner.p;
+  c.exc_param = exc_param.p;
+  c.force = force.p;
+  c.e_lj = e_lj.p;
+  c.e_coul = e_coul.p;
+  c.bond_atoms = bond_atoms.p;
+  c.bond_param = bond_param.p;
+  c.n_bonds = n_bonds;
+  c.angle_atoms = angle_atoms.p;
+  c.angle_param = angle_param.p;
+  c.n_angles = n_angles;
+  c.tor_atoms = tor_atoms.p;
+  c.tor_param = tor_param.p;
+  c.n_tors = n_tors;
+  c.rest_atom = rest_atom.p;
+  c.rest_param = rest_param.p;
+  c.n_rest = n_rest;
+  c.e_term = e_term.p;
+  c.pme_on = pme_on ? 1 : 0;
+  c.pme_order = pme_order;
+  c.fixed_grid = fixed_grid.p;
+  c.half = half.p;
+  c.real_grid = real_grid.p;
+  c.moduli = moduli.p;
+  c.twiddles = twiddles.p;
+  c.fft_plans = fft_plans.p;
+  c.tasks_z = tasks_z.p;
+  c.tasks_y = tasks_y.p;
+  c.tasks_x = tasks_x.p;
+  c.n_tasks_z = (int)tasks_z.n;
+  c.n_tasks_y = (int)tasks_y.n;
+  c.n_tasks_x = (int)tasks_x.n;
+  c.e_pme = e_pme.p;
+  return c;
+}
+
+IntegrateArgs Engine::iargs(int step_offset) const {
+  IntegrateArgs a{};
+  a.n_free = n_free;
+  a.n_clusters = n_clusters;
+  a.n_settle = n_settle;
+  a.n_units = n_free + n_clusters + n_settle;
+  a.n_atoms = N;
+  a.n_systems = S;
+  a.free_atoms = free_atoms.p;
+  a.cl_atom_start = cl_atom_start.p;
+  a.cl_atoms = cl_atoms.p;
+  a.cl_con_start = cl_con_start.p;
+  a.cl_con_pair = cl_con_pair.p;
+  a.cl_con_dist = cl_con_dist.p;
+  a.settle_atoms = settle_atoms.p;
+  a.settle_param = settle_param.p;
+  a.sys_of_atom = sys_of_atom.p;
+  a.sys_atom_start = sys_atom_start.p;
+  a.integ = integ.p;
+  a.step_base = step_base.p;
+  a.step_offset = step_offset;
+  a.posq = posq.p;
+  a.vel = vel.p;
+  a.force = force.p;
+  a.noise = noise.p;
+  a.origin = origin.p;
+  a.disp = disp.p;
+  a.diag = diag.p;
+  a.ke_post = ke_post.p;
+  a.ke_early = ke_early.p;
+  a.saved_posq = saved_posq.p;
+  return a;
+}
+
+BaroArgs Engine::bargs() const {
+  BaroArgs a{};
+  a.n_systems = S;
+  a.n_atoms = N;
+  a.n_molecules = n_molecules_total;
+  a.posq = posq.p;
+  a.saved_posq = saved_posq.p;
+  a.force = force.p;
+  a.saved_force = saved_force.p;
+  a.mol_start = mol_start.p;
+  a.mol_atoms = mol_atoms.p;
+  a.sys_of_atom = sys_of_atom.p;
+  a.sys = sys.p;
+  a.sysd = sysd.p;
+  a.baro = baro.p;
+  a.energies = energies.p;
+  a.saved_energies = saved_energies.p;
+  a.masses = masses.p;
+  return a;
+}
+
+// ------------------------------------------------------------------------ operations
+void Engine::record_forces(bool rebuild, bool energy) {
+  const LaunchCtx c = ctx();
+  if (rebuild) {
+    CUDA_OK(cudaMemsetAsync(required.p, 0, sizeof(int) * S, stream));
+    CUDA_OK(cudaMemsetAsync(disp.p, 0, sizeof(unsigned) * S, stream));  // slot 0: since rebuild
+    launch_rebuild(c, stream);
+    recorded += 5;
+  }
+  launch_nonbonded(c, energy, nb_lanes, stream);
+  launch_bonded(c, energy, stream);
+  launch_pme(c, energy, stream);
+  recorded += 1 + (n_bonds + n_angles + n_tors + n_rest > 0 ? 1 : 0) + (pme_on ? 7 : 0);
+  if (energy) {
+    launch_energy_reduce(segments.p, n_segments, seg_out.p, energies.p, sysd.p, S, stream);
+    recorded += 2;
+  }
+}
+
+void Engine::evaluate(bool rebuild, bool energy) {
+  const long long before = recorded;
+  record_forces(rebuild, energy);
+  kernel_launches += recorded - before;
+  CUDA_OK(cudaGetLastError());
+}
+
+void Engine::record_barostat() {
+  const BaroArgs b = bargs();
+  launch_baro_propose(b, stream);
+  launch_baro_scale(b, stream);
+  record_forces(true, true);
+  launch_baro_decide(b, stream);
+  launch_baro_restore(b, stream);
+  recorded += 4;
+}
+
+void Engine::set_state(int s, const double *pos, const double *vel_in, int64_t step, int supplied) {
+  HostSystem &h = hs[s];
+  // constraintToleranceFloor (clusters.js:136-148)
+  double span = 0;
+  for (int k = 0; k < 3 * h.n; ++k) span = std::max(span, std::fabs(pos[k]));
+  h.tol_floor = std::isfinite(h.min_constraint) ? 4.0 * span * std::ldexp(1.0, -24) / h.min_constraint : 0.0;
+  h.tolerance = std::max(h.requested_tol, h.tol_floor);
+  std::vector<float4> p(h.n), v(h.n);
+  for (int i = 0; i < h.n; ++i) {
+    p[i] = make_float4((float)pos[3 * i], (float)pos[3 * i + 1], (float)pos[3 * i + 2], (float)h.charges[i]);
+    v[i] = make_float4(vel_in ? (float)vel_in[3 * i] : 0.f, vel_in ? (float)vel_in[3 * i + 1] : 0.f,
+                       vel_in ? (float)vel_in[3 * i + 2] : 0.f, h.masses[i] > 0 ? (float)(1.0 / h.masses[i]) : 0.f);
+  }
+  CUDA_OK(cudaMemcpy(posq.p + h.atom_start, p.data(), sizeof(float4) * h.n, cudaMemcpyHostToDevice));
+  CUDA_OK(cudaMemcpy(vel.p + h.atom_start, v.data(), sizeof(float4) * h.n, cudaMemcpyHostToDevice));
+  long long sb = step;
+  CUDA_OK(cudaMemcpy(step_base.p + s, &sb, sizeof sb, cudaMemcpyHostToDevice));
+  DevInteg di;
+  CUDA_OK(cudaMemcpy(&di, integ.p + s, sizeof di, cudaMemcpyDeviceToHost));
+  di.tolerance = (float)h.tolerance;
+  di.supplied_noise = supplied;
+  CUDA_OK(cudaMemcpy(integ.p + s, &di, sizeof di, cudaMemcpyHostToDevice));
+  CUDA_OK(cudaMemset(diag.p + 4 * s, 0, sizeof(int) * 4));
+  h.step = step;
+  h.steps_since_rebuild = 1LL << 40;
+  h.kinetic_sampled_in_step = false;
+}
+
+int Engine::check_capacity() {
+  std::vector<int> req(S);
+  CUDA_OK(cudaMemcpy(req.data(), required.p, sizeof(int) * S, cudaMemcpyDeviceToHost));
+  bool grow = false;
+  int worst = 0;
+  for (int s = 0; s < S; ++s) {
+    hs[s].last_required = req[s];
+    hs[s].worst_required = std::max(hs[s].worst_required, req[s]);
+    worst = std::max(worst, req[s]);
+    if (req[s] > hs[s].capacity) {  // grownPlan (cells.js:282-288)
+      hs[s].capacity = std::max(hs[s].capacity + 32, (int)std::ceil(req[s] * 1.25));
+      hs[s].neighbour_growths++;
+      grow = true;
+    }
+  }
+  if (grow) {
+    allocate_neighbours();
+    evaluate(true, false);
+    sync();
+    CUDA_OK(cudaMemcpy(req.data(), required.p, sizeof(int) * S, cudaMemcpyDeviceToHost));
+    for (int s = 0; s < S; ++s) {
+      if (req[s] > hs[s].capacity)
+        throw Error(RMD_ERR_NEIGHBOUR_OVERFLOW,
+                    "the neighbour list needed " + std::to_string(req[s]) + " slots per atom and the capacity is " +
+                        std::to_string(hs[s].capacity) + ". Pairs were dropped, so the forces from this build are "
+                        "not usable. Rebuild with a larger neighbourSlack, or a smaller skin.");
+      hs[s].last_required = req[s];
+    }
+  }
+  return worst;
+}
+
+void Engine::initialise() {
+  evaluate(true, false);
+  sync();
+  for (auto &h : hs) h.steps_since_rebuild = 0;
+  check_capacity();
+  // kinetic energies of the current velocities, for energy() before any step
+  launch_integrate(iargs(0), INT_CLOSE_KINETIC, stream);
+  kernel_launches += 1;
+  sync();
+}
+
+void Engine::run_block(int n, bool barostat, bool energy_last) {
+  // rebuild pattern, identical for every system of the batch (the smallest interval wins)
+  int interval = 1 << 30;
+  int64_t since = 1LL << 40;
+  for (auto &h : hs) {
+    interval = std::min(interval, h.rebuild_interval);
+    since = std::min<int64_t>(since, h.steps_since_rebuild);
+  }
+  if (barostat) since = 1LL << 40;
+  std::string key = "n" + std::to_string(n) + (barostat ? "B" : "") + (energy_last ? "E" : "") + ":";
+  std::vector<char> rebuild(n, 0);
+  for (int k = 0; k < n; ++k) {
+    if (since >= interval) {
+      rebuild[k] = 1;
+      since = 0;
+    }
+    since++;
+    key.push_back(rebuild[k] ? 'r' : '.');
+  }
+  auto it = graphs.find(key);
+  if (it == graphs.end()) {
+    cudaGraph_t graph;
+    const long long before = recorded;
+    CUDA_OK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+    CUDA_OK(cudaMemsetAsync(disp.p + S, 0, sizeof(unsigned) * S, stream));  // slot 1: since block start
+    if (barostat) record_barostat();
+    for (int k = 0; k < n; ++k) {
+      int mode = (k == 0 ? INT_OPEN : (INT_CLOSE | INT_OPEN));
+      if (k == n - 1) mode |= INT_OPEN_KINETIC;
+      launch_integrate(iargs(k), mode, stream);
+      record_forces(rebuild[k] != 0, energy_last && k == n - 1);
+    }
+    launch_integrate(iargs(n - 1), INT_CLOSE | INT_CLOSE_KINETIC, stream);
+    launch_advance_steps(step_base.p, S, n, stream);
+    recorded += n + 2;
+    CUDA_OK(cudaStreamEndCapture(stream, &graph));
+    graph_launches[key] = recorded - before;
+    cudaGraphExec_t exec;
+    CUDA_OK(cudaGraphInstantiate(&exec, graph, 0));
+    CUDA_OK(cudaGraphDestroy(graph));
+    it = graphs.emplace(key, exec).first;
+  }
+  if (timing) {
+    if (flush) CUDA_OK(cudaMemsetAsync(flush_buffer.p, (int)(kernel_launches & 0xff), flush_buffer.n, stream));
+    CUDA_OK(cudaEventRecord(ev_a, stream));
+  }
+  CUDA_OK(cudaGraphLaunch(it->second, stream));
+  if (timing) {
+    CUDA_OK(cudaEventRecord(ev_b, stream));
+    CUDA_OK(cudaEventSynchronize(ev_b));
+    float ms = 0.f;
+    CUDA_OK(cudaEventElapsedTime(&ms, ev_a, ev_b));
+    timed_ms += ms;
+  }
+  kernel_launches += graph_launches[key];
+  // host bookkeeping mirrors the device
+  for (auto &h : hs) {
+    int64_t s2 = barostat ? (1LL << 40) : h.steps_since_rebuild;
+    for (int k = 0; k < n; ++k) {
+      if (s2 >= interval) s2 = 0;
+      s2++;
+    }
+    h.steps_since_rebuild = s2;
+    h.step += n;
+    h.kinetic_sampled_in_step = true;
+    h.kinetic_sampled_at = h.step;
+  }
+}
+
+// #checkSkin (simulation.js:544-623) and #checkNeighbourCapacity (simulation.js:424-443)
+void Engine::check_block(int steps) {
+  std::vector<unsigned> d(2 * S);
+  CUDA_OK(cudaMemcpy(d.data(), disp.p, sizeof(unsigned) * 2 * S, cudaMemcpyDeviceToHost));
+  for (int s = 0; s < S; ++s) {
+    HostSystem &h = hs[s];
+    float f0, f1;
+    memcpy(&f0, &d[s], 4);
+    memcpy(&f1, &d[S + s], 4);
+    const float sq = std::max(f0, f1);
+    if (!std::isfinite(f0) || !std::isfinite(f1))
+      throw Error(RMD_ERR_NON_FINITE,
+                  "the simulation is no longer a number: the maximum atomic displacement over the last block "
+                  "went non-finite at step " + std::to_string(h.step) +
+                  ". The usual causes, commonest first: a timestep too large for this system; two atoms at the "
+                  "same coordinate in the input; a structure that was never minimised; or a restart whose "
+                  "velocities do not belong to its positions.");
+    const double worst = std::sqrt(std::max(0.0, (double)sq));
+    h.worst_displacement = std::max(h.worst_displacement, worst);
+    const double usage = 2.0 * worst / h.skin;
+    h.worst_skin_usage = std::max(h.worst_skin_usage, usage);
+    if (usage <= 1.0) {
+      h.calm_blocks++;
+      if (h.adaptive && usage < 0.4 && h.calm_blocks >= 3 && h.rebuild_interval < h.requested_rebuild) {
+        h.rebuild_interval = std::min(h.requested_rebuild,
+                                      std::max(h.rebuild_interval + 1, (int)std::floor(h.rebuild_interval * 1.25)));
+        h.rebuild_growths++;
+        h.calm_blocks = 0;
+      }
+      continue;
+    }
+    h.skin_violations++;
+    h.calm_blocks = 0;
+    h.steps_with_stale += steps;
+    h.worst_skin_ratio = std::max(h.worst_skin_ratio, usage);
+    const int shrunk = std::max(1, h.rebuild_interval / 2);
+    if (h.adaptive && shrunk != h.rebuild_interval) {
+      h.rebuild_interval = shrunk;
+      h.rebuild_shrinks++;
+    }
+    h.steps_since_rebuild = 1LL << 40;
+  }
+  check_capacity();
+}
+
+void Engine::run(int64_t count, int block, const volatile int32_t *stop) {
+  int64_t remaining = count;
+  while (remaining > 0) {
+    if (stop && *stop) throw Error(RMD_ERR_STOPPED, "the simulation was stopped");
+    bool due = false;
+    for (auto &h : hs)
+      if (h.has_pressure && h.steps_since_barostat >= h.barostat_interval) due = true;
+    int interval = 1 << 30;
+    for (auto &h : hs) interval = std::min(interval, h.rebuild_interval);
+    int n = block > 0 ? block : interval;
+    n = (int)std::min<int64_t>(n, remaining);
+    // the last force evaluation of a block is energy-enabled when a volume move follows
+    bool next_due = false;
+    for (auto &h : hs)
+      if (h.has_pressure && (due ? 0 : h.steps_since_barostat) + n >= h.barostat_interval) next_due = true;
+    if (due) {
+      // the move needs the energy at the current positions
+      evaluate(false, true);
+    }
+    run_block(n, due, next_due);
+    sync();
+    if (due) {
+      for (auto &h : hs) h.steps_since_barostat = 0;
+      std::vector<double> b((size_t)S * N_BARO);
+      CUDA_OK(cudaMemcpy(b.data(), baro.p, sizeof(double) * b.size(), cudaMemcpyDeviceToHost));
+      for (int s = 0; s < S; ++s) {
+        HostSystem &h = hs[s];
+        const double *bb = b.data() + (size_t)s * N_BARO;
+        if (!h.has_pressure) continue;
+        rmd_volume_move &m = h.last_move;
+        m.attempted = 1;
+        m.accepted = bb[B_ACCEPT] != 0.0 && bb[B_REFUSED] == 0.0;
+        m.refused = bb[B_REFUSED] != 0.0;
+        m.weight = bb[B_WEIGHT];
+        m.delta_volume = bb[B_DV];
+        m.length_scale = bb[B_LSCALE];
+        m.old_potential = bb[B_OLD_E];
+        m.new_potential = bb[B_NEW_E];
+        m.volume_scale = bb[B_SCALE];
+        m.acceptance_rate = bb[B_ATTEMPTS] > 0 ? bb[B_ACCEPTED] / bb[B_ATTEMPTS] : 0;
+      }
+    }
+    for (auto &h : hs)
+      if (h.has_pressure) h.steps_since_barostat += n;
+    check_block(n);
+    remaining -= n;
+  }
+}
+
+std::vector<double> Engine::read_energies() {
+  std::vector<double> e((size_t)S * N_ENERGY);
+  CUDA_OK(cudaMemcpy(e.data(), energies.p, sizeof(double) * e.size(), cudaMemcpyDeviceToHost));
+  return e;
+}
+
+void Engine::energy(int s, rmd_energy_report *out) {
+  // forces and energies at the current positions, with the current list (no rebuild: the
+  // skin keeps it valid), then the kinetic sums (simulation.js:1073-1230)
+  evaluate(false, true);
+  sync();
+  const std::vector<double> all = read_energies();
+  const double *e = all.data() + (size_t)s * N_ENERGY;
+  HostSystem &h = hs[s];
+  DevSysD d;
+  CUDA_OK(cudaMemcpy(&d, sysd.p + s, sizeof d, cudaMemcpyDeviceToHost));
+  memset(out, 0, sizeof *out);
+  out->step = h.step;
+  out->time = h.step * h.opt.timestep;
+  out->harmonic_bond = e[E_BOND];
+  out->harmonic_angle = e[E_ANGLE];
+  out->periodic_torsion = e[E_TORSION];
+  out->bonded = e[E_BOND] + e[E_ANGLE] + e[E_TORSION];
+  out->lennard_jones = e[E_LJ];
+  out->dispersion = e[E_DISPERSION];
+  out->coulomb_direct = e[E_COUL_DIRECT];
+  out->coulomb_reciprocal = e[E_RECIP];
+  out->coulomb_self = e[E_SELF] + e[E_NET];
+  out->coulomb = e[E_COUL_DIRECT] + e[E_RECIP] + e[E_SELF] + e[E_NET];
+  out->position_restraint = e[E_RESTRAINT];
+  out->restrained_atoms = (int)h.restraint_atoms.size();
+  out->potential = e[E_POTENTIAL];
+  out->kinetic = e[E_KINETIC];
+  out->total = out->potential + out->kinetic;
+  double kt = e[E_KINETIC];
+  out->kinetic_sampled_before_closing_kick = 0;
+  if (h.kinetic_sampled_in_step && h.kinetic_sampled_at == h.step && (e[E_KINETIC_EARLY] > 0 || kt <= 0)) {
+    kt = e[E_KINETIC_EARLY];
+    out->kinetic_sampled_before_closing_kick = 1;
+  }
+  out->kinetic_for_temperature = kt;
+  out->temperature = 2.0 * kt / (h.dof * BOLTZMANN);
+  out->volume = d.volume;
+  for (int k = 0; k < 9; ++k) out->box_vectors[k] = d.box[k];
+  if (!std::isfinite(out->potential) || !std::isfinite(out->kinetic))
+    throw Error(RMD_ERR_NON_FINITE, std::string("the simulation is no longer a number: the ") +
+                                        (!std::isfinite(out->potential) ? "potential" : "kinetic") +
+                                        " energy went non-finite at step " + std::to_string(h.step));
+}
+
+void Engine::attempt_volume_change() {
+  // energy at the current positions, then one device-side move on every system
+  evaluate(false, true);
+  const BaroArgs b = bargs();
+  record_barostat();
+  CUDA_OK(cudaGetLastError());
+  sync();
+  for (auto &h : hs) h.steps_since_rebuild = 1LL << 40;
+  std::vector<double> bb((size_t)S * N_BARO);
+  CUDA_OK(cudaMemcpy(bb.data(), baro.p, sizeof(double) * bb.size(), cudaMemcpyDeviceToHost));
+  std::vector<DevSysD> dd(S);
+  CUDA_OK(cudaMemcpy(dd.data(), sysd.p, sizeof(DevSysD) * S, cudaMemcpyDeviceToHost));
+  (void)b;
+  for (int s = 0; s < S; ++s) {
+    HostSystem &h = hs[s];
+    const double *x = bb.data() + (size_t)s * N_BARO;
+    rmd_volume_move &m = h.last_move;
+    memset(&m, 0, sizeof m);
+    if (!h.has_pressure) continue;
+    m.attempted = 1;
+    m.refused = x[B_REFUSED] != 0.0;
+    m.accepted = !m.refused && x[B_ACCEPT] != 0.0;
+    m.weight = x[B_WEIGHT];
+    m.delta_volume = x[B_DV];
+    m.length_scale = x[B_LSCALE];
+    m.old_potential = x[B_OLD_E];
+    m.new_potential = x[B_NEW_E];
+    m.volume = dd[s].volume;
+    m.volume_scale = x[B_SCALE];
+    m.acceptance_rate = x[B_ATTEMPTS] > 0 ? x[B_ACCEPTED] / x[B_ATTEMPTS] : 0.0;
+  }
+}
+
+double Engine::scale_volume(int s, double ls) {
+  // scaleVolume (simulation.js:801-811): centroid scaling and the box, then the potential
+  std::vector<double> scales(S, 1.0);
+  scales[s] = ls;
+  CUDA_OK(cudaMemcpy(fixed_scales.p, scales.data(), sizeof(double) * S, cudaMemcpyHostToDevice));
+  launch_scale_fixed(bargs(), fixed_scales.p, stream);
+  DevSysD d;
+  CUDA_OK(cudaMemcpy(&d, sysd.p + s, sizeof d, cudaMemcpyDeviceToHost));
+  for (int k = 0; k < 9; ++k) d.box[k] *= ls;
+  CUDA_OK(cudaMemcpy(sysd.p + s, &d, sizeof d, cudaMemcpyHostToDevice));
+  launch_update_box(sys.p, sysd.p, S, stream);
+  evaluate(true, true);
+  sync();
+  for (auto &h : hs) h.steps_since_rebuild = 0;
+  check_capacity();
+  return read_energies()[(size_t)s * N_ENERGY + E_POTENTIAL];
+}
+
+std::vector<float> Engine::max_forces() {
+  DevArray<unsigned> bits;
+  bits.alloc(S);
+  bits.zero();
+  launch_max_force(force.p, sys_of_atom.p, N, bits.p, stream);
+  sync();
+  std::vector<unsigned> b(S);
+  CUDA_OK(cudaMemcpy(b.data(), bits.p, sizeof(unsigned) * S, cudaMemcpyDeviceToHost));
+  bits.release();
+  std::vector<float> out(S);
+  for (int s = 0; s < S; ++s) memcpy(&out[s], &b[s], 4);
+  return out;
+}
+
+// minimise (simulation.js:880-979): steepest descent with a backtracking line search, one
+// host decision per trial. Every system of a batch keeps its own step and acceptance.
+// Departure: the positions AND forces of the last accepted structure are restored after a
+// rejected trial, so the next trial moves along the accepted gradient.
+void Engine::minimise(int max_iterations, double force_tolerance, double max_step, double cap,
+                      rmd_minimise_result *out) {
+  if (max_iterations <= 0) max_iterations = 200;
+  if (!(force_tolerance > 0)) force_tolerance = 500;
+  if (!(max_step > 0)) max_step = 0.002;
+  if (!(cap > 0)) cap = 0.05;
+  auto potentials = [&]() {
+    evaluate(true, true);
+    sync();
+    for (auto &h : hs) h.steps_since_rebuild = 0;
+    check_capacity();
+    std::vector<double> e = read_energies(), p(S);
+    for (int s = 0; s < S; ++s) p[s] = e[(size_t)s * N_ENERGY + E_POTENTIAL];
+    return p;
+  };
+  std::vector<double> potential = potentials(), step(S, max_step);
+  std::vector<char> done(S, 0), stalled(S, 0);
+  std::vector<int> iterations(S, 0), rejected(S, 0);
+  DevArray<float> scale;
+  scale.alloc(S);
+  const size_t fbytes = sizeof(unsigned long long) * 3 * (size_t)N;
+  for (int it = 0; it < max_iterations; ++it) {
+    std::vector<float> worst = max_forces();
+    bool any = false;
+    for (int s = 0; s < S; ++s) {
+      if (done[s]) continue;
+      iterations[s] = it + 1;
+      if (worst[s] <= force_tolerance) done[s] = 1;
+      else any = true;
+    }
+    if (!any) break;
+    CUDA_OK(cudaMemcpyAsync(saved_posq.p, posq.p, sizeof(float4) * N, cudaMemcpyDeviceToDevice, stream));
+    CUDA_OK(cudaMemcpyAsync(saved_force.p, force.p, fbytes, cudaMemcpyDeviceToDevice, stream));
+    std::vector<char> accepted(S, 0), active(S, 0);
+    for (int s = 0; s < S; ++s) active[s] = !done[s];
+    for (int attempt = 0; attempt < 14; ++attempt) {
+      std::vector<float> sc(S, 0.f);
+      bool pending = false;
+      for (int s = 0; s < S; ++s)
+        if (active[s] && !accepted[s]) {
+          sc[s] = (float)(step[s] / std::max((double)worst[s], 1e-6));
+          pending = true;
+        }
+      if (!pending) break;
+      CUDA_OK(cudaMemcpyAsync(scale.p, sc.data(), sizeof(float) * S, cudaMemcpyHostToDevice, stream));
+      launch_displace(posq.p, force.p, sys_of_atom.p, N, scale.p, (float)cap, stream);
+      launch_integrate(iargs(0), INT_CONSTRAIN, stream);
+      std::vector<double> trial = potentials();
+      bool restore = false;
+      for (int s = 0; s < S; ++s) {
+        if (!active[s] || accepted[s]) continue;
+        if (trial[s] < potential[s]) {
+          potential[s] = trial[s];
+          step[s] *= 1.3;
+          accepted[s] = 1;
+        } else {
+          rejected[s]++;
+          step[s] *= 0.5;
+          restore = true;
+          if (step[s] < 1e-9) active[s] = 0;
+        }
+      }
+      if (restore) {
+        // put back every not-yet-accepted system (accepted ones keep their new state)
+        std::vector<float4> cur(N), old(N);
+        std::vector<unsigned long long> fc(3 * (size_t)N), fo(3 * (size_t)N);
+        CUDA_OK(cudaMemcpy(cur.data(), posq.p, sizeof(float4) * N, cudaMemcpyDeviceToHost));
+        CUDA_OK(cudaMemcpy(old.data(), saved_posq.p, sizeof(float4) * N, cudaMemcpyDeviceToHost));
+        CUDA_OK(cudaMemcpy(fc.data(), force.p, fbytes, cudaMemcpyDeviceToHost));
+        CUDA_OK(cudaMemcpy(fo.data(), saved_force.p, fbytes, cudaMemcpyDeviceToHost));
+        for (int s = 0; s < S; ++s) {
+          if (accepted[s]) continue;
+          for (int i = hs[s].atom_start; i < hs[s].atom_start + hs[s].n; ++i) {
+            cur[i] = old[i];
+            for (int c = 0; c < 3; ++c) fc[(size_t)c * N + i] = fo[(size_t)c * N + i];
+          }
+        }
+        CUDA_OK(cudaMemcpy(posq.p, cur.data(), sizeof(float4) * N, cudaMemcpyHostToDevice));
+        CUDA_OK(cudaMemcpy(force.p, fc.data(), fbytes, cudaMemcpyHostToDevice));
+      }
+    }
+    for (int s = 0; s < S; ++s)
+      if (!done[s] && !accepted[s]) {
+        stalled[s] = 1;
+        done[s] = 1;
+      }
+  }
+  scale.release();
+  // forces at the final structure, and velocities zeroed (simulation.js:971-973)
+  potential = potentials();
+  std::vector<float> worst = max_forces();
+  std::vector<float4> v(N);
+  CUDA_OK(cudaMemcpy(v.data(), vel.p, sizeof(float4) * N, cudaMemcpyDeviceToHost));
+  for (auto &x : v) x.x = x.y = x.z = 0.f;
+  CUDA_OK(cudaMemcpy(vel.p, v.data(), sizeof(float4) * N, cudaMemcpyHostToDevice));
+  launch_integrate(iargs(0), INT_CLOSE_KINETIC, stream);
+  sync();
+  if (out) {
+    out->iterations = iterations[0];
+    out->rejected = rejected[0];
+    out->stalled = stalled[0];
+    out->converged = worst[0] <= force_tolerance;
+    out->potential = potential[0];
+    out->max_force = worst[0];
+    out->max_step = step[0];
+  }
+}
+
+}  // namespace rmd
+
+// =========================================================================== C ABI
+struct rmd_sim {
+  rmd::Engine engine;
+};
+
+static std::string g_create_error;
+
+template <class F>
+static rmd_status guarded(rmd_sim *sim, F &&f) {
+  try {
+    f();
+    return RMD_OK;
+  } catch (const rmd::Error &e) {
+    if (sim) sim->engine.last_error = e.what();
+    else g_create_error = e.what();
+    return e.code;
+  } catch (const std::exception &e) {
+    if (sim) sim->engine.last_error = e.what();
+    else g_create_error = e.what();
+    return RMD_ERR_CUDA;
+  }
+}
+
+static rmd_status check_index(rmd_sim *sim, int32_t s) {
+  if (!sim) return RMD_ERR_INVALID;
+  if (s < 0 || s >= sim->engine.S) {
+    sim->engine.last_error = "system index out of range";
+    return RMD_ERR_INVALID;
+  }
+  return RMD_OK;
+}
+
+extern "C" {
+
+void rmd_default_options(rmd_options *o) {
+  memset(o, 0, sizeof *o);
+  o->timestep = 0.002;
+  o->temperature = 298.0;
+  o->friction = 1.0;
+  o->seed = 0;
+  o->tolerance = 1e-5;
+  o->max_constraint_iterations = 150;
+  o->rebuild_interval = 20;
+  o->adaptive_rebuild = 1;
+  o->pressure = RMD_NO_PRESSURE;
+  o->barostat_interval = 25;
+  o->dispersion_correction = 1;
+  o->neighbour_slack = 2.0;
+  o->ewald_tolerance = 5e-4;
+  o->pme_order = 5;
+}
+
+rmd_status rmd_create_batch(int32_t count, const rmd_system *systems, const rmd_options *options,
+                            rmd_sim **out) {
+  *out = nullptr;
+  if (count <= 0 || !systems) {
+    g_create_error = "rmd_create_batch needs at least one system";
+    return RMD_ERR_INVALID;
+  }
+  rmd_sim *sim = new rmd_sim();
+  rmd_options defaults;
+  rmd_default_options(&defaults);
+  std::vector<rmd_options> per(count, options ? options[0] : defaults);
+  if (options)
+    for (int s = 0; s < count; ++s) per[s] = options[s];
+  rmd_status st = guarded(nullptr, [&]() { sim->engine.build(count, systems, per.data()); });
+  if (st != RMD_OK) {
+    delete sim;
+    return st;
+  }
+  *out = sim;
+  return RMD_OK;
+}
+
+rmd_status rmd_create(const rmd_system *system, const rmd_options *options, rmd_sim **out) {
+  return rmd_create_batch(1, system, options, out);
+}
+
+int32_t rmd_system_count(const rmd_sim *sim) { return sim ? sim->engine.S : 0; }
+
+rmd_status rmd_set_state_at(rmd_sim *sim, int32_t s, const double *positions, const double *velocities,
+                            int64_t step, int32_t supplied_noise) {
+  if (rmd_status c = check_index(sim, s)) return c;
+  if (!positions) return RMD_ERR_INVALID;
+  return guarded(sim, [&]() { sim->engine.set_state(s, positions, velocities, step, supplied_noise); });
+}
+
+rmd_status rmd_set_state(rmd_sim *sim, const double *positions, const double *velocities, int64_t step,
+                         int32_t supplied_noise) {
+  return rmd_set_state_at(sim, 0, positions, velocities, step, supplied_noise);
+}
+
+rmd_status rmd_set_noise_at(rmd_sim *sim, int32_t s, const float *noise) {
+  if (rmd_status c = check_index(sim, s)) return c;
+  return guarded(sim, [&]() {
+    auto &e = sim->engine;
+    CUDA_OK(cudaMemcpy(e.noise.p + 3 * (size_t)e.hs[s].atom_start, noise, sizeof(float) * 3 * e.hs[s].n,
+                       cudaMemcpyHostToDevice));
+  });
+}
+
+rmd_status rmd_set_noise(rmd_sim *sim, const float *noise) { return rmd_set_noise_at(sim, 0, noise); }
+
+rmd_status rmd_initialise(rmd_sim *sim) {
+  if (!sim) return RMD_ERR_INVALID;
+  return guarded(sim, [&]() { sim->engine.initialise(); });
+}
+
+rmd_status rmd_run(rmd_sim *sim, int64_t count, int32_t block_size, const volatile int32_t *stop_flag,
+                   int64_t *step_out) {
+  if (!sim) return RMD_ERR_INVALID;
+  rmd_status st = guarded(sim, [&]() { sim->engine.run(count, block_size, stop_flag); });
+  if (step_out) *step_out = sim->engine.hs[0].step;
+  return st;
+}
+
+rmd_status rmd_attempt_volume_change(rmd_sim *sim, rmd_volume_move *out) {
+  if (!sim) return RMD_ERR_INVALID;
+  rmd_status st = guarded(sim, [&]() { sim->engine.attempt_volume_change(); });
+  if (out) *out = sim->engine.hs[0].last_move;
+  return st;
+}
+
+rmd_status rmd_last_volume_move_at(rmd_sim *sim, int32_t s, rmd_volume_move *out) {
+  if (rmd_status c = check_index(sim, s)) return c;
+  *out = sim->engine.hs[s].last_move;
+  return RMD_OK;
+}
+
+rmd_status rmd_scale_volume(rmd_sim *sim, double length_scale, double *potential_out) {
+  if (!sim) return RMD_ERR_INVALID;
+  return guarded(sim, [&]() {
+    const double e = sim->engine.scale_volume(0, length_scale);
+    if (potential_out) *potential_out = e;
+  });
+}
+
+rmd_status rmd_energy_at(rmd_sim *sim, int32_t s, rmd_energy_report *out) {
+  if (rmd_status c = check_index(sim, s)) return c;
+  return guarded(sim, [&]() { sim->engine.energy(s, out); });
+}
+
+rmd_status rmd_energy(rmd_sim *sim, rmd_energy_report *out) { return rmd_energy_at(sim, 0, out); }
+
+rmd_status rmd_read_state_at(rmd_sim *sim, int32_t s, float *positions, float *velocities, float *forces,
+                             double box_vectors[9], double *volume) {
+  if (rmd_status c = check_index(sim, s)) return c;
+  return guarded(sim, [&]() {
+    auto &e = sim->engine;
+    const auto &h = e.hs[s];
+    e.sync();
+    if (positions || velocities) {
+      std::vector<float4> buf(h.n);
+      if (positions) {
+        CUDA_OK(cudaMemcpy(buf.data(), e.posq.p + h.atom_start, sizeof(float4) * h.n, cudaMemcpyDeviceToHost));
+        for (int i = 0; i < h.n; ++i) {
+          positions[3 * i] = buf[i].x;
+          positions[3 * i + 1] = buf[i].y;
+          positions[3 * i + 2] = buf[i].z;
+        }
+      }
+      if (velocities) {
+        CUDA_OK(cudaMemcpy(buf.data(), e.vel.p + h.atom_start, sizeof(float4) * h.n, cudaMemcpyDeviceToHost));
+        for (int i = 0; i < h.n; ++i) {
+          velocities[3 * i] = buf[i].x;
+          velocities[3 * i + 1] = buf[i].y;
+          velocities[3 * i + 2] = buf[i].z;
+        }
+      }
+    }
+    if (forces) {
+      std::vector<long long> f(h.n);
+      for (int c = 0; c < 3; ++c) {
+        CUDA_OK(cudaMemcpy(f.data(), e.force.p + (size_t)c * e.N + h.atom_start, sizeof(long long) * h.n,
+                           cudaMemcpyDeviceToHost));
+        for (int i = 0; i < h.n; ++i) forces[3 * i + c] = (float)((double)f[i] / rmd::FORCE_SCALE);
+      }
+    }
+    if (box_vectors || volume) {
+      rmd::DevSysD d;
+      CUDA_OK(cudaMemcpy(&d, e.sysd.p + s, sizeof d, cudaMemcpyDeviceToHost));
+      if (box_vectors)
+        for (int k = 0; k < 9; ++k) box_vectors[k] = d.box[k];
+      if (volume) *volume = d.volume;
+    }
+  });
+}
+
+rmd_status rmd_read_state(rmd_sim *sim, float *positions, float *velocities, float *forces,
+                          double box_vectors[9], double *volume) {
+  return rmd_read_state_at(sim, 0, positions, velocities, forces, box_vectors, volume);
+}
+
+rmd_status rmd_read_positions(rmd_sim *sim, float *positions) {
+  return rmd_read_state_at(sim, 0, positions, nullptr, nullptr, nullptr, nullptr);
+}
+
+rmd_status rmd_diagnostics_at(rmd_sim *sim, int32_t s, rmd_diagnostics_report *out) {
+  if (rmd_status c = check_index(sim, s)) return c;
+  return guarded(sim, [&]() {
+    auto &e = sim->engine;
+    const auto &h = e.hs[s];
+    e.sync();
+    int dg[4];
+    CUDA_OK(cudaMemcpy(dg, e.diag.p + 4 * s, sizeof dg, cudaMemcpyDeviceToHost));
+    std::vector<double> b(rmd::N_BARO);
+    CUDA_OK(cudaMemcpy(b.data(), e.baro.p + (size_t)s * rmd::N_BARO, sizeof(double) * rmd::N_BARO,
+                       cudaMemcpyDeviceToHost));
+    rmd::DevSys ds;
+    rmd::DevSysD dd;
+    CUDA_OK(cudaMemcpy(&ds, e.sys.p + s, sizeof ds, cudaMemcpyDeviceToHost));
+    CUDA_OK(cudaMemcpy(&dd, e.sysd.p + s, sizeof dd, cudaMemcpyDeviceToHost));
+    memset(out, 0, sizeof *out);
+    out->max_shake_iterations = dg[0];
+    out->shake_hit_iteration_cap = dg[1];
+    out->rattle_hit_iteration_cap = dg[2];
+    float res;
+    memcpy(&res, &dg[3], 4);
+    out->worst_stalled_residual = res;
+    out->neighbour_required = h.last_required;
+    out->neighbour_capacity = h.capacity;
+    out->worst_neighbour_required = h.worst_required;
+    out->neighbour_growths = h.neighbour_growths;
+    out->skin = h.skin;
+    out->worst_displacement = h.worst_displacement;
+    out->worst_skin_ratio = h.worst_skin_ratio;
+    out->skin_violations = h.skin_violations;
+    out->steps_with_stale_list = h.steps_with_stale;
+    out->rebuild_interval = h.rebuild_interval;
+    out->requested_rebuild_interval = h.requested_rebuild;
+    out->rebuild_shrinks = h.rebuild_shrinks;
+    out->rebuild_growths = h.rebuild_growths;
+    out->worst_skin_usage = h.worst_skin_usage;
+    out->adaptive_rebuild = h.adaptive;
+    out->volume = dd.volume;
+    out->barostat_attempts = (int)b[rmd::B_ATTEMPTS];
+    out->barostat_accepted = (int)b[rmd::B_ACCEPTED];
+    out->barostat_refused = (int)b[rmd::B_REFUSALS];
+    out->barostat_screened = (int)b[rmd::B_SCREENED_TOTAL];
+    out->barostat_exact_evaluations = (int)b[rmd::B_EXACT_EVALS];
+    out->volume_scale = b[rmd::B_SCALE];
+    out->constraint_tolerance = h.tolerance;
+    out->requested_tolerance = h.requested_tol;
+    out->tolerance_floor = h.tol_floor;
+    for (int k = 0; k < 3; ++k) {
+      out->cell_counts[k] = ds.cell_counts[k];
+      out->pme_grid[k] = h.grid[k];
+    }
+    out->pme_alpha = h.alpha;
+    out->pme_order = h.order;
+    out->cluster_count = h.n_clusters;
+    out->settle_count = h.n_settle;
+    size_t bytes = 0;
+    bytes += e.posq.bytes() * 4 + e.force.bytes() * 2 + e.nbr.bytes() + e.fixed_grid.bytes() + e.half.bytes() +
+             e.real_grid.bytes() + e.cell_atoms.bytes() * 2 + e.e_lj.bytes() * 4;
+    out->device_bytes = (int64_t)bytes;
+  });
+}
+
+rmd_status rmd_diagnostics(rmd_sim *sim, rmd_diagnostics_report *out) { return rmd_diagnostics_at(sim, 0, out); }
+
+rmd_status rmd_minimise(rmd_sim *sim, int32_t max_iterations, double force_tolerance, double max_step,
+                        double max_displacement, rmd_minimise_result *out) {
+  if (!sim) return RMD_ERR_INVALID;
+  return guarded(sim, [&]() { sim->engine.minimise(max_iterations, force_tolerance, max_step, max_displacement, out); });
+}
+
+void rmd_destroy(rmd_sim *sim) { delete sim; }
+
+const char *rmd_last_error(const rmd_sim *sim) {
+  return sim ? sim->engine.last_error.c_str() : g_create_error.c_str();
+}
+
+rmd_status rmd_debug_cells(rmd_sim *sim, int32_t s, int32_t counts[3], int32_t *cstart, int32_t *catoms) {
+  if (rmd_status c = check_index(sim, s)) return c;
+  return guarded(sim, [&]() {
+    auto &e = sim->engine;
+    e.sync();
+    rmd::DevSys ds;
+    CUDA_OK(cudaMemcpy(&ds, e.sys.p + s, sizeof ds, cudaMemcpyDeviceToHost));
+    for (int k = 0; k < 3; ++k) counts[k] = ds.cell_counts[k];
+    const int cells = ds.cell_counts[0] * ds.cell_counts[1] * ds.cell_counts[2];
+    if (cstart) CUDA_OK(cudaMemcpy(cstart, e.cell_start.p + ds.cell_start_base, sizeof(int) * (cells + 1),
+                                   cudaMemcpyDeviceToHost));
+    if (catoms) {
+      CUDA_OK(cudaMemcpy(catoms, e.cell_atoms.p + ds.atom_start, sizeof(int) * ds.atom_count, cudaMemcpyDeviceToHost));
+      for (int i = 0; i < ds.atom_count; ++i) catoms[i] -= ds.atom_start;
+    }
+  });
+}
+
+rmd_status rmd_debug_neighbours(rmd_sim *sim, int32_t s, int32_t *capacity, int32_t *counts, int32_t *rows,
+                                int32_t *req) {
+  if (rmd_status c = check_index(sim, s)) return c;
+  return guarded(sim, [&]() {
+    auto &e = sim->engine;
+    e.sync();
+    const auto &h = e.hs[s];
+    const auto &ds = e.h_sys[s];
+    if (capacity) *capacity = ds.nbr_capacity;
+    if (counts) CUDA_OK(cudaMemcpy(counts, e.nbr_count.p + h.atom_start, sizeof(int) * h.n, cudaMemcpyDeviceToHost));
+    if (rows) {
+      CUDA_OK(cudaMemcpy(rows, e.nbr.p + ds.nbr_base, sizeof(int) * (size_t)h.n * ds.nbr_capacity,
+                         cudaMemcpyDeviceToHost));
+      for (size_t k = 0; k < (size_t)h.n * ds.nbr_capacity; ++k) rows[k] -= h.atom_start;
+    }
+    if (req) CUDA_OK(cudaMemcpy(req, e.required.p + s, sizeof(int), cudaMemcpyDeviceToHost));
+  });
+}
+
+rmd_status rmd_debug_evaluate(rmd_sim *sim, int32_t s, rmd_energy_report *energy, double *forces) {
+  if (rmd_status c = check_index(sim, s)) return c;
+  return guarded(sim, [&]() {
+    auto &e = sim->engine;
+    e.evaluate(true, true);
+    e.sync();
+    for (auto &h : e.hs) h.steps_since_rebuild = 0;
+    e.check_capacity();
+    e.energy(s, energy);
+    if (forces) {
+      const auto &h = e.hs[s];
+      std::vector<long long> f(h.n);
+      for (int c = 0; c < 3; ++c) {
+        CUDA_OK(cudaMemcpy(f.data(), e.force.p + (size_t)c * e.N + h.atom_start, sizeof(long long) * h.n,
+                           cudaMemcpyDeviceToHost));
+        for (int i = 0; i < h.n; ++i) forces[3 * i + c] = (double)f[i] / rmd::FORCE_SCALE;
+      }
+    }
+  });
+}
+
+rmd_status rmd_debug_charge_grid(rmd_sim *sim, int32_t s, double *grid) {
+  if (rmd_status c = check_index(sim, s)) return c;
+  return guarded(sim, [&]() {
+    auto &e = sim->engine;
+    const auto &h = e.hs[s];
+    const rmd::LaunchCtx c = e.ctx();
+    // the z pass consumes (and zeroes) the fixed grid inside an evaluation, so spread again
+    // into a cleared grid and read it before anything else runs
+    e.sync();
+    const size_t pts = (size_t)h.grid[0] * h.grid[1] * h.grid[2];
+    CUDA_OK(cudaMemsetAsync(e.fixed_grid.p, 0, e.fixed_grid.bytes(), e.stream));
+    rmd::launch_spread_only(c, e.stream);
+    e.sync();
+    std::vector<long long> g(pts);
+    CUDA_OK(cudaMemcpy(g.data(), e.fixed_grid.p + e.h_sys[s].grid_base, sizeof(long long) * pts,
+                       cudaMemcpyDeviceToHost));
+    for (size_t k = 0; k < pts; ++k) grid[k] = (double)g[k] / rmd::FORCE_SCALE;
+    CUDA_OK(cudaMemsetAsync(e.fixed_grid.p, 0, e.fixed_grid.bytes(), e.stream));
+    e.sync();
+  });
+}
+
+rmd_status rmd_bench_run(rmd_sim *sim, int64_t count, int32_t block_size, int32_t flush_l2,
+                         double *device_ms) {
+  if (!sim) return RMD_ERR_INVALID;
+  return guarded(sim, [&]() {
+    auto &e = sim->engine;
+    if (!e.ev_a) {
+      CUDA_OK(cudaEventCreate(&e.ev_a));
+      CUDA_OK(cudaEventCreate(&e.ev_b));
+    }
+    if (flush_l2 && e.flush_buffer.n == 0) e.flush_buffer.alloc((size_t)256 << 20);  // 2x the 126 MB L2
+    e.timing = true;
+    e.flush = flush_l2 != 0;
+    e.timed_ms = 0.0;
+    try {
+      e.run(count, block_size, nullptr);
+    } catch (...) {
+      e.timing = false;
+      throw;
+    }
+    e.timing = false;
+    *device_ms = e.timed_ms;
+  });
+}
+
+rmd_status rmd_debug_time_kernel(rmd_sim *sim, int32_t which, int32_t reps, double *ms_per_launch) {
+  if (!sim || reps <= 0) return RMD_ERR_INVALID;
+  return guarded(sim, [&]() {
+    auto &e = sim->engine;
+    const rmd::LaunchCtx c = e.ctx();
+    auto one = [&]() {
+      switch (which) {
+        case 0: rmd::launch_nonbonded(c, false, e.nb_lanes, e.stream); break;
+        case 1: rmd::launch_pme(c, false, e.stream); break;
+        case 2: rmd::launch_integrate(e.iargs(0), rmd::INT_CLOSE | rmd::INT_OPEN, e.stream); break;
+        case 3: rmd::launch_bonded(c, false, e.stream); break;
+        case 4: rmd::launch_rebuild(c, e.stream); break;
+        case 5: rmd::launch_nonbonded(c, true, e.nb_lanes, e.stream); break;
+        default: throw rmd::Error(RMD_ERR_INVALID, "unknown kernel group");
+      }
+    };
+    e.sync();
+    one();  // warm
+    cudaEvent_t a, b;
+    CUDA_OK(cudaEventCreate(&a));
+    CUDA_OK(cudaEventCreate(&b));
+    CUDA_OK(cudaEventRecord(a, e.stream));
+    for (int k = 0; k < reps; ++k) one();
+    CUDA_OK(cudaEventRecord(b, e.stream));
+    CUDA_OK(cudaEventSynchronize(b));
+    float ms = 0;
+    CUDA_OK(cudaEventElapsedTime(&ms, a, b));
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    CUDA_OK(cudaGetLastError());
+    *ms_per_launch = ms / reps;
+  });
+}
+
+int64_t rmd_debug_kernel_launches(const rmd_sim *sim) { return sim ? sim->engine.kernel_launches : 0; }
+
+rmd_status rmd_debug_set_nonbonded_lanes(rmd_sim *sim, int32_t lanes) {
+  if (!sim || (lanes != 8 && lanes != 16 && lanes != 32)) return RMD_ERR_INVALID;
+  auto &e = sim->engine;
+  e.nb_lanes = lanes;
+  for (auto &kv : e.graphs) cudaGraphExecDestroy(kv.second);
+  e.graphs.clear();
+  e.graph_launches.clear();
+  return RMD_OK;
+}
+
+rmd_status rmd_debug_fft(rmd_sim *sim, int32_t s, const double *data, double *half_spectrum, double *round_trip) {
+  if (rmd_status c = check_index(sim, s)) return c;
+  return guarded(sim, [&]() {
+    auto &e = sim->engine;
+    const auto &h = e.hs[s];
+    const auto &ds = e.h_sys[s];
+    const int nx = h.grid[0], ny = h.grid[1], nz = h.grid[2], nzh = nz / 2 + 1;
+    const size_t pts = (size_t)nx * ny * nz, hp = (size_t)nx * ny * nzh;
+    e.sync();
+    std::vector<long long> fx(pts);
+    for (size_t k = 0; k < pts; ++k) fx[k] = (long long)std::llround(data[k] * rmd::FORCE_SCALE);
+    CUDA_OK(cudaMemset(e.fixed_grid.p, 0, e.fixed_grid.bytes()));
+    CUDA_OK(cudaMemcpy(e.fixed_grid.p + ds.grid_base, fx.data(), sizeof(long long) * pts, cudaMemcpyHostToDevice));
+    const rmd::LaunchCtx c = e.ctx();
+    rmd::launch_fft_forward(c, e.stream);
+    e.sync();
+    std::vector<float2> hs_(hp);
+    CUDA_OK(cudaMemcpy(hs_.data(), e.half.p + ds.half_base, sizeof(float2) * hp, cudaMemcpyDeviceToHost));
+    for (size_t k = 0; k < hp; ++k) {
+      half_spectrum[2 * k] = hs_[k].x;
+      half_spectrum[2 * k + 1] = hs_[k].y;
+    }
+    rmd::launch_fft_inverse(c, e.stream);
+    e.sync();
+    std::vector<float> rg(pts);
+    CUDA_OK(cudaMemcpy(rg.data(), e.real_grid.p + ds.grid_base, sizeof(float) * pts, cudaMemcpyDeviceToHost));
+    for (size_t k = 0; k < pts; ++k) round_trip[k] = rg[k];
+  });
+}
+
+}  // extern "C"

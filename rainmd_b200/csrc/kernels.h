@@ -1,0 +1,180 @@
+// Launch interface between the host engine (engine.cu) and the kernels.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+
+namespace rmd {
+
+// One FFT axis of one system: length, Stockham radices and its twiddle table offset.
+struct FftAxis {
+  int n;
+  int nstages;
+  int radix[12];
+  int tw_base;
+};
+struct FftPlan {
+  FftAxis axis[3];
+};
+// A block's share of an FFT pass: lines [first, first+count) of system `sys`; `fixed` is
+// the other fixed index (x for the y pass, y for the x pass).
+struct FftTask {
+  int sys, fixed, first, count;
+};
+
+// Integrator parameters per system (integrate.js:39-63 `Integrator`).
+struct DevInteg {
+  float half_step, decay, noise_scale, kT;
+  float tolerance;
+  uint32_t seed;
+  int max_iterations;
+  int supplied_noise;
+};
+
+// SETTLE geometry of one water (masses and the canonical triangle).
+struct DevSettle {
+  float m_o, m_h, ra, rb, rc, d_oh, d_hh, pad;
+};
+
+enum IntegrateMode {
+  INT_OPEN = 1,          // B R A S O R A S
+  INT_CLOSE = 2,         // B R (the closing half kick of the previous step)
+  INT_OPEN_KINETIC = 4,  // per-atom kinetic energy after the opening part
+  INT_CLOSE_KINETIC = 8, // per-atom kinetic energy after the closing part
+  INT_CONSTRAIN = 16     // positions only: SHAKE/SETTLE towards saved_posq (minimiser)
+};
+
+struct IntegrateArgs {
+  int n_units, n_free, n_clusters, n_settle, n_atoms, n_systems;
+  const int *free_atoms;
+  const int *cl_atom_start, *cl_atoms, *cl_con_start;
+  const int2 *cl_con_pair;
+  const float *cl_con_dist;
+  const int3 *settle_atoms;
+  const DevSettle *settle_param;
+  const int *sys_of_atom;
+  const int *sys_atom_start;
+  const DevInteg *integ;
+  const long long *step_base;
+  int step_offset;
+  float4 *posq;
+  float4 *vel;
+  const unsigned long long *force;
+  const float *noise;
+  const float4 *origin;
+  unsigned *disp;  // [n_systems] since the last rebuild, then [n_systems] since block start
+  int *diag;
+  double *ke_post, *ke_early;
+  const float4 *saved_posq;
+};
+
+struct LaunchCtx {
+  int n_atoms, n_systems;
+  float4 *posq;
+  const int *atom_type;
+  const int *sys_of_atom;
+  DevSys *sys;
+  DevSysD *sysd;
+  // lists
+  int *cell_of_atom, *cell_count, *cell_start, *cell_atoms, *cell_sys;
+  int n_cells_total;
+  const int *excl_start, *excl_partners;
+  int *nbr, *nbr_count, *required;
+  float4 *origin;
+  // nonbonded
+  const float2 *lj;
+  const int *exc_start, *exc_partner;
+  const float4 *exc_param;
+  unsigned long long *force;
+  double *e_lj, *e_coul;
+  // bonded
+  const int2 *bond_atoms;
+  const float2 *bond_param;
+  int n_bonds;
+  const int4 *angle_atoms;
+  const float2 *angle_param;
+  int n_angles;
+  const int4 *tor_atoms;
+  const float4 *tor_param;
+  int n_tors;
+  const int *rest_atom;
+  const float4 *rest_param;
+  int n_rest;
+  double *e_term;
+  // pme
+  int pme_on, pme_order;
+  unsigned long long *fixed_grid;
+  float2 *half;
+  float *real_grid;
+  const float *moduli;
+  const float2 *twiddles;
+  const FftPlan *fft_plans;
+  const FftTask *tasks_z, *tasks_y, *tasks_x;
+  int n_tasks_z, n_tasks_y, n_tasks_x;
+  double *e_pme;
+};
+
+void launch_rebuild(const LaunchCtx &c, cudaStream_t stream);
+void launch_nonbonded(const LaunchCtx &c, bool energy, int lanes, cudaStream_t stream);
+void launch_bonded(const LaunchCtx &c, bool energy, cudaStream_t stream);
+void launch_pme(const LaunchCtx &c, bool energy, cudaStream_t stream);
+void launch_fft_forward(const LaunchCtx &c, cudaStream_t stream);
+void launch_spread_only(const LaunchCtx &c, cudaStream_t stream);
+void launch_fft_inverse(const LaunchCtx &c, cudaStream_t stream);
+void launch_integrate(const IntegrateArgs &a, int mode, cudaStream_t stream);
+
+// Energy segments reduced per system (reduce.cu). Each segment is [start, end) of one
+// per-item FP64 array; the result lands in energies[sys * N_ENERGY + term].
+enum EnergyTerm {
+  E_BOND = 0, E_ANGLE, E_TORSION, E_LJ, E_COUL_DIRECT, E_RECIP, E_RESTRAINT, E_KINETIC,
+  E_KINETIC_EARLY, E_SELF, E_NET, E_DISPERSION, E_POTENTIAL, N_ENERGY
+};
+struct Segment {
+  int sys, term;
+  const double *data;
+  long long start, end;
+  const double *data2;  // optional second array summed over the same range (LJ: nonbonded)
+};
+void launch_energy_reduce(const Segment *segments, int n_segments, double *seg_out,
+                          double *energies, const DevSysD *sysd, int n_systems, cudaStream_t stream);
+
+// Barostat and utility kernels (reduce.cu).
+struct BaroArgs {
+  int n_systems, n_atoms, n_molecules;
+  float4 *posq;
+  float4 *saved_posq;
+  unsigned long long *force, *saved_force;
+  const int *mol_start, *mol_atoms, *mol_of_atom;
+  const int *sys_of_atom;
+  float4 *centroid;  // per molecule
+  DevSys *sys;
+  DevSysD *sysd;
+  double *baro;      // per system BARO_* slots
+  double *energies;  // per system N_ENERGY
+  double *saved_energies;
+  const float *masses;
+};
+enum BaroSlot {
+  B_ACTIVE = 0, B_PRESSURE, B_KT, B_NMOL, B_SEED, B_ATTEMPTS, B_ACCEPTED, B_WINDOW_ATT, B_WINDOW_ACC,
+  B_SCALE, B_DV, B_LSCALE, B_OLD_E, B_NEW_E, B_WEIGHT, B_ACCEPT, B_REFUSED, B_REFUSALS,
+  B_OLD_VOL, B_MAX_SHRINK, B_MIN_LIST_WIDTH, B_SCREENED, B_SCREENED_TOTAL, B_EXACT_EVALS,
+  B_PRED, B_PRED_REV, B_FEATURE0, B_LEARNED, B_VOL_REF, N_BARO = 48
+};
+void launch_baro_propose(const BaroArgs &a, cudaStream_t stream);
+void launch_baro_scale(const BaroArgs &a, cudaStream_t stream);
+void launch_baro_decide(const BaroArgs &a, cudaStream_t stream);
+void launch_baro_restore(const BaroArgs &a, cudaStream_t stream);
+void launch_scale_fixed(const BaroArgs &a, const double *scales, cudaStream_t stream);
+void launch_update_box(DevSys *sys, DevSysD *sysd, int n_systems, cudaStream_t stream);
+void launch_advance_steps(long long *step_base, int n_systems, int count, cudaStream_t stream);
+
+// Minimiser helpers (minimise.cu): largest force magnitude per system (as float bits), and
+// x += scale_s * F capped at max_disp per atom (integrate.js:589-666).
+void launch_max_force(const unsigned long long *force, const int *sys_of_atom, int n_atoms,
+                      unsigned *out_bits, cudaStream_t stream);
+void launch_displace(float4 *posq, const unsigned long long *force, const int *sys_of_atom, int n_atoms,
+                     const float *scale, float max_disp, cudaStream_t stream);
+
+}  // namespace rmd

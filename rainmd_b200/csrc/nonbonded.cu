@@ -1,0 +1,277 @@
+// Direct-space Lennard-Jones + Ewald-screened Coulomb over the neighbour list, fused with
+// the exception pass (1-4 pairs and the erf correction of every excluded pair).
+//
+// Physics as RainMD's nonbonded.js:30-200 / cpu/forces/nonbonded.js:24-162: a full
+// (both-direction) list, so each atom's force is a gather and needs no atomics; energies
+// are halved because each pair is seen from both atoms; the screened-Coulomb force carries
+// the Gaussian term 2a exp(-a^2 r^2)/sqrt(pi); exceptions have no cutoff and the erf
+// correction uses the atoms' full charges.
+//
+// B200 shape: LANES lanes per atom (32 = one warp; 16 or 8 = 2 or 4 atoms per warp, chosen
+// by the autotuner). Lanes stride the atom's neighbour row, so the row read is coalesced
+// and the j positions (float4 x,y,z,q) are gathered through L1. exp(-z^2) is computed
+// once per pair and shared by erfc and the Gaussian. Per-lane partial forces are converted
+// to 64-bit fixed point and reduced with integer shuffles, so the sum is exact and
+// order-independent; lane 0 stores the atom's force (this kernel is the first writer of
+// the force array in every evaluation). Energies are only computed in the ENERGY variant.
+#include "common.cuh"
+#include "kernels.h"
+
+namespace rmd {
+
+template <int LANES>
+__device__ __forceinline__ long long group_sum(long long v) {
+#pragma unroll
+  for (int o = LANES / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+template <int LANES>
+__device__ __forceinline__ double group_sum(double v) {
+#pragma unroll
+  for (int o = LANES / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+template <bool ENERGY, int LANES>
+__global__ void __launch_bounds__(128) k_nonbonded(
+    const float4 *__restrict__ posq, const int *__restrict__ atom_type,
+    const int *__restrict__ sys_of_atom, const DevSys *__restrict__ sys,
+    const float2 *__restrict__ lj, const int *__restrict__ nbr, const int *__restrict__ nbr_count,
+    const int *__restrict__ exc_start, const int *__restrict__ exc_partner,
+    const float4 *__restrict__ exc_param, unsigned long long *__restrict__ force,
+    double *__restrict__ e_lj, double *__restrict__ e_coul, int n_atoms) {
+  const int gid = blockIdx.x * blockDim.x + threadIdx.x;
+  // A warp may hold a group past the last atom (LANES < 32): it works on a clamped atom
+  // with an empty row and stores nothing, so every lane reaches the shuffles.
+  const bool valid = gid / LANES < n_atoms;
+  if (!valid && LANES == 32) return;
+  const int i = valid ? gid / LANES : n_atoms - 1;
+  const int lane = gid % LANES;
+  const DevSys &s = sys[sys_of_atom[i]];
+  const float4 pi = posq[i];
+  const float qik = (float)ONE_4PI_EPS0 * pi.w;
+  const int ti = atom_type[i];
+  const float2 *ljrow = lj + s.lj_base + ti * s.type_count;
+  const float alpha = s.alpha;
+  const float gauss_k = 2.0f * alpha * 0.5641895835477563f;  // 2a/sqrt(pi)
+  const float cut2 = s.cutoff2;
+  const int count = valid ? nbr_count[i] : 0;
+  const int *row = nbr + s.nbr_base + (long long)(i - s.atom_start) * s.nbr_capacity;
+
+  float fx = 0.f, fy = 0.f, fz = 0.f, elj = 0.f, ecoul = 0.f;
+  for (int k = lane; k < count; k += LANES) {
+    const int j = __ldg(row + k);
+    const float4 pj = __ldg(posq + j);
+    float3 d = min_image(make_float3(pi.x - pj.x, pi.y - pj.y, pi.z - pj.z), s);
+    const float r2 = fmaf(d.x, d.x, fmaf(d.y, d.y, d.z * d.z));
+    if (r2 <= cut2) {
+      const float inv_r = rsqrtf(r2);
+      const float inv_r2 = inv_r * inv_r;
+      const float inv_r6 = inv_r2 * inv_r2 * inv_r2;
+      const float2 ab = __ldg(ljrow + __ldg(atom_type + j));
+      const float a12 = ab.x * inv_r6 * inv_r6, b6 = ab.y * inv_r6;
+      float scalar = (12.0f * a12 - 6.0f * b6) * inv_r2;
+      const float qq = qik * pj.w;
+      const float r = r2 * inv_r;
+      float gauss;
+      const float screened = erfc_and_gauss(alpha * r, gauss);
+      scalar = fmaf(qq * fmaf(screened, inv_r, gauss_k * gauss), inv_r2, scalar);
+      fx = fmaf(scalar, d.x, fx);
+      fy = fmaf(scalar, d.y, fy);
+      fz = fmaf(scalar, d.z, fz);
+      if (ENERGY) {
+        elj += a12 - b6;
+        ecoul = fmaf(qq * screened, inv_r, ecoul);
+      }
+    }
+  }
+  // Exceptions: 1-4 scaled LJ/Coulomb and -q_i q_j erf(a r)/r, no cutoff.
+  const int eb = exc_start[i], ee = valid ? exc_start[i + 1] : eb;
+  for (int e = eb + lane; e < ee; e += LANES) {
+    const int j = exc_partner[e];
+    const float4 prm = exc_param[e];  // chargeProduct, ljA, ljB, fullProduct
+    const float4 pj = posq[j];
+    float3 d = min_image(make_float3(pi.x - pj.x, pi.y - pj.y, pi.z - pj.z), s);
+    const float r2 = fmaf(d.x, d.x, fmaf(d.y, d.y, d.z * d.z));
+    const float inv_r = rsqrtf(r2);
+    const float inv_r2 = inv_r * inv_r, inv_r6 = inv_r2 * inv_r2 * inv_r2;
+    float scalar = 0.f;
+    if (prm.y != 0.f || prm.z != 0.f) {
+      const float a12 = prm.y * inv_r6 * inv_r6, b6 = prm.z * inv_r6;
+      scalar += (12.0f * a12 - 6.0f * b6) * inv_r2;
+      if (ENERGY) elj += a12 - b6;
+    }
+    if (prm.x != 0.f) {
+      const float qq = (float)ONE_4PI_EPS0 * prm.x;
+      scalar += qq * inv_r * inv_r2;
+      if (ENERGY) ecoul += qq * inv_r;
+    }
+    if (alpha > 0.f && prm.w != 0.f) {
+      const float qq = (float)ONE_4PI_EPS0 * prm.w;
+      float gauss;
+      const float r = r2 * inv_r;
+      const float unscreened = 1.0f - erfc_and_gauss(alpha * r, gauss);
+      scalar -= qq * (unscreened * inv_r - gauss_k * gauss) * inv_r2;
+      if (ENERGY) ecoul -= qq * unscreened * inv_r;
+    }
+    fx = fmaf(scalar, d.x, fx);
+    fy = fmaf(scalar, d.y, fy);
+    fz = fmaf(scalar, d.z, fz);
+  }
+  const long long gx = group_sum<LANES>((long long)to_fixed(fx));
+  const long long gy = group_sum<LANES>((long long)to_fixed(fy));
+  const long long gz = group_sum<LANES>((long long)to_fixed(fz));
+  double dl = 0, dc = 0;
+  if (ENERGY) {
+    dl = group_sum<LANES>((double)elj);
+    dc = group_sum<LANES>((double)ecoul);
+  }
+  if (lane == 0 && valid) {
+    force[i] = (unsigned long long)gx;
+    force[n_atoms + i] = (unsigned long long)gy;
+    force[2 * (long long)n_atoms + i] = (unsigned long long)gz;
+    if (ENERGY) {
+      e_lj[i] = 0.5 * dl;
+      e_coul[i] = 0.5 * dc;
+    }
+  }
+}
+
+template <bool ENERGY, int LANES>
+static void launch_nb(const LaunchCtx &c, cudaStream_t stream) {
+  const int threads = 128;
+  const long long total = (long long)c.n_atoms * LANES;
+  const int blocks = (int)((total + threads - 1) / threads);
+  k_nonbonded<ENERGY, LANES><<<blocks, threads, 0, stream>>>(
+      c.posq, c.atom_type, c.sys_of_atom, c.sys, c.lj, c.nbr, c.nbr_count, c.exc_start,
+      c.exc_partner, c.exc_param, c.force, c.e_lj, c.e_coul, c.n_atoms);
+}
+
+void launch_nonbonded(const LaunchCtx &c, bool energy, int lanes, cudaStream_t stream) {
+  if (energy) {
+    if (lanes == 8) launch_nb<true, 8>(c, stream);
+    else if (lanes == 16) launch_nb<true, 16>(c, stream);
+    else launch_nb<true, 32>(c, stream);
+  } else {
+    if (lanes == 8) launch_nb<false, 8>(c, stream);
+    else if (lanes == 16) launch_nb<false, 16>(c, stream);
+    else launch_nb<false, 32>(c, stream);
+  }
+}
+
+// ------------------------------------------------------------------ bonded + restraints
+// One thread per term (bonds | angles | torsions | restraints); forces are added to the
+// fixed-point array with 64-bit integer atomics (order-independent, deterministic).
+// Functional forms as cpu/forces/bonded.js:22-207 and shared/topology/restraints.js:93-126.
+template <bool ENERGY>
+__global__ void k_bonded(const float4 *__restrict__ posq, const int *__restrict__ sys_of_atom,
+                         const DevSys *__restrict__ sys, const int2 *__restrict__ bond_atoms,
+                         const float2 *__restrict__ bond_param, int n_bonds,
+                         const int4 *__restrict__ angle_atoms, const float2 *__restrict__ angle_param,
+                         int n_angles, const int4 *__restrict__ tor_atoms,
+                         const float4 *__restrict__ tor_param, int n_tors,
+                         const int *__restrict__ rest_atom, const float4 *__restrict__ rest_param,
+                         int n_rest, unsigned long long *__restrict__ force,
+                         double *__restrict__ e_term, int n_atoms) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned long long *fxp = force, *fyp = force + n_atoms, *fzp = force + 2 * (long long)n_atoms;
+  const int total = n_bonds + n_angles + n_tors + n_rest;
+  if (t >= total) return;
+  float energy = 0.f;
+  if (t < n_bonds) {
+    const int2 a = bond_atoms[t];
+    const float2 p = bond_param[t];
+    const float4 A = posq[a.x], B = posq[a.y];
+    const float dx = A.x - B.x, dy = A.y - B.y, dz = A.z - B.z;
+    const float r = sqrtf(dx * dx + dy * dy + dz * dz);
+    const float stretch = r - p.y;
+    energy = 0.5f * p.x * stretch * stretch;
+    const float sc = r > 0.f ? p.x * stretch / r : 0.f;
+    add_fixed(fxp + a.x, -sc * dx); add_fixed(fyp + a.x, -sc * dy); add_fixed(fzp + a.x, -sc * dz);
+    add_fixed(fxp + a.y, sc * dx); add_fixed(fyp + a.y, sc * dy); add_fixed(fzp + a.y, sc * dz);
+  } else if ((t -= n_bonds) < n_angles) {
+    const int4 a = angle_atoms[t];
+    const float2 p = angle_param[t];
+    const float4 A = posq[a.x], B = posq[a.y], Cc = posq[a.z];
+    const float v1x = A.x - B.x, v1y = A.y - B.y, v1z = A.z - B.z;
+    const float v2x = Cc.x - B.x, v2y = Cc.y - B.y, v2z = Cc.z - B.z;
+    const float n1 = v1x * v1x + v1y * v1y + v1z * v1z, n2 = v2x * v2x + v2y * v2y + v2z * v2z;
+    const float nx = v1y * v2z - v1z * v2y, ny = v1z * v2x - v1x * v2z, nz = v1x * v2y - v1y * v2x;
+    const float cm = sqrtf(nx * nx + ny * ny + nz * nz);
+    const float dot = v1x * v2x + v1y * v2y + v1z * v2z;
+    const float theta = atan2f(cm, dot), dev = theta - p.y;
+    energy = 0.5f * p.x * dev * dev;
+    const float dE = p.x * dev, safe = fmaxf(cm, 1e-12f);
+    const float s1 = -dE / (n1 * safe), s2 = dE / (n2 * safe);
+    const float fax = s1 * (v1y * nz - v1z * ny), fay = s1 * (v1z * nx - v1x * nz), faz = s1 * (v1x * ny - v1y * nx);
+    const float fcx = s2 * (v2y * nz - v2z * ny), fcy = s2 * (v2z * nx - v2x * nz), fcz = s2 * (v2x * ny - v2y * nx);
+    add_fixed(fxp + a.x, fax); add_fixed(fyp + a.x, fay); add_fixed(fzp + a.x, faz);
+    add_fixed(fxp + a.z, fcx); add_fixed(fyp + a.z, fcy); add_fixed(fzp + a.z, fcz);
+    add_fixed(fxp + a.y, -(fax + fcx)); add_fixed(fyp + a.y, -(fay + fcy)); add_fixed(fzp + a.y, -(faz + fcz));
+  } else if ((t -= n_angles) < n_tors) {
+    const int4 a = tor_atoms[t];
+    const float4 p = tor_param[t];  // k, n, phase
+    const float4 A = posq[a.x], B = posq[a.y], Cc = posq[a.z], D = posq[a.w];
+    const float b1x = B.x - A.x, b1y = B.y - A.y, b1z = B.z - A.z;
+    const float b2x = Cc.x - B.x, b2y = Cc.y - B.y, b2z = Cc.z - B.z;
+    const float b3x = D.x - Cc.x, b3y = D.y - Cc.y, b3z = D.z - Cc.z;
+    const float n1x = b1y * b2z - b1z * b2y, n1y = b1z * b2x - b1x * b2z, n1z = b1x * b2y - b1y * b2x;
+    const float n2x = b2y * b3z - b2z * b3y, n2y = b2z * b3x - b2x * b3z, n2z = b2x * b3y - b2y * b3x;
+    const float n1s = n1x * n1x + n1y * n1y + n1z * n1z, n2s = n2x * n2x + n2y * n2y + n2z * n2z;
+    const float b2l = sqrtf(b2x * b2x + b2y * b2y + b2z * b2z);
+    if (!(n1s < 1e-24f || n2s < 1e-24f || b2l < 1e-12f)) {
+      const float dn = n1x * n2x + n1y * n2y + n1z * n2z;
+      const float cdb = (n1y * n2z - n1z * n2y) * b2x + (n1z * n2x - n1x * n2z) * b2y +
+                        (n1x * n2y - n1y * n2x) * b2z;
+      const float phi = atan2f(cdb / b2l, dn);
+      const float arg = p.y * phi - p.z;
+      float sa, ca;
+      sincosf(arg, &sa, &ca);
+      energy = p.x * (1.0f + ca);
+      const float dEdphi = -p.x * p.y * sa;
+      const float fA = dEdphi * b2l / n1s, fD = -dEdphi * b2l / n2s;
+      const float inv = 1.0f / (b2l * b2l);
+      const float tt = (b1x * b2x + b1y * b2y + b1z * b2z) * inv;
+      const float uu = (b3x * b2x + b3y * b2y + b3z * b2z) * inv;
+      const float fax = fA * n1x, fay = fA * n1y, faz = fA * n1z;
+      const float fdx = fD * n2x, fdy = fD * n2y, fdz = fD * n2z;
+      add_fixed(fxp + a.x, fax); add_fixed(fyp + a.x, fay); add_fixed(fzp + a.x, faz);
+      add_fixed(fxp + a.w, fdx); add_fixed(fyp + a.w, fdy); add_fixed(fzp + a.w, fdz);
+      add_fixed(fxp + a.y, -(1.f + tt) * fax + uu * fdx);
+      add_fixed(fyp + a.y, -(1.f + tt) * fay + uu * fdy);
+      add_fixed(fzp + a.y, -(1.f + tt) * faz + uu * fdz);
+      add_fixed(fxp + a.z, tt * fax - (1.f + uu) * fdx);
+      add_fixed(fyp + a.z, tt * fay - (1.f + uu) * fdy);
+      add_fixed(fzp + a.z, tt * faz - (1.f + uu) * fdz);
+    }
+  } else {
+    t -= n_tors;
+    const int atom = rest_atom[t];
+    const float4 p = rest_param[t];  // reference x, y, z, k
+    const DevSys &s = sys[sys_of_atom[atom]];
+    const float4 A = posq[atom];
+    float3 d = min_image(make_float3(A.x - p.x, A.y - p.y, A.z - p.z), s);
+    energy = p.w * (d.x * d.x + d.y * d.y + d.z * d.z);
+    const float sc = -2.0f * p.w;
+    add_fixed(fxp + atom, sc * d.x); add_fixed(fyp + atom, sc * d.y); add_fixed(fzp + atom, sc * d.z);
+  }
+  if (ENERGY) e_term[blockIdx.x * blockDim.x + threadIdx.x] = (double)energy;
+}
+
+void launch_bonded(const LaunchCtx &c, bool energy, cudaStream_t stream) {
+  const int total = c.n_bonds + c.n_angles + c.n_tors + c.n_rest;
+  if (total == 0) return;
+  const int tb = 128;
+  if (energy)
+    k_bonded<true><<<(total + tb - 1) / tb, tb, 0, stream>>>(
+        c.posq, c.sys_of_atom, c.sys, c.bond_atoms, c.bond_param, c.n_bonds, c.angle_atoms,
+        c.angle_param, c.n_angles, c.tor_atoms, c.tor_param, c.n_tors, c.rest_atom, c.rest_param,
+        c.n_rest, c.force, c.e_term, c.n_atoms);
+  else
+    k_bonded<false><<<(total + tb - 1) / tb, tb, 0, stream>>>(
+        c.posq, c.sys_of_atom, c.sys, c.bond_atoms, c.bond_param, c.n_bonds, c.angle_atoms,
+        c.angle_param, c.n_angles, c.tor_atoms, c.tor_param, c.n_tors, c.rest_atom, c.rest_param,
+        c.n_rest, c.force, c.e_term, c.n_atoms);
+}
+
+}  // namespace rmd

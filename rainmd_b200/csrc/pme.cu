@@ -1,0 +1,466 @@
+// Particle-mesh Ewald reciprocal space for a batch of systems.
+//
+// Same mathematics and conventions as RainMD's pme.js:137-345 / cpu/forces/pme.js:76-259:
+// B-spline spreading with grid index (floor(u) + k - order + 1) mod K, signed frequencies,
+// wave vectors from the ROWS of the inverse box, moduli dividing the kernel, the factor 2
+// folded into the convolved grid, an unnormalised inverse transform, and no 1/2 in the
+// force gather. The spline order is a template parameter (4 or 5).
+//
+// B200 design (not the reference's pass structure):
+//   spread   one thread per atom, 64-bit fixed-point integer atomics (deterministic);
+//   z pass   R2C: two real z-lines packed as one complex line, FFT in shared memory,
+//            split into two half spectra; also converts fixed point -> f32 and zeroes the
+//            fixed grid for the next step (no separate clear/convert kernels);
+//   y pass   complex FFT along y on the half spectrum, in place;
+//   x pass   forward FFT along x, the Ewald convolution and the FP64 energy partial, and
+//            the inverse FFT along x, all while the lines are in shared memory;
+//   y pass   inverse; z pass C2R back to a real f32 grid; gather one thread per atom.
+// The FFT is a mixed-radix (4, 2, 3, 5) Stockham autosort over lines held in shared
+// memory; a host-built task table gives each block a set of lines of one system, so
+// systems with different grid sizes run in the same launch.
+#include "common.cuh"
+#include "kernels.h"
+
+namespace rmd {
+
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+// multiply by -i (forward) or +i (inverse)
+__device__ __forceinline__ float2 rot(float2 a, bool inverse) {
+  return inverse ? make_float2(-a.y, a.x) : make_float2(a.y, -a.x);
+}
+
+template <int R>
+__device__ __forceinline__ void dft_small(float2 *v, bool inv) {
+  if (R == 2) {
+    float2 a = v[0], b = v[1];
+    v[0] = cadd(a, b);
+    v[1] = csub(a, b);
+  } else if (R == 4) {
+    float2 a0 = cadd(v[0], v[2]), a1 = csub(v[0], v[2]);
+    float2 a2 = cadd(v[1], v[3]), a3 = rot(csub(v[1], v[3]), inv);
+    v[0] = cadd(a0, a2);
+    v[2] = csub(a0, a2);
+    v[1] = cadd(a1, a3);
+    v[3] = csub(a1, a3);
+  } else if (R == 3) {
+    const float h = 0.86602540378443864676f;  // sqrt(3)/2
+    float2 t1 = cadd(v[1], v[2]), t2 = csub(v[1], v[2]);
+    float2 b = make_float2(v[0].x - 0.5f * t1.x, v[0].y - 0.5f * t1.y);
+    float2 r = rot(make_float2(h * t2.x, h * t2.y), inv);  // -i*h*t2 forward
+    v[0] = cadd(v[0], t1);
+    v[1] = cadd(b, r);
+    v[2] = csub(b, r);
+  } else if (R == 5) {
+    const float c1 = 0.30901699437494742410f, c2 = -0.80901699437494742410f;
+    const float s1 = 0.95105651629515357212f, s2 = 0.58778525229247312917f;
+    float2 t1 = cadd(v[1], v[4]), t2 = cadd(v[2], v[3]);
+    float2 t3 = csub(v[1], v[4]), t4 = csub(v[2], v[3]);
+    float2 b1 = make_float2(v[0].x + c1 * t1.x + c2 * t2.x, v[0].y + c1 * t1.y + c2 * t2.y);
+    float2 b2 = make_float2(v[0].x + c2 * t1.x + c1 * t2.x, v[0].y + c2 * t1.y + c1 * t2.y);
+    float2 q1 = rot(make_float2(s1 * t3.x + s2 * t4.x, s1 * t3.y + s2 * t4.y), inv);
+    float2 q2 = rot(make_float2(s2 * t3.x - s1 * t4.x, s2 * t3.y - s1 * t4.y), inv);
+    v[0] = cadd(v[0], cadd(t1, t2));
+    v[1] = cadd(b1, q1);
+    v[4] = csub(b1, q1);
+    v[2] = cadd(b2, q2);
+    v[3] = csub(b2, q2);
+  }
+}
+
+template <int R>
+__device__ __forceinline__ void stockham_stage(const float2 *__restrict__ in, float2 *__restrict__ out,
+                                               int lines, int N, int Ns, const float2 *__restrict__ tw,
+                                               bool inv) {
+  const int per_line = N / R;
+  const int stride_tw = N / (Ns * R);
+  for (int idx = threadIdx.x; idx < lines * per_line; idx += blockDim.x) {
+    const int line = idx / per_line, j = idx - line * per_line;
+    const float2 *src = in + line * N;
+    float2 v[R];
+    const int k = j % Ns;
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[r] = src[j + r * per_line];
+#pragma unroll
+    for (int r = 1; r < R; ++r) {
+      float2 w = tw[k * r * stride_tw];
+      if (inv) w.y = -w.y;
+      v[r] = cmul(v[r], w);
+    }
+    dft_small<R>(v, inv);
+    float2 *dst = out + line * N + (j / Ns) * Ns * R + k;
+#pragma unroll
+    for (int r = 0; r < R; ++r) dst[r * Ns] = v[r];
+  }
+}
+
+// Transform `lines` lines of length N held in a; returns the buffer holding the result.
+__device__ float2 *fft_lines(float2 *a, float2 *b, int lines, int N, const FftAxis &ax,
+                             const float2 *__restrict__ tw, bool inv) {
+  int Ns = 1;
+  for (int st = 0; st < ax.nstages; ++st) {
+    const int R = ax.radix[st];
+    __syncthreads();
+    if (R == 4) stockham_stage<4>(a, b, lines, N, Ns, tw, inv);
+    else if (R == 2) stockham_stage<2>(a, b, lines, N, Ns, tw, inv);
+    else if (R == 3) stockham_stage<3>(a, b, lines, N, Ns, tw, inv);
+    else stockham_stage<5>(a, b, lines, N, Ns, tw, inv);
+    Ns *= R;
+    float2 *t = a;
+    a = b;
+    b = t;
+  }
+  __syncthreads();
+  return a;
+}
+
+constexpr int FFT_SMEM = 2048;  // complex values per buffer per block
+
+// ------------------------------------------------------------------------ spreading
+template <int ORDER>
+__global__ void k_spread(const float4 *__restrict__ posq, const int *__restrict__ sys_of_atom,
+                         const DevSys *__restrict__ sys, unsigned long long *__restrict__ fixed_grid,
+                         int n_atoms) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_atoms) return;
+  const float4 p = posq[i];
+  if (p.w == 0.f) return;
+  const DevSys &s = sys[sys_of_atom[i]];
+  float w[3][ORDER], dw[3][ORDER];
+  int base[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const float f = p.x * s.recip[d] + p.y * s.recip[3 + d] + p.z * s.recip[6 + d];
+    const float scaled = (f - floorf(f)) * (float)s.grid[d];
+    const float fl = floorf(scaled);
+    base[d] = (int)fl;
+    bspline<ORDER>(scaled - fl, w[d], dw[d]);
+  }
+  const int nx = s.grid[0], ny = s.grid[1], nz = s.grid[2];
+  unsigned long long *g = fixed_grid + s.grid_base;
+#pragma unroll
+  for (int kx = 0; kx < ORDER; ++kx) {
+    const int ix = wrap_index(base[0] + kx - ORDER + 1, nx);
+    const float wx = p.w * w[0][kx];
+#pragma unroll
+    for (int ky = 0; ky < ORDER; ++ky) {
+      const int iy = wrap_index(base[1] + ky - ORDER + 1, ny);
+      const float wxy = wx * w[1][ky];
+      unsigned long long *rowp = g + ((long long)ix * ny + iy) * nz;
+#pragma unroll
+      for (int kz = 0; kz < ORDER; ++kz) {
+        const int iz = wrap_index(base[2] + kz - ORDER + 1, nz);
+        atomicAdd(rowp + iz, to_fixed(wxy * w[2][kz]));
+      }
+    }
+  }
+}
+
+// -------------------------------------------------------------- z pass, forward (R2C)
+__global__ void __launch_bounds__(256) k_fft_z_r2c(const FftTask *__restrict__ tasks,
+                                                   const DevSys *__restrict__ sys,
+                                                   const FftPlan *__restrict__ plans,
+                                                   const float2 *__restrict__ twiddles,
+                                                   unsigned long long *__restrict__ fixed_grid,
+                                                   float2 *__restrict__ half) {
+  __shared__ float2 bufa[FFT_SMEM], bufb[FFT_SMEM];
+  const FftTask t = tasks[blockIdx.x];
+  const DevSys &s = sys[t.sys];
+  const FftPlan &pl = plans[t.sys];
+  const int N = s.grid[2], nzh = N / 2 + 1;
+  const int nlines = s.grid[0] * s.grid[1];
+  const int M = t.count;
+  unsigned long long *g = fixed_grid + s.grid_base;
+  for (int idx = threadIdx.x; idx < M * N; idx += blockDim.x) {
+    const int p = idx / N, k = idx - p * N;
+    const int l = 2 * (t.first + p);
+    unsigned long long *ra = g + (long long)l * N + k;
+    float re = from_fixed(*ra);
+    *ra = 0ull;
+    float im = 0.f;
+    if (l + 1 < nlines) {
+      unsigned long long *rb = ra + N;
+      im = from_fixed(*rb);
+      *rb = 0ull;
+    }
+    bufa[idx] = make_float2(re, im);
+  }
+  float2 *r = fft_lines(bufa, bufb, M, N, pl.axis[2], twiddles + pl.axis[2].tw_base, false);
+  float2 *h = half + s.half_base;
+  for (int idx = threadIdx.x; idx < M * nzh; idx += blockDim.x) {
+    const int p = idx / nzh, k = idx - p * nzh;
+    const int l = 2 * (t.first + p);
+    const float2 z = r[p * N + k];
+    const float2 zc = r[p * N + (N - k) % N];
+    // A = (Z + conj(Zc))/2, B = -i (Z - conj(Zc))/2
+    const float2 a = make_float2(0.5f * (z.x + zc.x), 0.5f * (z.y - zc.y));
+    const float2 b = make_float2(0.5f * (z.y + zc.y), -0.5f * (z.x - zc.x));
+    h[(long long)l * nzh + k] = a;
+    if (l + 1 < nlines) h[(long long)(l + 1) * nzh + k] = b;
+  }
+}
+
+// -------------------------------------------------------------- z pass, inverse (C2R)
+__global__ void __launch_bounds__(256) k_fft_z_c2r(const FftTask *__restrict__ tasks,
+                                                   const DevSys *__restrict__ sys,
+                                                   const FftPlan *__restrict__ plans,
+                                                   const float2 *__restrict__ twiddles,
+                                                   const float2 *__restrict__ half,
+                                                   float *__restrict__ real_grid) {
+  __shared__ float2 bufa[FFT_SMEM], bufb[FFT_SMEM];
+  const FftTask t = tasks[blockIdx.x];
+  const DevSys &s = sys[t.sys];
+  const FftPlan &pl = plans[t.sys];
+  const int N = s.grid[2], nzh = N / 2 + 1;
+  const int nlines = s.grid[0] * s.grid[1];
+  const int M = t.count;
+  const float2 *h = half + s.half_base;
+  for (int idx = threadIdx.x; idx < M * N; idx += blockDim.x) {
+    const int p = idx / N, k = idx - p * N;
+    const int l = 2 * (t.first + p);
+    const bool has_b = l + 1 < nlines;
+    float2 a, b;
+    if (k < nzh) {
+      a = h[(long long)l * nzh + k];
+      b = has_b ? h[(long long)(l + 1) * nzh + k] : make_float2(0.f, 0.f);
+      if (k == 0 || 2 * k == N) {
+        a.y = 0.f;
+        b.y = 0.f;
+      }
+    } else {
+      a = h[(long long)l * nzh + (N - k)];
+      b = has_b ? h[(long long)(l + 1) * nzh + (N - k)] : make_float2(0.f, 0.f);
+      a.y = -a.y;
+      b.y = -b.y;
+    }
+    bufa[idx] = make_float2(a.x - b.y, a.y + b.x);  // A + iB
+  }
+  float2 *r = fft_lines(bufa, bufb, M, N, pl.axis[2], twiddles + pl.axis[2].tw_base, true);
+  float *g = real_grid + s.grid_base;
+  for (int idx = threadIdx.x; idx < M * N; idx += blockDim.x) {
+    const int p = idx / N, k = idx - p * N;
+    const int l = 2 * (t.first + p);
+    const float2 z = r[idx];
+    g[(long long)l * N + k] = z.x;
+    if (l + 1 < nlines) g[(long long)(l + 1) * N + k] = z.y;
+  }
+}
+
+// ------------------------------------------------------ y pass (either direction, in place)
+__global__ void __launch_bounds__(256) k_fft_y(const FftTask *__restrict__ tasks,
+                                               const DevSys *__restrict__ sys,
+                                               const FftPlan *__restrict__ plans,
+                                               const float2 *__restrict__ twiddles,
+                                               float2 *__restrict__ half, int inverse) {
+  __shared__ float2 bufa[FFT_SMEM], bufb[FFT_SMEM];
+  const FftTask t = tasks[blockIdx.x];
+  const DevSys &s = sys[t.sys];
+  const FftPlan &pl = plans[t.sys];
+  const int ny = s.grid[1], nzh = s.grid[2] / 2 + 1;
+  const int x = t.fixed, kz0 = t.first, M = t.count;
+  float2 *h = half + s.half_base + (long long)x * ny * nzh + kz0;
+  for (int idx = threadIdx.x; idx < ny * M; idx += blockDim.x) {
+    const int y = idx / M, m = idx - y * M;
+    bufa[m * ny + y] = h[(long long)y * nzh + m];
+  }
+  float2 *r = fft_lines(bufa, bufb, M, ny, pl.axis[1], twiddles + pl.axis[1].tw_base, inverse != 0);
+  for (int idx = threadIdx.x; idx < ny * M; idx += blockDim.x) {
+    const int y = idx / M, m = idx - y * M;
+    h[(long long)y * nzh + m] = r[m * ny + y];
+  }
+}
+
+// ------------------------------ x pass: forward FFT, Ewald convolution + energy, inverse
+template <bool ENERGY>
+__global__ void __launch_bounds__(256) k_fft_x_convolve(const FftTask *__restrict__ tasks,
+                                                        const DevSys *__restrict__ sys,
+                                                        const DevSysD *__restrict__ sysd,
+                                                        const FftPlan *__restrict__ plans,
+                                                        const float2 *__restrict__ twiddles,
+                                                        const float *__restrict__ moduli,
+                                                        float2 *__restrict__ half,
+                                                        double *__restrict__ e_pme) {
+  __shared__ float2 bufa[FFT_SMEM], bufb[FFT_SMEM];
+  __shared__ double red[256 / 32];
+  const FftTask t = tasks[blockIdx.x];
+  const DevSys &s = sys[t.sys];
+  const FftPlan &pl = plans[t.sys];
+  const int nx = s.grid[0], ny = s.grid[1], nz = s.grid[2], nzh = nz / 2 + 1;
+  const int y = t.fixed, kz0 = t.first, M = t.count;
+  const long long stride = (long long)ny * nzh;
+  float2 *h = half + s.half_base + (long long)y * nzh + kz0;
+  for (int idx = threadIdx.x; idx < nx * M; idx += blockDim.x) {
+    const int x = idx / M, m = idx - x * M;
+    bufa[m * nx + x] = h[x * stride + m];
+  }
+  float2 *r = fft_lines(bufa, bufb, M, nx, pl.axis[0], twiddles + pl.axis[0].tw_base, false);
+  const double volume = sysd[t.sys].volume;
+  const double alpha = sysd[t.sys].alpha;
+  const float factor = (float)(M_PI * M_PI / (alpha * alpha));
+  const float two_pref = (float)(2.0 * ONE_4PI_EPS0 / (2.0 * M_PI * volume));
+  const float *modx = moduli + s.moduli_base, *mody = modx + nx, *modz = mody + ny;
+  const int ky = y <= ny / 2 ? y : y - ny;
+  double energy = 0.0;
+  for (int idx = threadIdx.x; idx < nx * M; idx += blockDim.x) {
+    const int m = idx / nx, mx = idx - m * nx;
+    const int kz = kz0 + m;
+    const int kx = mx <= nx / 2 ? mx : mx - nx;
+    float2 v = r[idx];
+    if (kx == 0 && ky == 0 && kz == 0) {
+      r[idx] = make_float2(0.f, 0.f);
+      continue;
+    }
+    const float fx = (float)kx, fy = (float)ky, fz = (float)kz;
+    const float cx = fx * s.recip[0] + fy * s.recip[1] + fz * s.recip[2];
+    const float cy = fx * s.recip[3] + fy * s.recip[4] + fz * s.recip[5];
+    const float cz = fx * s.recip[6] + fy * s.recip[7] + fz * s.recip[8];
+    const float m2 = cx * cx + cy * cy + cz * cz;
+    const float kernel = __expf(-factor * m2) / (m2 * modx[mx] * mody[y] * modz[kz]);
+    if (ENERGY) {
+      const double weight = (kz == 0 || 2 * kz == nz) ? 1.0 : 2.0;
+      energy += weight * 0.5 * (double)two_pref * (double)kernel * ((double)v.x * v.x + (double)v.y * v.y);
+    }
+    const float sc = kernel * two_pref;
+    r[idx] = make_float2(v.x * sc, v.y * sc);
+  }
+  float2 *other = (r == bufa) ? bufb : bufa;
+  float2 *q = fft_lines(r, other, M, nx, pl.axis[0], twiddles + pl.axis[0].tw_base, true);
+  for (int idx = threadIdx.x; idx < nx * M; idx += blockDim.x) {
+    const int x = idx / M, m = idx - x * M;
+    h[x * stride + m] = q[m * nx + x];
+  }
+  if (ENERGY) {
+    energy = warp_sum(energy);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = energy;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double total = 0;
+      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) total += red[w];
+      e_pme[blockIdx.x] = total;
+    }
+  }
+}
+
+// ------------------------------------------------------------------------- gather
+template <int ORDER>
+__global__ void k_gather(const float4 *__restrict__ posq, const int *__restrict__ sys_of_atom,
+                         const DevSys *__restrict__ sys, const float *__restrict__ real_grid,
+                         unsigned long long *__restrict__ force, int n_atoms) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_atoms) return;
+  const float4 p = posq[i];
+  if (p.w == 0.f) return;
+  const DevSys &s = sys[sys_of_atom[i]];
+  float w[3][ORDER], dw[3][ORDER];
+  int base[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const float f = p.x * s.recip[d] + p.y * s.recip[3 + d] + p.z * s.recip[6 + d];
+    const float scaled = (f - floorf(f)) * (float)s.grid[d];
+    const float fl = floorf(scaled);
+    base[d] = (int)fl;
+    bspline<ORDER>(scaled - fl, w[d], dw[d]);
+  }
+  const int nx = s.grid[0], ny = s.grid[1], nz = s.grid[2];
+  const float *g = real_grid + s.grid_base;
+  float gu = 0.f, gv = 0.f, gw = 0.f;
+#pragma unroll
+  for (int kx = 0; kx < ORDER; ++kx) {
+    const int ix = wrap_index(base[0] + kx - ORDER + 1, nx);
+#pragma unroll
+    for (int ky = 0; ky < ORDER; ++ky) {
+      const int iy = wrap_index(base[1] + ky - ORDER + 1, ny);
+      const float *rowp = g + ((long long)ix * ny + iy) * nz;
+      const float wxy = w[0][kx] * w[1][ky], dxy = dw[0][kx] * w[1][ky], wdy = w[0][kx] * dw[1][ky];
+#pragma unroll
+      for (int kz = 0; kz < ORDER; ++kz) {
+        const int iz = wrap_index(base[2] + kz - ORDER + 1, nz);
+        const float v = __ldg(rowp + iz);
+        gu = fmaf(dxy * w[2][kz], v, gu);
+        gv = fmaf(wdy * w[2][kz], v, gv);
+        gw = fmaf(wxy * dw[2][kz], v, gw);
+      }
+    }
+  }
+  const float su = gu * (float)nx * p.w, sv = gv * (float)ny * p.w, sw = gw * (float)nz * p.w;
+  add_fixed(force + i, -(su * s.recip[0] + sv * s.recip[1] + sw * s.recip[2]));
+  add_fixed(force + n_atoms + i, -(su * s.recip[3] + sv * s.recip[4] + sw * s.recip[5]));
+  add_fixed(force + 2 * (long long)n_atoms + i, -(su * s.recip[6] + sv * s.recip[7] + sw * s.recip[8]));
+}
+
+void launch_pme(const LaunchCtx &c, bool energy, cudaStream_t stream) {
+  if (!c.pme_on) return;
+  const int n = c.n_atoms, tb = 128;
+  if (c.pme_order == 4)
+    k_spread<4><<<(n + tb - 1) / tb, tb, 0, stream>>>(c.posq, c.sys_of_atom, c.sys, c.fixed_grid, n);
+  else
+    k_spread<5><<<(n + tb - 1) / tb, tb, 0, stream>>>(c.posq, c.sys_of_atom, c.sys, c.fixed_grid, n);
+  k_fft_z_r2c<<<c.n_tasks_z, 256, 0, stream>>>(c.tasks_z, c.sys, c.fft_plans, c.twiddles,
+                                                c.fixed_grid, c.half);
+  k_fft_y<<<c.n_tasks_y, 256, 0, stream>>>(c.tasks_y, c.sys, c.fft_plans, c.twiddles, c.half, 0);
+  if (energy)
+    k_fft_x_convolve<true><<<c.n_tasks_x, 256, 0, stream>>>(c.tasks_x, c.sys, c.sysd, c.fft_plans,
+                                                            c.twiddles, c.moduli, c.half, c.e_pme);
+  else
+    k_fft_x_convolve<false><<<c.n_tasks_x, 256, 0, stream>>>(c.tasks_x, c.sys, c.sysd, c.fft_plans,
+                                                             c.twiddles, c.moduli, c.half, c.e_pme);
+  k_fft_y<<<c.n_tasks_y, 256, 0, stream>>>(c.tasks_y, c.sys, c.fft_plans, c.twiddles, c.half, 1);
+  k_fft_z_c2r<<<c.n_tasks_z, 256, 0, stream>>>(c.tasks_z, c.sys, c.fft_plans, c.twiddles, c.half,
+                                                c.real_grid);
+  if (c.pme_order == 4)
+    k_gather<4><<<(n + tb - 1) / tb, tb, 0, stream>>>(c.posq, c.sys_of_atom, c.sys, c.real_grid, c.force, n);
+  else
+    k_gather<5><<<(n + tb - 1) / tb, tb, 0, stream>>>(c.posq, c.sys_of_atom, c.sys, c.real_grid, c.force, n);
+}
+
+// Debug: forward R2C then C2R of a given real grid (already in real_grid as f32 values
+// converted to fixed point by the caller), without the convolution. Used to check the FFT
+// against a DFT.
+__global__ void k_fft_x_plain(const FftTask *__restrict__ tasks, const DevSys *__restrict__ sys,
+                              const FftPlan *__restrict__ plans, const float2 *__restrict__ twiddles,
+                              float2 *__restrict__ half, int inverse) {
+  __shared__ float2 bufa[FFT_SMEM], bufb[FFT_SMEM];
+  const FftTask t = tasks[blockIdx.x];
+  const DevSys &s = sys[t.sys];
+  const FftPlan &pl = plans[t.sys];
+  const int nx = s.grid[0], ny = s.grid[1], nzh = s.grid[2] / 2 + 1;
+  const int y = t.fixed, kz0 = t.first, M = t.count;
+  const long long stride = (long long)ny * nzh;
+  float2 *h = half + s.half_base + (long long)y * nzh + kz0;
+  for (int idx = threadIdx.x; idx < nx * M; idx += blockDim.x) {
+    const int x = idx / M, m = idx - x * M;
+    bufa[m * nx + x] = h[x * stride + m];
+  }
+  float2 *r = fft_lines(bufa, bufb, M, nx, pl.axis[0], twiddles + pl.axis[0].tw_base, inverse != 0);
+  for (int idx = threadIdx.x; idx < nx * M; idx += blockDim.x) {
+    const int x = idx / M, m = idx - x * M;
+    h[x * stride + m] = r[m * nx + x];
+  }
+}
+
+void launch_spread_only(const LaunchCtx &c, cudaStream_t stream) {
+  const int n = c.n_atoms, tb = 128;
+  if (c.pme_order == 4)
+    k_spread<4><<<(n + tb - 1) / tb, tb, 0, stream>>>(c.posq, c.sys_of_atom, c.sys, c.fixed_grid, n);
+  else
+    k_spread<5><<<(n + tb - 1) / tb, tb, 0, stream>>>(c.posq, c.sys_of_atom, c.sys, c.fixed_grid, n);
+}
+
+void launch_fft_forward(const LaunchCtx &c, cudaStream_t stream) {
+  k_fft_z_r2c<<<c.n_tasks_z, 256, 0, stream>>>(c.tasks_z, c.sys, c.fft_plans, c.twiddles,
+                                                c.fixed_grid, c.half);
+  k_fft_y<<<c.n_tasks_y, 256, 0, stream>>>(c.tasks_y, c.sys, c.fft_plans, c.twiddles, c.half, 0);
+  k_fft_x_plain<<<c.n_tasks_x, 256, 0, stream>>>(c.tasks_x, c.sys, c.fft_plans, c.twiddles, c.half, 0);
+}
+
+void launch_fft_inverse(const LaunchCtx &c, cudaStream_t stream) {
+  k_fft_x_plain<<<c.n_tasks_x, 256, 0, stream>>>(c.tasks_x, c.sys, c.fft_plans, c.twiddles, c.half, 1);
+  k_fft_y<<<c.n_tasks_y, 256, 0, stream>>>(c.tasks_y, c.sys, c.fft_plans, c.twiddles, c.half, 1);
+  k_fft_z_c2r<<<c.n_tasks_z, 256, 0, stream>>>(c.tasks_z, c.sys, c.fft_plans, c.twiddles, c.half,
+                                                c.real_grid);
+}
+
+}  // namespace rmd
