@@ -183,6 +183,14 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def aggregate(device_ms: float, steps: int, world: int, reduce_max=None):
+    """Replica timing: the slowest rank's device time sets the time; every rank's
+    simulated nanoseconds count. Returns (value ns/day, seconds per step)."""
+    slowest = reduce_max(device_ms) if reduce_max is not None else device_ms
+    seconds_per_step = slowest / 1e3 / steps
+    return world * ns_per_day(seconds_per_step), seconds_per_step
+
+
 def ns_to_ms(value_ns_day):
     return TIMESTEP_PS * 1e-3 * 86400.0 / value_ns_day * 1e3
 
@@ -249,12 +257,13 @@ def main():
         device_ms = sim.benchRun(args.steps, block, flushL2=True)
     barrier()
     launches = sim.kernelLaunches() - launches0
-    ms = torch.tensor([device_ms], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(ms, op=dist.ReduceOp.MAX)
-    device_ms = float(ms.item())
-    seconds_per_step = device_ms / 1e3 / args.steps
-    value = world * ns_per_day(seconds_per_step)
+    def reduce_max(x):
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        if world > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    value, seconds_per_step = aggregate(device_ms, args.steps, world, reduce_max)
 
     # energies stay finite and the run was physical
     e = sim.energy()

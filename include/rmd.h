@@ -100,6 +100,9 @@ typedef struct {
   int32_t pme_order;            /* B-spline order, 4 or 5; default 5 (the reference's PME_ORDER) */
   int32_t water_solver;         /* 0 = SHAKE/RATTLE per cluster (reference); 1 = SETTLE for rigid 3-site water */
   int32_t learned_barostat;     /* 0 = exact Metropolis test; 1 = two-stage delayed acceptance with the MLP */
+  int32_t force_accumulation;   /* 0 = each pair force quantised to 64-bit fixed point before summing
+                                   (order-independent, bitwise reproducible; default);
+                                   1 = per-lane f32 partial sums, converted once per lane */
 } rmd_options;
 
 #define RMD_NO_PRESSURE (-1.0e300)
@@ -250,6 +253,12 @@ rmd_status rmd_debug_neighbours(rmd_sim *sim, int32_t system_index, int32_t *cap
  * the per-term breakdown (same fields as rmd_energy) and forces (f64 from fixed point). */
 rmd_status rmd_debug_evaluate(rmd_sim *sim, int32_t system_index, rmd_energy_report *energy,
                               double *forces);
+/* Forces of one term alone at the current positions and list: 0 direct space with the
+ * exceptions, 1 bonded and restraints, 2 PME reciprocal space. */
+rmd_status rmd_debug_force_term(rmd_sim *sim, int32_t system_index, int32_t term, double *forces);
+/* Copy a PME work buffer of the last evaluation: 0 the real grid after the inverse
+ * transform (K^3 doubles), 1 the half spectrum (2*Kx*Ky*(Kz/2+1) doubles). */
+rmd_status rmd_debug_read(rmd_sim *sim, int32_t system_index, int32_t which, double *out);
 /* The real spread charge grid (K^3, z fastest) of the last evaluation. */
 rmd_status rmd_debug_charge_grid(rmd_sim *sim, int32_t system_index, double *grid);
 /* A forward+inverse 3D transform check: runs the engine's R2C/C2R FFT on `data`

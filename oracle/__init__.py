@@ -209,6 +209,26 @@ class Oracle:
         energy["coulomb"] = terms[4] + terms[5] + terms[6] + terms[7]
         return energy, forces
 
+    def term_forces(self, positions, term, alpha=None, grid=None, order=5):
+        """Forces of one term: "direct" (direct space + exceptions), "bonded", "reciprocal"."""
+        L = lib()
+        pos = np.ascontiguousarray(positions, dtype=np.float64)
+        f = np.zeros(3 * self.n)
+        a, b = C.c_double(0), C.c_double(0)
+        if term == "direct":
+            L.orc_direct_space(self.ref, _p(pos, C.c_double), float(alpha), float(self.struct.cutoff),
+                               _p(f, C.c_double), C.byref(a), C.byref(b))
+            L.orc_exceptions(self.ref, _p(pos, C.c_double), float(alpha), _p(f, C.c_double),
+                             C.byref(a), C.byref(b))
+        elif term == "bonded":
+            for name in ("orc_bonds", "orc_angles", "orc_torsions"):
+                getattr(L, name)(self.ref, _p(pos, C.c_double), _p(f, C.c_double))
+        else:
+            g = np.ascontiguousarray(grid, dtype=np.int32)
+            L.orc_reciprocal(self.ref, _p(pos, C.c_double), float(alpha), _p(g, C.c_int), int(order),
+                             _p(f, C.c_double), None)
+        return f
+
     def reciprocal(self, positions, alpha, grid, order, want_grid=False):
         L = lib()
         pos = np.ascontiguousarray(positions, dtype=np.float64)

@@ -51,6 +51,7 @@ class RmdOptions(C.Structure):
         ("skin", C.c_double), ("neighbour_slack", C.c_double), ("max_neighbours", C.c_int32),
         ("ewald_tolerance", C.c_double), ("alpha", C.c_double), ("grid", C.c_int32 * 3),
         ("pme_order", C.c_int32), ("water_solver", C.c_int32), ("learned_barostat", C.c_int32),
+        ("force_accumulation", C.c_int32),
     ]
 
 
@@ -114,7 +115,7 @@ EXPORTS = [
     "rmd_diagnostics", "rmd_diagnostics_at", "rmd_destroy", "rmd_last_error", "rmd_debug_cells",
     "rmd_debug_neighbours", "rmd_debug_evaluate", "rmd_debug_charge_grid", "rmd_debug_fft",
     "rmd_debug_time_kernel", "rmd_debug_kernel_launches", "rmd_debug_set_nonbonded_lanes",
-    "rmd_bench_run",
+    "rmd_bench_run", "rmd_debug_force_term", "rmd_debug_read",
 ]
 
 _lib = None
@@ -172,6 +173,8 @@ def load():
     lib.rmd_debug_kernel_launches.restype = C.c_int64
     lib.rmd_debug_set_nonbonded_lanes.argtypes = [sim, C.c_int32]
     lib.rmd_bench_run.argtypes = [sim, C.c_int64, C.c_int32, C.c_int32, _dp]
+    lib.rmd_debug_force_term.argtypes = [sim, C.c_int32, C.c_int32, _dp]
+    lib.rmd_debug_read.argtypes = [sim, C.c_int32, C.c_int32, _dp]
     for name in EXPORTS:
         fn = getattr(lib, name)
         if fn.restype is C.c_int and name not in ("rmd_system_count",):

@@ -211,6 +211,10 @@ __device__ __forceinline__ int3 cell_coord(float3 p, const DevSys &s) {
 // read at order-1 before the final recursion step (shared/pme/parameters.js:121-149).
 template <int ORDER>
 __device__ __forceinline__ void bspline(float u, float *w, float *dw) {
+  // The derivative below reads w[ORDER-1] before the last recursion step sets it: the
+  // weights of order ORDER-1 padded with a zero, so every entry starts at zero.
+#pragma unroll
+  for (int k = 0; k < ORDER; ++k) w[k] = 0.0f;
   w[0] = 1.0f - u;
   w[1] = u;
 #pragma unroll

@@ -158,6 +158,7 @@ struct Engine {
   cudaStream_t stream = nullptr;
   std::string last_error;
   int nb_lanes = 32;
+  int pair_fixed = 1;
   int pme_order = 5;
   bool pme_on = true;
 
@@ -395,6 +396,7 @@ void Engine::build(int count, const rmd_system *systems, const rmd_options *opti
     N += hs[s].n;
   }
   pme_order = hs[0].order;
+  pair_fixed = options[0].force_accumulation == 1 ? 0 : 1;
   for (auto &h : hs)
     if (h.order != pme_order) throw Error(RMD_ERR_INVALID, "every system of a batch must use the same PME order");
   CUDA_OK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
@@ -930,6 +932,7 @@ LaunchCtx Engine::ctx() const {
   c.force = force.p;
   c.e_lj = e_lj.p;
   c.e_coul = e_coul.p;
+  c.pair_fixed = pair_fixed;
   c.bond_atoms = bond_atoms.p;
   c.bond_param = bond_param.p;
   c.n_bonds = n_bonds;
@@ -1842,6 +1845,58 @@ rmd_status rmd_debug_evaluate(rmd_sim *sim, int32_t s, rmd_energy_report *energy
                            cudaMemcpyDeviceToHost));
         for (int i = 0; i < h.n; ++i) forces[3 * i + c] = (double)f[i] / rmd::FORCE_SCALE;
       }
+    }
+  });
+}
+
+rmd_status rmd_debug_force_term(rmd_sim *sim, int32_t s, int32_t term, double *forces) {
+  if (rmd_status c = check_index(sim, s)) return c;
+  return guarded(sim, [&]() {
+    auto &e = sim->engine;
+    const rmd::LaunchCtx c = e.ctx();
+    e.sync();
+    CUDA_OK(cudaMemsetAsync(e.force.p, 0, e.force.bytes(), e.stream));
+    if (term == 0) rmd::launch_nonbonded(c, false, e.nb_lanes, e.stream);
+    else if (term == 1) rmd::launch_bonded(c, false, e.stream);
+    else if (term == 2) rmd::launch_pme(c, false, e.stream);
+    else throw rmd::Error(RMD_ERR_INVALID, "term is 0 (nonbonded), 1 (bonded) or 2 (reciprocal)");
+    e.sync();
+    CUDA_OK(cudaGetLastError());
+    const auto &h = e.hs[s];
+    std::vector<long long> f(h.n);
+    for (int k = 0; k < 3; ++k) {
+      CUDA_OK(cudaMemcpy(f.data(), e.force.p + (size_t)k * e.N + h.atom_start, sizeof(long long) * h.n,
+                         cudaMemcpyDeviceToHost));
+      for (int i = 0; i < h.n; ++i) forces[3 * i + k] = (double)f[i] / rmd::FORCE_SCALE;
+    }
+    // leave the full forces in place for whatever runs next
+    e.evaluate(false, false);
+    e.sync();
+  });
+}
+
+rmd_status rmd_debug_read(rmd_sim *sim, int32_t s, int32_t which, double *out) {
+  if (rmd_status c = check_index(sim, s)) return c;
+  return guarded(sim, [&]() {
+    auto &e = sim->engine;
+    e.sync();
+    const auto &h = e.hs[s];
+    const auto &ds = e.h_sys[s];
+    const size_t pts = (size_t)h.grid[0] * h.grid[1] * h.grid[2];
+    const size_t hp = (size_t)h.grid[0] * h.grid[1] * (h.grid[2] / 2 + 1);
+    if (which == 0) {  // real grid after the inverse transform
+      std::vector<float> g(pts);
+      CUDA_OK(cudaMemcpy(g.data(), e.real_grid.p + ds.grid_base, sizeof(float) * pts, cudaMemcpyDeviceToHost));
+      for (size_t k = 0; k < pts; ++k) out[k] = g[k];
+    } else if (which == 1) {  // half spectrum
+      std::vector<float2> g(hp);
+      CUDA_OK(cudaMemcpy(g.data(), e.half.p + ds.half_base, sizeof(float2) * hp, cudaMemcpyDeviceToHost));
+      for (size_t k = 0; k < hp; ++k) {
+        out[2 * k] = g[k].x;
+        out[2 * k + 1] = g[k].y;
+      }
+    } else {
+      throw rmd::Error(RMD_ERR_INVALID, "buffer is 0 (real grid) or 1 (half spectrum)");
     }
   });
 }

@@ -89,6 +89,7 @@ struct LaunchCtx {
   const float4 *exc_param;
   unsigned long long *force;
   double *e_lj, *e_coul;
+  int pair_fixed;  // 1: per-pair fixed-point accumulation (precision form), 0: per-lane f32
   // bonded
   const int2 *bond_atoms;
   const float2 *bond_param;

@@ -32,7 +32,11 @@ __device__ __forceinline__ double group_sum(double v) {
   return v;
 }
 
-template <bool ENERGY, int LANES>
+// PAIR_FIXED (the precision form): each pair force is quantised to 64-bit fixed point
+// before it is summed, so the atom's force is an exact integer sum and does not depend on
+// the order of its neighbour row (a rebuilt list, a resumed run, a different batch all give
+// the same bits). Without it (the plain form) lanes sum in f32 and convert once.
+template <bool ENERGY, int LANES, bool PAIR_FIXED>
 __global__ void __launch_bounds__(128) k_nonbonded(
     const float4 *__restrict__ posq, const int *__restrict__ atom_type,
     const int *__restrict__ sys_of_atom, const DevSys *__restrict__ sys,
@@ -59,6 +63,7 @@ __global__ void __launch_bounds__(128) k_nonbonded(
   const int *row = nbr + s.nbr_base + (long long)(i - s.atom_start) * s.nbr_capacity;
 
   float fx = 0.f, fy = 0.f, fz = 0.f, elj = 0.f, ecoul = 0.f;
+  long long qx = 0, qy = 0, qz = 0;
   for (int k = lane; k < count; k += LANES) {
     const int j = __ldg(row + k);
     const float4 pj = __ldg(posq + j);
@@ -76,9 +81,15 @@ __global__ void __launch_bounds__(128) k_nonbonded(
       float gauss;
       const float screened = erfc_and_gauss(alpha * r, gauss);
       scalar = fmaf(qq * fmaf(screened, inv_r, gauss_k * gauss), inv_r2, scalar);
-      fx = fmaf(scalar, d.x, fx);
-      fy = fmaf(scalar, d.y, fy);
-      fz = fmaf(scalar, d.z, fz);
+      if (PAIR_FIXED) {
+        qx += (long long)to_fixed(scalar * d.x);
+        qy += (long long)to_fixed(scalar * d.y);
+        qz += (long long)to_fixed(scalar * d.z);
+      } else {
+        fx = fmaf(scalar, d.x, fx);
+        fy = fmaf(scalar, d.y, fy);
+        fz = fmaf(scalar, d.z, fz);
+      }
       if (ENERGY) {
         elj += a12 - b6;
         ecoul = fmaf(qq * screened, inv_r, ecoul);
@@ -114,13 +125,24 @@ __global__ void __launch_bounds__(128) k_nonbonded(
       scalar -= qq * (unscreened * inv_r - gauss_k * gauss) * inv_r2;
       if (ENERGY) ecoul -= qq * unscreened * inv_r;
     }
-    fx = fmaf(scalar, d.x, fx);
-    fy = fmaf(scalar, d.y, fy);
-    fz = fmaf(scalar, d.z, fz);
+    if (PAIR_FIXED) {
+      qx += (long long)to_fixed(scalar * d.x);
+      qy += (long long)to_fixed(scalar * d.y);
+      qz += (long long)to_fixed(scalar * d.z);
+    } else {
+      fx = fmaf(scalar, d.x, fx);
+      fy = fmaf(scalar, d.y, fy);
+      fz = fmaf(scalar, d.z, fz);
+    }
   }
-  const long long gx = group_sum<LANES>((long long)to_fixed(fx));
-  const long long gy = group_sum<LANES>((long long)to_fixed(fy));
-  const long long gz = group_sum<LANES>((long long)to_fixed(fz));
+  if (!PAIR_FIXED) {
+    qx = (long long)to_fixed(fx);
+    qy = (long long)to_fixed(fy);
+    qz = (long long)to_fixed(fz);
+  }
+  const long long gx = group_sum<LANES>(qx);
+  const long long gy = group_sum<LANES>(qy);
+  const long long gz = group_sum<LANES>(qz);
   double dl = 0, dc = 0;
   if (ENERGY) {
     dl = group_sum<LANES>((double)elj);
@@ -137,26 +159,32 @@ __global__ void __launch_bounds__(128) k_nonbonded(
   }
 }
 
-template <bool ENERGY, int LANES>
+template <bool ENERGY, int LANES, bool PAIR_FIXED>
 static void launch_nb(const LaunchCtx &c, cudaStream_t stream) {
   const int threads = 128;
   const long long total = (long long)c.n_atoms * LANES;
   const int blocks = (int)((total + threads - 1) / threads);
-  k_nonbonded<ENERGY, LANES><<<blocks, threads, 0, stream>>>(
+  k_nonbonded<ENERGY, LANES, PAIR_FIXED><<<blocks, threads, 0, stream>>>(
       c.posq, c.atom_type, c.sys_of_atom, c.sys, c.lj, c.nbr, c.nbr_count, c.exc_start,
       c.exc_partner, c.exc_param, c.force, c.e_lj, c.e_coul, c.n_atoms);
 }
 
-void launch_nonbonded(const LaunchCtx &c, bool energy, int lanes, cudaStream_t stream) {
+template <bool PAIR_FIXED>
+static void launch_nb_lanes(const LaunchCtx &c, bool energy, int lanes, cudaStream_t stream) {
   if (energy) {
-    if (lanes == 8) launch_nb<true, 8>(c, stream);
-    else if (lanes == 16) launch_nb<true, 16>(c, stream);
-    else launch_nb<true, 32>(c, stream);
+    if (lanes == 8) launch_nb<true, 8, PAIR_FIXED>(c, stream);
+    else if (lanes == 16) launch_nb<true, 16, PAIR_FIXED>(c, stream);
+    else launch_nb<true, 32, PAIR_FIXED>(c, stream);
   } else {
-    if (lanes == 8) launch_nb<false, 8>(c, stream);
-    else if (lanes == 16) launch_nb<false, 16>(c, stream);
-    else launch_nb<false, 32>(c, stream);
+    if (lanes == 8) launch_nb<false, 8, PAIR_FIXED>(c, stream);
+    else if (lanes == 16) launch_nb<false, 16, PAIR_FIXED>(c, stream);
+    else launch_nb<false, 32, PAIR_FIXED>(c, stream);
   }
+}
+
+void launch_nonbonded(const LaunchCtx &c, bool energy, int lanes, cudaStream_t stream) {
+  if (c.pair_fixed) launch_nb_lanes<true>(c, energy, lanes, stream);
+  else launch_nb_lanes<false>(c, energy, lanes, stream);
 }
 
 // ------------------------------------------------------------------ bonded + restraints

@@ -54,6 +54,7 @@ _OPTION_NAMES = {
     "restraintForce": "restraint_force", "skin": "skin", "neighbourSlack": "neighbour_slack",
     "maxNeighbours": "max_neighbours", "ewaldTolerance": "ewald_tolerance", "alpha": "alpha",
     "pmeOrder": "pme_order", "waterSolver": "water_solver", "learnedBarostat": "learned_barostat",
+    "forceAccumulation": "force_accumulation",
 }
 
 
@@ -279,6 +280,19 @@ class BatchSimulation:
         self._check(self._lib.rmd_debug_evaluate(self._h, index, C.byref(out),
                                                  forces.ctypes.data_as(C.POINTER(C.c_double))))
         return _struct_dict(out), forces
+
+    def debugForceTerm(self, term: str, index=0):
+        code = {"direct": 0, "bonded": 1, "reciprocal": 2}[term]
+        forces = np.zeros(3 * self.atom_counts[index])
+        self._check(self._lib.rmd_debug_force_term(self._h, index, code,
+                                                   forces.ctypes.data_as(C.POINTER(C.c_double))))
+        return forces
+
+    def debugRead(self, which: str, count: int, index=0):
+        code = {"real_grid": 0, "half": 1}[which]
+        out = np.zeros(count)
+        self._check(self._lib.rmd_debug_read(self._h, index, code, out.ctypes.data_as(C.POINTER(C.c_double))))
+        return out
 
     def debugChargeGrid(self, index=0, points=None):
         grid = np.zeros(points)
