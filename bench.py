@@ -212,6 +212,8 @@ def main():
     parser.add_argument("--block", type=int, default=100)
     parser.add_argument("--reference-budget", type=float, default=20.0)
     parser.add_argument("--no-cpu-baseline", action="store_true")
+    parser.add_argument("--minimise", type=int, default=200, help="minimiser iterations before dynamics")
+    parser.add_argument("--equilibrate", type=int, default=3000, help="untimed steps before warm-up")
     args = parser.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -238,9 +240,9 @@ def main():
     sim = GpuSimulation(system, options_for(grid, seed=7 + rank))
     sim.setState(pos)
     sim.initialise()
-    sim.minimise(maxIterations=200, forceTolerance=1000.0)
+    sim.minimise(maxIterations=args.minimise, forceTolerance=1000.0)
     # equilibrate and settle the adaptive rebuild interval (untimed), then W warm-up blocks
-    sim.run(3000, blockSize=args.block)
+    sim.run(args.equilibrate, blockSize=args.block)
     block = min(args.block, args.steps)
     for _ in range(max(3, args.warmup)):
         sim.benchRun(block, block, flushL2=True)
