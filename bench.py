@@ -292,6 +292,9 @@ def main():
     # CUDA-event launch time on the engine's stream
     pairs = unique_pairs_within(out["positions"].astype(np.float64), system["boxVectors"][0], 0.9)
     nb_ms = sim.timeKernel("nonbonded", reps=50)
+    sim.setNonbonded(32, pairFixed=False)
+    nb_plain_ms = sim.timeKernel("nonbonded", reps=50)
+    sim.setNonbonded(32, pairFixed=True)
     pme_ms = sim.timeKernel("pme", reps=50)
     integ_ms = sim.timeKernel("integrate", reps=50)
     rebuild_ms = sim.timeKernel("rebuild", reps=20)
@@ -320,7 +323,8 @@ def main():
                      "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
                      "algorithmic_bytes": bytes_nb, "unique_pairs_within_cutoff": pairs,
                      "ms_per_launch": nb_ms},
-        "kernels_ms": {"nonbonded": nb_ms, "pme_7_kernels": pme_ms, "integrate": integ_ms,
+        "kernels_ms": {"nonbonded": nb_ms, "nonbonded_per_lane_f32": nb_plain_ms,
+                       "pme_7_kernels": pme_ms, "integrate": integ_ms,
                        "rebuild_5_kernels": rebuild_ms,
                        "pme_roofline_frac": bytes_pme / (pme_ms * 1e-3) / 1e9 / peak},
         "clocks": clocks.summary(),

@@ -280,8 +280,9 @@ rmd_status rmd_bench_run(rmd_sim *sim, int64_t count, int32_t block_size, int32_
                          double *device_ms);
 /* Kernels this handle has launched so far (graph replays included). */
 int64_t rmd_debug_kernel_launches(const rmd_sim *sim);
-/* Lanes per atom of the nonbonded kernel (8, 16 or 32), the autotuner's knob. */
-rmd_status rmd_debug_set_nonbonded_lanes(rmd_sim *sim, int32_t lanes);
+/* The nonbonded kernel's shape, the autotuner's knobs: lanes per atom (8, 16 or 32) and
+ * per-pair fixed-point (1) or per-lane f32 (0) force accumulation. */
+rmd_status rmd_debug_set_nonbonded(rmd_sim *sim, int32_t lanes, int32_t pair_fixed);
 
 #ifdef __cplusplus
 }

@@ -114,7 +114,7 @@ EXPORTS = [
     "rmd_energy", "rmd_energy_at", "rmd_read_positions", "rmd_read_state", "rmd_read_state_at",
     "rmd_diagnostics", "rmd_diagnostics_at", "rmd_destroy", "rmd_last_error", "rmd_debug_cells",
     "rmd_debug_neighbours", "rmd_debug_evaluate", "rmd_debug_charge_grid", "rmd_debug_fft",
-    "rmd_debug_time_kernel", "rmd_debug_kernel_launches", "rmd_debug_set_nonbonded_lanes",
+    "rmd_debug_time_kernel", "rmd_debug_kernel_launches", "rmd_debug_set_nonbonded",
     "rmd_bench_run", "rmd_debug_force_term", "rmd_debug_read",
 ]
 
@@ -171,7 +171,7 @@ def load():
     lib.rmd_debug_time_kernel.argtypes = [sim, C.c_int32, C.c_int32, _dp]
     lib.rmd_debug_kernel_launches.argtypes = [sim]
     lib.rmd_debug_kernel_launches.restype = C.c_int64
-    lib.rmd_debug_set_nonbonded_lanes.argtypes = [sim, C.c_int32]
+    lib.rmd_debug_set_nonbonded.argtypes = [sim, C.c_int32, C.c_int32]
     lib.rmd_bench_run.argtypes = [sim, C.c_int64, C.c_int32, C.c_int32, _dp]
     lib.rmd_debug_force_term.argtypes = [sim, C.c_int32, C.c_int32, _dp]
     lib.rmd_debug_read.argtypes = [sim, C.c_int32, C.c_int32, _dp]

@@ -784,15 +784,23 @@ void Engine::upload_all(const std::vector<const rmd_system *> &src) {
           h_tw.push_back(make_float2((float)std::cos(a), (float)std::sin(a)));
         }
       }
+      // Lines per block: as many as fit the shared buffers, but few enough that a pass has
+      // at least ~4 blocks per SM (592 on 148 SMs) and about 2 elements per thread.
+      auto lines_per_block = [](int total_lines, int n, int cap) {
+        int m = std::max(1, std::min(cap, FFT_SMEM_HOST / n));
+        m = std::min(m, std::max(1, (int)std::ceil(total_lines / 592.0)));
+        m = std::min(m, std::max(1, 512 / n));
+        return m;
+      };
       // z pass: pairs of real lines
       const int lines = nx * ny, pairs = (lines + 1) / 2;
-      const int mz = std::max(1, std::min(64, FFT_SMEM_HOST / nz));
+      const int mz = lines_per_block(pairs, nz, 64);
       for (int p = 0; p < pairs; p += mz) tz.push_back(FftTask{s, 0, p, std::min(mz, pairs - p)});
-      const int my = std::max(1, std::min(nzh, FFT_SMEM_HOST / ny));
+      const int my = lines_per_block(nx * nzh, ny, nzh);
       for (int x = 0; x < nx; ++x)
         for (int k = 0; k < nzh; k += my) ty.push_back(FftTask{s, x, k, std::min(my, nzh - k)});
       task_x_start[s] = (int)tx.size();
-      const int mx = std::max(1, std::min(nzh, FFT_SMEM_HOST / nx));
+      const int mx = lines_per_block(ny * nzh, nx, nzh);
       for (int y = 0; y < ny; ++y)
         for (int k = 0; k < nzh; k += mx) tx.push_back(FftTask{s, y, k, std::min(mx, nzh - k)});
     }
@@ -1983,10 +1991,11 @@ rmd_status rmd_debug_time_kernel(rmd_sim *sim, int32_t which, int32_t reps, doub
 
 int64_t rmd_debug_kernel_launches(const rmd_sim *sim) { return sim ? sim->engine.kernel_launches : 0; }
 
-rmd_status rmd_debug_set_nonbonded_lanes(rmd_sim *sim, int32_t lanes) {
+rmd_status rmd_debug_set_nonbonded(rmd_sim *sim, int32_t lanes, int32_t pair_fixed) {
   if (!sim || (lanes != 8 && lanes != 16 && lanes != 32)) return RMD_ERR_INVALID;
   auto &e = sim->engine;
   e.nb_lanes = lanes;
+  e.pair_fixed = pair_fixed ? 1 : 0;
   for (auto &kv : e.graphs) cudaGraphExecDestroy(kv.second);
   e.graphs.clear();
   e.graph_launches.clear();

@@ -16,11 +16,14 @@
 
 namespace rmd {
 
+// A unit's atoms, held in registers when CAP is small and every index is static (free
+// atoms: CAP 1, SETTLE waters: CAP 3); generic SHAKE clusters use CAP = MAX_CLUSTER_ATOMS.
+template <int CAP>
 struct UnitState {
   int n;
-  int atom[MAX_CLUSTER_ATOMS];
-  float x[MAX_CLUSTER_ATOMS][3], v[MAX_CLUSTER_ATOMS][3], im[MAX_CLUSTER_ATOMS], f[MAX_CLUSTER_ATOMS][3];
-  float ref[MAX_CLUSTER_ATOMS][3], corr[MAX_CLUSTER_ATOMS][3];
+  int atom[CAP];
+  float x[CAP][3], v[CAP][3], im[CAP], f[CAP][3];
+  float ref[CAP][3], corr[CAP][3];
 };
 
 struct ConstraintSet {
@@ -35,9 +38,11 @@ struct SolverDiag {
   float stalled_residual;
 };
 
-__device__ __forceinline__ void kick(UnitState &u, float h) {
-  for (int k = 0; k < u.n; ++k) {
-    if (u.im[k] <= 0.f) continue;
+template <int CAP>
+__device__ __forceinline__ void kick(UnitState<CAP> &u, float h) {
+#pragma unroll
+  for (int k = 0; k < CAP; ++k) {
+    if (k >= u.n || u.im[k] <= 0.f) continue;
     const float sc = h * u.im[k];
 #pragma unroll
     for (int c = 0; c < 3; ++c) u.v[k][c] = fmaf(sc, u.f[k][c], u.v[k][c]);
@@ -45,7 +50,7 @@ __device__ __forceinline__ void kick(UnitState &u, float h) {
 }
 
 // integrate.js:337-395
-__device__ void rattle(UnitState &u, const ConstraintSet &cs, const DevInteg &p, SolverDiag &dg) {
+__device__ void rattle(UnitState<MAX_CLUSTER_ATOMS> &u, const ConstraintSet &cs, const DevInteg &p, SolverDiag &dg) {
   if (cs.n == 0) return;
   bool converged = false, stalled = false;
   float previous = 1e30f;
@@ -75,7 +80,7 @@ __device__ void rattle(UnitState &u, const ConstraintSet &cs, const DevInteg &p,
 
 // integrate.js:188-335: SHAKE along the pre-drift bond vectors, corrections accumulated so
 // the velocity update v += correction / h never subtracts two box-spanning coordinates.
-__device__ void shake(UnitState &u, const ConstraintSet &cs, const DevInteg &p, SolverDiag &dg) {
+__device__ void shake(UnitState<MAX_CLUSTER_ATOMS> &u, const ConstraintSet &cs, const DevInteg &p, SolverDiag &dg) {
   if (cs.n == 0) return;
   for (int k = 0; k < u.n; ++k) u.corr[k][0] = u.corr[k][1] = u.corr[k][2] = 0.f;
   bool converged = false, stalled = false;
@@ -119,19 +124,24 @@ __device__ void shake(UnitState &u, const ConstraintSet &cs, const DevInteg &p, 
   dg.stalled_residual = fmaxf(dg.stalled_residual, achieved);
 }
 
-__device__ __forceinline__ void drift(UnitState &u, float h) {
-  for (int k = 0; k < u.n; ++k)
+template <int CAP>
+__device__ __forceinline__ void drift(UnitState<CAP> &u, float h) {
+#pragma unroll
+  for (int k = 0; k < CAP; ++k)
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
+      if (k >= u.n) continue;
       u.ref[k][c] = u.x[k][c];
       u.x[k][c] = fmaf(h, u.v[k][c], u.x[k][c]);
     }
 }
 
-__device__ __forceinline__ void thermostat(UnitState &u, const DevInteg &p, uint32_t step,
+template <int CAP>
+__device__ __forceinline__ void thermostat(UnitState<CAP> &u, const DevInteg &p, uint32_t step,
                                            const float *__restrict__ noise, int local_base) {
-  for (int k = 0; k < u.n; ++k) {
-    if (u.im[k] <= 0.f) continue;
+#pragma unroll
+  for (int k = 0; k < CAP; ++k) {
+    if (k >= u.n || u.im[k] <= 0.f) continue;
     float3 g;
     if (p.supplied_noise) {
       const float *nz = noise + 3 * (long long)u.atom[k];
@@ -151,7 +161,7 @@ __device__ __forceinline__ void thermostat(UnitState &u, const DevInteg &p, uint
 // triangle from the pre-drift one (reference `ref`) by a rigid motion conserving linear
 // and angular momentum; velocities (the RATTLE analogue): the 3x3 linear system for the
 // three bond-direction impulses, solved exactly.
-__device__ void settle_positions(UnitState &u, const DevSettle &w, float inv_h) {
+__device__ void settle_positions(UnitState<3> &u, const DevSettle &w, float inv_h) {
   const float mO = w.m_o, mH = w.m_h;
   const float wt = mO + 2.f * mH;
   const float ra = w.ra, rb = w.rb, rc = w.rc;  // geometry constants
@@ -219,7 +229,7 @@ __device__ void settle_positions(UnitState &u, const DevSettle &w, float inv_h) 
 
 // Remove the bond-direction relative velocity of the three water bonds exactly: solve
 // A tau = -(e_ij . v_ij) for the impulses along the unit bond vectors.
-__device__ void settle_velocities(UnitState &u, const DevSettle &w) {
+__device__ void settle_velocities(UnitState<3> &u, const DevSettle &w) {
   const int P[3][2] = {{0, 1}, {0, 2}, {1, 2}};
   float e[3][3], rhs[3];
 #pragma unroll
@@ -274,151 +284,166 @@ __device__ void settle_velocities(UnitState &u, const DevSettle &w) {
   }
 }
 
+struct UnitResult {
+  int sidx;
+  unsigned worst_bits;
+  SolverDiag dg;
+};
+
+// Apply this launch's part of the step to one unit. KIND: 0 free atom, 1 SHAKE cluster,
+// 2 SETTLE water; CAP is the unit's static capacity.
+template <int MODE, int KIND, int CAP>
+__device__ __forceinline__ void process_unit(const IntegrateArgs &g, int index, UnitResult &res) {
+  UnitState<CAP> u;
+  ConstraintSet cs;
+  cs.n = 0;
+  int settle_index = -1;
+  if (KIND == 0) {
+    u.n = 1;
+    u.atom[0] = g.free_atoms[index];
+  } else if (KIND == 1) {
+    const int ab = g.cl_atom_start[index], ae = g.cl_atom_start[index + 1];
+    u.n = ae - ab;
+    for (int k = 0; k < u.n; ++k) u.atom[k] = g.cl_atoms[ab + k];
+    const int cb = g.cl_con_start[index], ce = g.cl_con_start[index + 1];
+    cs.n = ce - cb;
+    for (int k = 0; k < cs.n; ++k) {
+      const int2 pr = g.cl_con_pair[cb + k];
+      cs.a[k] = pr.x;
+      cs.b[k] = pr.y;
+      cs.d[k] = g.cl_con_dist[cb + k];
+    }
+  } else {
+    settle_index = index;
+    const int3 w = g.settle_atoms[index];
+    u.n = 3;
+    u.atom[0] = w.x;
+    u.atom[1] = w.y;
+    u.atom[2] = w.z;
+  }
+  const int sidx = g.sys_of_atom[u.atom[0]];
+  res.sidx = sidx;
+  const DevInteg p = g.integ[sidx];
+  SolverDiag dg = {0, 0, 0, 0.f};
+  if (MODE & INT_CONSTRAIN) {
+    // minimiser: project the displaced positions back onto the constraints along the
+    // pre-displacement geometry (encodeConstrainPositions, integrate.js:672-688)
+    if (KIND == 0) return;
+#pragma unroll
+    for (int k = 0; k < CAP; ++k) {
+      if (k >= u.n) continue;
+      const int a = u.atom[k];
+      const float4 x = g.posq[a], r = g.saved_posq[a];
+      u.x[k][0] = x.x; u.x[k][1] = x.y; u.x[k][2] = x.z;
+      u.ref[k][0] = r.x; u.ref[k][1] = r.y; u.ref[k][2] = r.z;
+      u.v[k][0] = u.v[k][1] = u.v[k][2] = 0.f;
+      u.im[k] = g.vel[a].w;
+    }
+    if constexpr (KIND == 1) shake(u, cs, p, dg);
+    if constexpr (KIND == 2) settle_positions(u, g.settle_param[settle_index], 1.0f);
+#pragma unroll
+    for (int k = 0; k < CAP; ++k) {
+      if (k >= u.n) continue;
+      const float4 old = g.posq[u.atom[k]];
+      g.posq[u.atom[k]] = make_float4(u.x[k][0], u.x[k][1], u.x[k][2], old.w);
+    }
+    return;
+  }
+#pragma unroll
+  for (int k = 0; k < CAP; ++k) {
+    if (k >= u.n) continue;
+    const int a = u.atom[k];
+    const float4 x = g.posq[a];
+    const float4 v = g.vel[a];
+    u.x[k][0] = x.x; u.x[k][1] = x.y; u.x[k][2] = x.z;
+    u.v[k][0] = v.x; u.v[k][1] = v.y; u.v[k][2] = v.z;
+    u.im[k] = v.w;  // inverse mass (0 for a massless site)
+    u.f[k][0] = from_fixed(g.force[a]);
+    u.f[k][1] = from_fixed(g.force[g.n_atoms + a]);
+    u.f[k][2] = from_fixed(g.force[2 * (long long)g.n_atoms + a]);
+  }
+  const float h = p.half_step;
+  const int local_base = g.sys_atom_start[sidx];
+  const uint32_t step = (uint32_t)(g.step_base[sidx] + g.step_offset);
+  DevSettle sw;
+  if constexpr (KIND == 2) sw = g.settle_param[settle_index];
+  auto velocity_constraint = [&]() {
+    if constexpr (KIND == 1) rattle(u, cs, p, dg);
+    if constexpr (KIND == 2) settle_velocities(u, sw);
+  };
+  auto position_constraint = [&]() {
+    if constexpr (KIND == 1) shake(u, cs, p, dg);
+    if constexpr (KIND == 2) settle_positions(u, sw, 1.0f / h);
+  };
+  if (MODE & INT_CLOSE) {
+    kick(u, h);
+    velocity_constraint();
+  }
+  if (MODE & INT_CLOSE_KINETIC) {
+#pragma unroll
+    for (int k = 0; k < CAP; ++k) {
+      if (k >= u.n) continue;
+      const float m = u.im[k] > 0.f ? 1.0f / u.im[k] : 0.f;
+      g.ke_post[u.atom[k]] = 0.5 * (double)m *
+          ((double)u.v[k][0] * u.v[k][0] + (double)u.v[k][1] * u.v[k][1] + (double)u.v[k][2] * u.v[k][2]);
+    }
+  }
+  if (MODE & INT_OPEN) {
+    kick(u, h);
+    velocity_constraint();
+    drift(u, h);
+    position_constraint();
+    thermostat(u, p, step, g.noise, local_base);
+    velocity_constraint();
+    drift(u, h);
+    position_constraint();
+  }
+  if (MODE & INT_OPEN_KINETIC) {
+#pragma unroll
+    for (int k = 0; k < CAP; ++k) {
+      if (k >= u.n) continue;
+      const float m = u.im[k] > 0.f ? 1.0f / u.im[k] : 0.f;
+      g.ke_early[u.atom[k]] = 0.5 * (double)m *
+          ((double)u.v[k][0] * u.v[k][0] + (double)u.v[k][1] * u.v[k][1] + (double)u.v[k][2] * u.v[k][2]);
+    }
+  }
+  unsigned worst = 0u;
+#pragma unroll
+  for (int k = 0; k < CAP; ++k) {
+    if (k >= u.n) continue;
+    const int a = u.atom[k];
+    if (MODE & INT_OPEN) {
+      const float4 old = g.posq[a];
+      g.posq[a] = make_float4(u.x[k][0], u.x[k][1], u.x[k][2], old.w);
+      const float4 o = g.origin[a];
+      const float dx = u.x[k][0] - o.x, dy = u.x[k][1] - o.y, dz = u.x[k][2] - o.z;
+      worst = max(worst, __float_as_uint(dx * dx + dy * dy + dz * dz));
+    }
+    g.vel[a] = make_float4(u.v[k][0], u.v[k][1], u.v[k][2], u.im[k]);
+  }
+  res.worst_bits = worst;
+  res.dg = dg;
+}
+
 template <int MODE>
-__global__ void __launch_bounds__(128) k_integrate(IntegrateArgs g) {
+__global__ void __launch_bounds__(64) k_integrate(IntegrateArgs g) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int lane = threadIdx.x & 31;
   const bool active = t < g.n_units;
-  UnitState u;
-  ConstraintSet cs;
-  cs.n = 0;
-  u.n = 0;
-  int sidx = 0, kind = 0;  // 0 free, 1 cluster, 2 settle
-  int settle_index = -1;
+  UnitResult res = {0, 0u, {0, 0, 0, 0.f}};
   if (active) {
-    if (t < g.n_free) {
-      const int a = g.free_atoms[t];
-      u.n = 1;
-      u.atom[0] = a;
-      sidx = g.sys_of_atom[a];
-    } else if (t < g.n_free + g.n_clusters) {
-      kind = 1;
-      const int c = t - g.n_free;
-      const int ab = g.cl_atom_start[c], ae = g.cl_atom_start[c + 1];
-      u.n = ae - ab;
-      for (int k = 0; k < u.n; ++k) u.atom[k] = g.cl_atoms[ab + k];
-      const int cb = g.cl_con_start[c], ce = g.cl_con_start[c + 1];
-      cs.n = ce - cb;
-      for (int k = 0; k < cs.n; ++k) {
-        const int2 pr = g.cl_con_pair[cb + k];
-        cs.a[k] = pr.x;
-        cs.b[k] = pr.y;
-        cs.d[k] = g.cl_con_dist[cb + k];
-      }
-      sidx = g.sys_of_atom[u.atom[0]];
-    } else {
-      kind = 2;
-      settle_index = t - g.n_free - g.n_clusters;
-      const int3 w = g.settle_atoms[settle_index];
-      u.n = 3;
-      u.atom[0] = w.x;
-      u.atom[1] = w.y;
-      u.atom[2] = w.z;
-      sidx = g.sys_of_atom[w.x];
-      // the three constraints, for RATTLE-style diagnostics-free velocity solve
-    }
-  }
-  const DevInteg p = g.integ[sidx];
-  SolverDiag dg = {0, 0, 0, 0.f};
-  if (active) {
-    if (MODE & INT_CONSTRAIN) {
-      // minimiser: project the displaced positions back onto the constraints along the
-      // pre-displacement geometry (encodeConstrainPositions, integrate.js:672-688)
-      if (kind != 0) {
-      for (int k = 0; k < u.n; ++k) {
-        const int a = u.atom[k];
-        const float4 x = g.posq[a], r = g.saved_posq[a];
-        const float4 v = g.vel[a];
-        u.x[k][0] = x.x; u.x[k][1] = x.y; u.x[k][2] = x.z;
-        u.ref[k][0] = r.x; u.ref[k][1] = r.y; u.ref[k][2] = r.z;
-        u.v[k][0] = u.v[k][1] = u.v[k][2] = 0.f;
-        u.im[k] = v.w;
-      }
-      if (kind == 1) shake(u, cs, p, dg);
-      else settle_positions(u, g.settle_param[settle_index], 1.0f);
-      for (int k = 0; k < u.n; ++k) {
-        const float4 old = g.posq[u.atom[k]];
-        g.posq[u.atom[k]] = make_float4(u.x[k][0], u.x[k][1], u.x[k][2], old.w);
-      }
-      }
-    } else {
-    for (int k = 0; k < u.n; ++k) {
-      const int a = u.atom[k];
-      const float4 x = g.posq[a];
-      const float4 v = g.vel[a];
-      u.x[k][0] = x.x; u.x[k][1] = x.y; u.x[k][2] = x.z;
-      u.v[k][0] = v.x; u.v[k][1] = v.y; u.v[k][2] = v.z;
-      u.im[k] = v.w;  // inverse mass (0 for a massless site)
-      u.f[k][0] = from_fixed(g.force[a]);
-      u.f[k][1] = from_fixed(g.force[g.n_atoms + a]);
-      u.f[k][2] = from_fixed(g.force[2 * (long long)g.n_atoms + a]);
-    }
-    const float h = p.half_step;
-    const int local_base = g.sys_atom_start[sidx];
-    const uint32_t step = (uint32_t)(g.step_base[sidx] + g.step_offset);
-    DevSettle sw;
-    if (kind == 2) sw = g.settle_param[settle_index];
-    auto velocity_constraint = [&]() {
-      if (kind == 1) rattle(u, cs, p, dg);
-      else if (kind == 2) settle_velocities(u, sw);
-    };
-    auto position_constraint = [&]() {
-      if (kind == 1) shake(u, cs, p, dg);
-      else if (kind == 2) settle_positions(u, sw, 1.0f / h);
-    };
-    if (MODE & INT_CLOSE) {
-      kick(u, h);
-      velocity_constraint();
-    }
-    if (MODE & INT_CLOSE_KINETIC) {
-      for (int k = 0; k < u.n; ++k) {
-        const float m = u.im[k] > 0.f ? 1.0f / u.im[k] : 0.f;
-        g.ke_post[u.atom[k]] = 0.5 * (double)m *
-            ((double)u.v[k][0] * u.v[k][0] + (double)u.v[k][1] * u.v[k][1] + (double)u.v[k][2] * u.v[k][2]);
-      }
-    }
-    if (MODE & INT_OPEN) {
-      kick(u, h);
-      velocity_constraint();
-      drift(u, h);
-      position_constraint();
-      thermostat(u, p, step, g.noise, local_base);
-      velocity_constraint();
-      drift(u, h);
-      position_constraint();
-    }
-    if (MODE & INT_OPEN_KINETIC) {
-      for (int k = 0; k < u.n; ++k) {
-        const float m = u.im[k] > 0.f ? 1.0f / u.im[k] : 0.f;
-        g.ke_early[u.atom[k]] = 0.5 * (double)m *
-            ((double)u.v[k][0] * u.v[k][0] + (double)u.v[k][1] * u.v[k][1] + (double)u.v[k][2] * u.v[k][2]);
-      }
-    }
-    for (int k = 0; k < u.n; ++k) {
-      const int a = u.atom[k];
-      if (MODE & INT_OPEN) {
-        const float4 old = g.posq[a];
-        g.posq[a] = make_float4(u.x[k][0], u.x[k][1], u.x[k][2], old.w);
-      }
-      g.vel[a] = make_float4(u.v[k][0], u.v[k][1], u.v[k][2], u.im[k]);
-    }
-    }
+    if (t < g.n_free) process_unit<MODE, 0, 1>(g, t, res);
+    else if (t < g.n_free + g.n_clusters) process_unit<MODE, 1, MAX_CLUSTER_ATOMS>(g, t - g.n_free, res);
+    else process_unit<MODE, 2, 3>(g, t - g.n_free - g.n_clusters, res);
   }
   if (MODE & INT_CONSTRAIN) return;  // every thread of the launch leaves here together
   // --- skin displacement and solver diagnostics, aggregated per warp when it is one system
-  unsigned worst_bits = 0u;
-  if (active && (MODE & INT_OPEN)) {
-    for (int k = 0; k < u.n; ++k) {
-      const float4 o = g.origin[u.atom[k]];
-      const float dx = u.x[k][0] - o.x, dy = u.x[k][1] - o.y, dz = u.x[k][2] - o.z;
-      const float d2 = dx * dx + dy * dy + dz * dz;
-      worst_bits = max(worst_bits, __float_as_uint(d2));
-    }
-  }
+  const int sidx = res.sidx;
+  unsigned worst_bits = res.worst_bits;
   const int sref = __shfl_sync(0xffffffffu, sidx, 0);
   const bool uniform = __all_sync(0xffffffffu, !active || sidx == sref);
-  int diag_iter = dg.max_iterations, diag_shake = dg.shake_cap, diag_rattle = dg.rattle_cap;
-  unsigned diag_res = __float_as_uint(dg.stalled_residual);
+  int diag_iter = res.dg.max_iterations, diag_shake = res.dg.shake_cap, diag_rattle = res.dg.rattle_cap;
+  unsigned diag_res = __float_as_uint(res.dg.stalled_residual);
   if (uniform) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
@@ -444,7 +469,7 @@ __global__ void __launch_bounds__(128) k_integrate(IntegrateArgs g) {
 
 void launch_integrate(const IntegrateArgs &a, int mode, cudaStream_t stream) {
   if (a.n_units == 0) return;
-  const int tb = 128, blocks = (a.n_units + tb - 1) / tb;
+  const int tb = 64, blocks = (a.n_units + tb - 1) / tb;
   switch (mode) {
     case INT_OPEN: k_integrate<INT_OPEN><<<blocks, tb, 0, stream>>>(a); break;
     case INT_OPEN | INT_OPEN_KINETIC:

@@ -181,9 +181,15 @@ __global__ void k_neighbours(const float4 *__restrict__ posq, const int *__restr
           ok = ok && j != i;
           if (ok) {
             const float4 pj = posq[j];
-            float3 d = make_float3(__fsub_rn(pi.x, pj.x), __fsub_rn(pi.y, pj.y), __fsub_rn(pi.z, pj.z));
-            d = min_image_exact(d, s);
-            ok = !(dot_exact(d) > lc2);
+            const float3 d0 = make_float3(__fsub_rn(pi.x, pj.x), __fsub_rn(pi.y, pj.y), __fsub_rn(pi.z, pj.z));
+            // Cull with the cheap form (reciprocal multiply, rint, FMA); it agrees with the
+            // exact-rounding form to a few ulp, so only candidates within a 1e-5 relative band
+            // of the list cutoff need the exact test that decides membership.
+            const float3 df = min_image(d0, s);
+            const float r2f = fmaf(df.x, df.x, fmaf(df.y, df.y, df.z * df.z));
+            if (r2f > lc2 * 1.00001f) ok = false;
+            else if (r2f < lc2 * 0.99999f) ok = true;
+            else ok = !(dot_exact(min_image_exact(d0, s)) > lc2);
           }
           if (ok) ok = !is_excluded(excl_start, excl_partners, i, j);
           const unsigned mask = __ballot_sync(0xffffffffu, ok);

@@ -120,12 +120,17 @@ __device__ float2 *fft_lines(float2 *a, float2 *b, int lines, int N, const FftAx
 constexpr int FFT_SMEM = 2048;  // complex values per buffer per block
 
 // ------------------------------------------------------------------------ spreading
+// ORDER*ORDER threads per atom: thread (kx, ky) adds the ORDER points of one z-row. Each
+// thread recomputes the atom's splines (cheap) so no cross-thread exchange is needed, and
+// the atom's p^3 atomics are issued by many threads at once instead of serially.
 template <int ORDER>
 __global__ void k_spread(const float4 *__restrict__ posq, const int *__restrict__ sys_of_atom,
                          const DevSys *__restrict__ sys, unsigned long long *__restrict__ fixed_grid,
                          int n_atoms) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = (int)(t / (ORDER * ORDER));
   if (i >= n_atoms) return;
+  const int kx = (int)(t % (ORDER * ORDER)) / ORDER, ky = (int)(t % ORDER);
   const float4 p = posq[i];
   if (p.w == 0.f) return;
   const DevSys &s = sys[sys_of_atom[i]];
@@ -140,22 +145,20 @@ __global__ void k_spread(const float4 *__restrict__ posq, const int *__restrict_
     bspline<ORDER>(scaled - fl, w[d], dw[d]);
   }
   const int nx = s.grid[0], ny = s.grid[1], nz = s.grid[2];
-  unsigned long long *g = fixed_grid + s.grid_base;
+  const int ix = wrap_index(base[0] + kx - ORDER + 1, nx);
+  const int iy = wrap_index(base[1] + ky - ORDER + 1, ny);
+  float wx = 0.f, wy = 0.f;
 #pragma unroll
-  for (int kx = 0; kx < ORDER; ++kx) {
-    const int ix = wrap_index(base[0] + kx - ORDER + 1, nx);
-    const float wx = p.w * w[0][kx];
+  for (int k = 0; k < ORDER; ++k) {
+    if (k == kx) wx = w[0][k];
+    if (k == ky) wy = w[1][k];
+  }
+  const float wxy = p.w * wx * wy;
+  unsigned long long *rowp = fixed_grid + s.grid_base + ((long long)ix * ny + iy) * nz;
 #pragma unroll
-    for (int ky = 0; ky < ORDER; ++ky) {
-      const int iy = wrap_index(base[1] + ky - ORDER + 1, ny);
-      const float wxy = wx * w[1][ky];
-      unsigned long long *rowp = g + ((long long)ix * ny + iy) * nz;
-#pragma unroll
-      for (int kz = 0; kz < ORDER; ++kz) {
-        const int iz = wrap_index(base[2] + kz - ORDER + 1, nz);
-        atomicAdd(rowp + iz, to_fixed(wxy * w[2][kz]));
-      }
-    }
+  for (int kz = 0; kz < ORDER; ++kz) {
+    const int iz = wrap_index(base[2] + kz - ORDER + 1, nz);
+    atomicAdd(rowp + iz, to_fixed(wxy * w[2][kz]));
   }
 }
 
@@ -395,9 +398,11 @@ void launch_pme(const LaunchCtx &c, bool energy, cudaStream_t stream) {
   if (!c.pme_on) return;
   const int n = c.n_atoms, tb = 128;
   if (c.pme_order == 4)
-    k_spread<4><<<(n + tb - 1) / tb, tb, 0, stream>>>(c.posq, c.sys_of_atom, c.sys, c.fixed_grid, n);
+    k_spread<4><<<(int)(((long long)n * 16 + tb - 1) / tb), tb, 0, stream>>>(c.posq, c.sys_of_atom, c.sys,
+                                                                            c.fixed_grid, n);
   else
-    k_spread<5><<<(n + tb - 1) / tb, tb, 0, stream>>>(c.posq, c.sys_of_atom, c.sys, c.fixed_grid, n);
+    k_spread<5><<<(int)(((long long)n * 25 + tb - 1) / tb), tb, 0, stream>>>(c.posq, c.sys_of_atom, c.sys,
+                                                                            c.fixed_grid, n);
   k_fft_z_r2c<<<c.n_tasks_z, 256, 0, stream>>>(c.tasks_z, c.sys, c.fft_plans, c.twiddles,
                                                 c.fixed_grid, c.half);
   k_fft_y<<<c.n_tasks_y, 256, 0, stream>>>(c.tasks_y, c.sys, c.fft_plans, c.twiddles, c.half, 0);
@@ -444,9 +449,11 @@ __global__ void k_fft_x_plain(const FftTask *__restrict__ tasks, const DevSys *_
 void launch_spread_only(const LaunchCtx &c, cudaStream_t stream) {
   const int n = c.n_atoms, tb = 128;
   if (c.pme_order == 4)
-    k_spread<4><<<(n + tb - 1) / tb, tb, 0, stream>>>(c.posq, c.sys_of_atom, c.sys, c.fixed_grid, n);
+    k_spread<4><<<(int)(((long long)n * 16 + tb - 1) / tb), tb, 0, stream>>>(c.posq, c.sys_of_atom, c.sys,
+                                                                            c.fixed_grid, n);
   else
-    k_spread<5><<<(n + tb - 1) / tb, tb, 0, stream>>>(c.posq, c.sys_of_atom, c.sys, c.fixed_grid, n);
+    k_spread<5><<<(int)(((long long)n * 25 + tb - 1) / tb), tb, 0, stream>>>(c.posq, c.sys_of_atom, c.sys,
+                                                                            c.fixed_grid, n);
 }
 
 void launch_fft_forward(const LaunchCtx &c, cudaStream_t stream) {

@@ -326,8 +326,8 @@ class BatchSimulation:
     def kernelLaunches(self) -> int:
         return int(self._lib.rmd_debug_kernel_launches(self._h))
 
-    def setNonbondedLanes(self, lanes: int):
-        self._check(self._lib.rmd_debug_set_nonbonded_lanes(self._h, int(lanes)))
+    def setNonbonded(self, lanes: int = 32, pairFixed: bool = True):
+        self._check(self._lib.rmd_debug_set_nonbonded(self._h, int(lanes), 1 if pairFixed else 0))
 
     def release(self):
         if getattr(self, "_h", None):
