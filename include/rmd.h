@@ -284,6 +284,22 @@ int64_t rmd_debug_kernel_launches(const rmd_sim *sim);
  * per-pair fixed-point (1) or per-lane f32 (0) force accumulation. */
 rmd_status rmd_debug_set_nonbonded(rmd_sim *sim, int32_t lanes, int32_t pair_fixed);
 
+/* Allocation-free PME charge spreading, for callers that cannot call cudaMalloc: code
+ * recording into its own CUDA graph during stream capture, hosts whose device memory all
+ * comes from their own arena, and latency-bound callers that cannot take cudaMalloc's
+ * implicit synchronisation. This entry point has no counterpart in the reference.
+ * `posq` is a device array of float4 (x, y, z in nm, charge in e) for `atom_count` atoms;
+ * `grid_out` a device array of grid[0]*grid[1]*grid[2] doubles (z fastest) that receives
+ * the spread charge, exactly as the engine's spreading computes it (B-spline `order` 4 or 5,
+ * 64-bit fixed-point accumulation). The fixed-point grid lives in a static device array of
+ * at most 64^3 points (2 MiB); larger grids return RMD_ERR_INVALID. Work is queued on
+ * `stream` (NULL: the legacy default stream) and is complete when the stream is. The
+ * array is shared by all calls: calls that overlap on the GPU race. The first call on a
+ * device resolves the array's device address (cudaGetSymbolAddress) and must come before
+ * any stream capture; later calls allocate nothing and can be captured. */
+rmd_status rmd_spread_charges_noalloc(const void *posq, int32_t atom_count, const double box_vectors[9],
+                                      const int32_t grid[3], int32_t order, double *grid_out, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -115,7 +115,7 @@ EXPORTS = [
     "rmd_diagnostics", "rmd_diagnostics_at", "rmd_destroy", "rmd_last_error", "rmd_debug_cells",
     "rmd_debug_neighbours", "rmd_debug_evaluate", "rmd_debug_charge_grid", "rmd_debug_fft",
     "rmd_debug_time_kernel", "rmd_debug_kernel_launches", "rmd_debug_set_nonbonded",
-    "rmd_bench_run", "rmd_debug_force_term", "rmd_debug_read",
+    "rmd_bench_run", "rmd_debug_force_term", "rmd_debug_read", "rmd_spread_charges_noalloc",
 ]
 
 _lib = None
@@ -175,6 +175,8 @@ def load():
     lib.rmd_bench_run.argtypes = [sim, C.c_int64, C.c_int32, C.c_int32, _dp]
     lib.rmd_debug_force_term.argtypes = [sim, C.c_int32, C.c_int32, _dp]
     lib.rmd_debug_read.argtypes = [sim, C.c_int32, C.c_int32, _dp]
+    lib.rmd_spread_charges_noalloc.argtypes = [C.c_void_p, C.c_int32, _dp, _i32p, C.c_int32, C.c_void_p,
+                                               C.c_void_p]
     for name in EXPORTS:
         fn = getattr(lib, name)
         if fn.restype is C.c_int and name not in ("rmd_system_count",):
