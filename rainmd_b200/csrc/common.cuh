@@ -48,6 +48,10 @@ struct DevSys {
   int moduli_base;      // moduli[x][y][z] concatenated (Kx+Ky+Kz)
   int order;
   int molecule_start, molecule_count;  // into molecule CSR
+  // Lattice shifts S = ka*a + kb*b + kc*c for ka, kb, kc in {-1, 0, 1}, indexed by
+  // code = (ka+1)*9 + (kb+1)*3 + (kc+1): a neighbour entry carries the code of the image of
+  // its partner that was nearest when the list was built (d = x_i - x_j - S).
+  float4 shift[27];
 };
 
 // FP64 per-system state owned by the device (box for the barostat, energies, counters).
@@ -237,6 +241,10 @@ __device__ __forceinline__ void bspline(float u, float *w, float *dw) {
         div * ((u + (float)j) * w[ORDER - j - 2] + ((float)(ORDER - j) - u) * w[ORDER - j - 1]);
   w[0] = div * (1.0f - u) * w[0];
 }
+
+__device__ __forceinline__ int shift_code(int ka, int kb, int kc) { return (ka + 1) * 9 + (kb + 1) * 3 + (kc + 1); }
+constexpr int NBR_SLOT_BITS = 27;
+constexpr int NBR_SLOT_MASK = (1 << NBR_SLOT_BITS) - 1;
 
 __device__ __forceinline__ int wrap_index(int v, int n) {
   int r = v % n;

@@ -174,6 +174,8 @@ struct Engine {
   DevArray<int> cell_of_atom, cell_count, cell_start, cell_atoms, cell_sys;
   int n_cells_total = 0;
   DevArray<int> nbr, nbr_count, required;
+  DevArray<float4> spos, wrap;
+  DevArray<int> sorted_orig, sorted_type, rank;
   DevArray<int2> bond_atoms;
   DevArray<float2> bond_param, angle_param;
   DevArray<int4> angle_atoms, tor_atoms;
@@ -755,6 +757,16 @@ void Engine::upload_all(const std::vector<const rmd_system *> &src) {
   cell_start.zero();
   cell_atoms.alloc(N);
   cell_of_atom.alloc(N);
+  spos.alloc(N);
+  spos.zero();
+  wrap.alloc(N);
+  wrap.zero();
+  sorted_orig.alloc(N);
+  sorted_orig.zero();
+  sorted_type.alloc(N);
+  sorted_type.zero();
+  rank.alloc(N);
+  rank.zero();
   required.alloc(S);
   required.zero();
 
@@ -933,6 +945,11 @@ LaunchCtx Engine::ctx() const {
   c.nbr_count = nbr_count.p;
   c.required = required.p;
   c.origin = origin.p;
+  c.spos = spos.p;
+  c.wrap = wrap.p;
+  c.sorted_orig = sorted_orig.p;
+  c.sorted_type = sorted_type.p;
+  c.rank = rank.p;
   c.lj = lj.p;
   c.exc_start = exc_start.p;
   c.exc_partner = exc_partner.p;
@@ -1003,6 +1020,9 @@ IntegrateArgs Engine::iargs(int step_offset) const {
   a.ke_post = ke_post.p;
   a.ke_early = ke_early.p;
   a.saved_posq = saved_posq.p;
+  a.spos = spos.p;
+  a.rank = rank.p;
+  a.wrap = wrap.p;
   return a;
 }
 
@@ -1826,11 +1846,22 @@ rmd_status rmd_debug_neighbours(rmd_sim *sim, int32_t s, int32_t *capacity, int3
     const auto &h = e.hs[s];
     const auto &ds = e.h_sys[s];
     if (capacity) *capacity = ds.nbr_capacity;
-    if (counts) CUDA_OK(cudaMemcpy(counts, e.nbr_count.p + h.atom_start, sizeof(int) * h.n, cudaMemcpyDeviceToHost));
-    if (rows) {
-      CUDA_OK(cudaMemcpy(rows, e.nbr.p + ds.nbr_base, sizeof(int) * (size_t)h.n * ds.nbr_capacity,
-                         cudaMemcpyDeviceToHost));
-      for (size_t k = 0; k < (size_t)h.n * ds.nbr_capacity; ++k) rows[k] -= h.atom_start;
+    // rows are stored per cell-ordered slot with (slot | image code) entries: map both back
+    // to the system's own atom indices, as the reference lists them
+    const int cap = ds.nbr_capacity;
+    std::vector<int> slot_counts(h.n), order(h.n), raw((size_t)h.n * cap);
+    CUDA_OK(cudaMemcpy(slot_counts.data(), e.nbr_count.p + h.atom_start, sizeof(int) * h.n, cudaMemcpyDeviceToHost));
+    CUDA_OK(cudaMemcpy(order.data(), e.sorted_orig.p + h.atom_start, sizeof(int) * h.n, cudaMemcpyDeviceToHost));
+    CUDA_OK(cudaMemcpy(raw.data(), e.nbr.p + ds.nbr_base, sizeof(int) * raw.size(), cudaMemcpyDeviceToHost));
+    for (int sl = 0; sl < h.n; ++sl) {
+      const int atom = order[sl] - h.atom_start;
+      if (counts) counts[atom] = slot_counts[sl];
+      if (rows)
+        for (int k = 0; k < cap; ++k) {
+          const unsigned entry = (unsigned)raw[(size_t)sl * cap + k];
+          rows[(size_t)atom * cap + k] =
+              k < slot_counts[sl] ? order[(int)(entry & rmd::NBR_SLOT_MASK) - h.atom_start] - h.atom_start : 0;
+        }
     }
     if (req) CUDA_OK(cudaMemcpy(req, e.required.p + s, sizeof(int), cudaMemcpyDeviceToHost));
   });

@@ -415,6 +415,9 @@ __device__ __forceinline__ void process_unit(const IntegrateArgs &g, int index, 
     if (MODE & INT_OPEN) {
       const float4 old = g.posq[a];
       g.posq[a] = make_float4(u.x[k][0], u.x[k][1], u.x[k][2], old.w);
+      // keep the cell-ordered copy current: same wrap shift as at the last rebuild
+      const float4 w = g.wrap[a];
+      g.spos[g.rank[a]] = make_float4(u.x[k][0] - w.x, u.x[k][1] - w.y, u.x[k][2] - w.z, old.w);
       const float4 o = g.origin[a];
       const float dx = u.x[k][0] - o.x, dy = u.x[k][1] - o.y, dz = u.x[k][2] - o.z;
       worst = max(worst, __float_as_uint(dx * dx + dy * dy + dz * dz));

@@ -68,6 +68,9 @@ struct IntegrateArgs {
   int *diag;
   double *ke_post, *ke_early;
   const float4 *saved_posq;
+  float4 *spos;
+  const int *rank;
+  const float4 *wrap;
 };
 
 struct LaunchCtx {
@@ -83,6 +86,12 @@ struct LaunchCtx {
   const int *excl_start, *excl_partners;
   int *nbr, *nbr_count, *required;
   float4 *origin;
+  // cell-ordered copies written at each rebuild and kept current by the integrator:
+  // spos[slot] = position minus the atom's wrap shift (w = charge), the original index,
+  // the LJ type; rank[atom] = slot and wrap[atom] = that shift
+  float4 *spos;
+  int *sorted_orig, *sorted_type, *rank;
+  float4 *wrap;
   // nonbonded
   const float2 *lj;
   const int *exc_start, *exc_partner;

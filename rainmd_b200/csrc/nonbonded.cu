@@ -38,8 +38,8 @@ __device__ __forceinline__ double group_sum(double v) {
 // the same bits). Without it (the plain form) lanes sum in f32 and convert once.
 template <bool ENERGY, int LANES, bool PAIR_FIXED>
 __global__ void __launch_bounds__(128) k_nonbonded(
-    const float4 *__restrict__ posq, const int *__restrict__ atom_type,
-    const int *__restrict__ sys_of_atom, const DevSys *__restrict__ sys,
+    const float4 *__restrict__ posq, const float4 *__restrict__ spos, const int *__restrict__ sorted_orig,
+    const int *__restrict__ sorted_type, const int *__restrict__ sys_of_atom, const DevSys *__restrict__ sys,
     const float2 *__restrict__ lj, const int *__restrict__ nbr, const int *__restrict__ nbr_count,
     const int *__restrict__ exc_start, const int *__restrict__ exc_partner,
     const float4 *__restrict__ exc_param, unsigned long long *__restrict__ force,
@@ -49,31 +49,34 @@ __global__ void __launch_bounds__(128) k_nonbonded(
   // with an empty row and stores nothing, so every lane reaches the shuffles.
   const bool valid = gid / LANES < n_atoms;
   if (!valid && LANES == 32) return;
-  const int i = valid ? gid / LANES : n_atoms - 1;
+  const int si = valid ? gid / LANES : n_atoms - 1;  // atoms are visited in cell order
   const int lane = gid % LANES;
+  const int i = sorted_orig[si];
   const DevSys &s = sys[sys_of_atom[i]];
-  const float4 pi = posq[i];
-  const float qik = (float)ONE_4PI_EPS0 * pi.w;
-  const int ti = atom_type[i];
+  const float4 pw = spos[si];
+  const float qik = (float)ONE_4PI_EPS0 * pw.w;
+  const int ti = sorted_type[si];
   const float2 *ljrow = lj + s.lj_base + ti * s.type_count;
   const float alpha = s.alpha;
   const float gauss_k = 2.0f * alpha * 0.5641895835477563f;  // 2a/sqrt(pi)
   const float cut2 = s.cutoff2;
-  const int count = valid ? nbr_count[i] : 0;
-  const int *row = nbr + s.nbr_base + (long long)(i - s.atom_start) * s.nbr_capacity;
+  const int count = valid ? nbr_count[si] : 0;
+  const int *row = nbr + s.nbr_base + (long long)(si - s.atom_start) * s.nbr_capacity;
 
   float fx = 0.f, fy = 0.f, fz = 0.f, elj = 0.f, ecoul = 0.f;
   long long qx = 0, qy = 0, qz = 0;
   for (int k = lane; k < count; k += LANES) {
-    const int j = __ldg(row + k);
-    const float4 pj = __ldg(posq + j);
-    float3 d = min_image(make_float3(pi.x - pj.x, pi.y - pj.y, pi.z - pj.z), s);
+    const unsigned e = (unsigned)__ldg(row + k);
+    const int g = (int)(e & NBR_SLOT_MASK);
+    const float4 pj = __ldg(spos + g);
+    const float4 S = s.shift[e >> NBR_SLOT_BITS];  // the partner's image (code 0..26), fixed at the rebuild
+    const float3 d = make_float3(pw.x - pj.x - S.x, pw.y - pj.y - S.y, pw.z - pj.z - S.z);
     const float r2 = fmaf(d.x, d.x, fmaf(d.y, d.y, d.z * d.z));
     if (r2 <= cut2) {
       const float inv_r = rsqrtf(r2);
       const float inv_r2 = inv_r * inv_r;
       const float inv_r6 = inv_r2 * inv_r2 * inv_r2;
-      const float2 ab = __ldg(ljrow + __ldg(atom_type + j));
+      const float2 ab = __ldg(ljrow + __ldg(sorted_type + g));
       const float a12 = ab.x * inv_r6 * inv_r6, b6 = ab.y * inv_r6;
       float scalar = (12.0f * a12 - 6.0f * b6) * inv_r2;
       const float qq = qik * pj.w;
@@ -98,6 +101,7 @@ __global__ void __launch_bounds__(128) k_nonbonded(
   }
   // Exceptions: 1-4 scaled LJ/Coulomb and -q_i q_j erf(a r)/r, no cutoff.
   const int eb = exc_start[i], ee = valid ? exc_start[i + 1] : eb;
+  const float4 pi = posq[i];
   for (int e = eb + lane; e < ee; e += LANES) {
     const int j = exc_partner[e];
     const float4 prm = exc_param[e];  // chargeProduct, ljA, ljB, fullProduct
@@ -165,7 +169,7 @@ static void launch_nb(const LaunchCtx &c, cudaStream_t stream) {
   const long long total = (long long)c.n_atoms * LANES;
   const int blocks = (int)((total + threads - 1) / threads);
   k_nonbonded<ENERGY, LANES, PAIR_FIXED><<<blocks, threads, 0, stream>>>(
-      c.posq, c.atom_type, c.sys_of_atom, c.sys, c.lj, c.nbr, c.nbr_count, c.exc_start,
+      c.posq, c.spos, c.sorted_orig, c.sorted_type, c.sys_of_atom, c.sys, c.lj, c.nbr, c.nbr_count, c.exc_start,
       c.exc_partner, c.exc_param, c.force, c.e_lj, c.e_coul, c.n_atoms);
 }
 

@@ -77,6 +77,11 @@ __device__ void set_box(DevSys &s, DevSysD &d, const double *b) {
     s.box[k] = (float)b[k];
     s.recip[k] = (float)r[k];
   }
+  for (int code = 0; code < 27; ++code) {
+    const int ka = code / 9 - 1, kb = (code / 3) % 3 - 1, kc = code % 3 - 1;
+    s.shift[code] = make_float4((float)(ka * b[0] + kb * b[3] + kc * b[6]), (float)(ka * b[1] + kb * b[4] + kc * b[7]),
+                                (float)(ka * b[2] + kb * b[5] + kc * b[8]), 0.f);
+  }
   s.inv_diag[0] = (float)(1.0 / ax);
   s.inv_diag[1] = (float)(1.0 / by);
   s.inv_diag[2] = (float)(1.0 / cz);
