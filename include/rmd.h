@@ -103,6 +103,10 @@ typedef struct {
   int32_t force_accumulation;   /* 0 = each pair force quantised to 64-bit fixed point before summing
                                    (order-independent, bitwise reproducible; default);
                                    1 = per-lane f32 partial sums, converted once per lane */
+  /* kernel shapes; 0 = chosen by the engine's autotuner at initialise() */
+  int32_t neighbour_group_atoms; /* atoms per neighbour-search warp: 8, 16 or 32 */
+  int32_t nonbonded_lanes;       /* lanes per atom in the pair loop: 8, 16 or 32 */
+  int32_t spread_atoms_per_block; /* atoms per PME charge-spreading block: 4, 8 or 16 */
 } rmd_options;
 
 #define RMD_NO_PRESSURE (-1.0e300)
@@ -280,6 +284,17 @@ rmd_status rmd_bench_run(rmd_sim *sim, int64_t count, int32_t block_size, int32_
                          double *device_ms);
 /* Kernels this handle has launched so far (graph replays included). */
 int64_t rmd_debug_kernel_launches(const rmd_sim *sim);
+/* Kernel launch shapes in use: shapes = {atoms per neighbour-search warp, lanes per atom in
+ * the pair loop, atoms per PME spreading block}. When the options left a shape at 0,
+ * initialise() chose it by timing every candidate (the engine's autotuner); tune_ms (may be
+ * NULL) receives those times in ms per launch, in the order group 8/16/32, lanes 8/16/32,
+ * spreading 4/8/16, with -1 for shapes that were not tuned. No reference counterpart: the
+ * reference's WGSL kernels have fixed workgroup sizes. */
+rmd_status rmd_kernel_shapes(const rmd_sim *sim, int32_t shapes[3], double tune_ms[9]);
+/* Set launch shapes by hand (0 keeps the current one). Results do not depend on them, except
+ * the pair loop's lanes under per-lane f32 accumulation. */
+rmd_status rmd_set_kernel_shapes(rmd_sim *sim, int32_t group_atoms, int32_t nonbonded_lanes,
+                                 int32_t spread_atoms);
 /* The nonbonded kernel's shape, the autotuner's knobs: lanes per atom (8, 16 or 32) and
  * per-pair fixed-point (1) or per-lane f32 (0) force accumulation. */
 rmd_status rmd_debug_set_nonbonded(rmd_sim *sim, int32_t lanes, int32_t pair_fixed);

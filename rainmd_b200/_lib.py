@@ -51,7 +51,8 @@ class RmdOptions(C.Structure):
         ("skin", C.c_double), ("neighbour_slack", C.c_double), ("max_neighbours", C.c_int32),
         ("ewald_tolerance", C.c_double), ("alpha", C.c_double), ("grid", C.c_int32 * 3),
         ("pme_order", C.c_int32), ("water_solver", C.c_int32), ("learned_barostat", C.c_int32),
-        ("force_accumulation", C.c_int32),
+        ("force_accumulation", C.c_int32), ("neighbour_group_atoms", C.c_int32),
+        ("nonbonded_lanes", C.c_int32), ("spread_atoms_per_block", C.c_int32),
     ]
 
 
@@ -116,6 +117,7 @@ EXPORTS = [
     "rmd_debug_neighbours", "rmd_debug_evaluate", "rmd_debug_charge_grid", "rmd_debug_fft",
     "rmd_debug_time_kernel", "rmd_debug_kernel_launches", "rmd_debug_set_nonbonded",
     "rmd_bench_run", "rmd_debug_force_term", "rmd_debug_read", "rmd_spread_charges_noalloc",
+    "rmd_kernel_shapes", "rmd_set_kernel_shapes",
 ]
 
 _lib = None
@@ -172,6 +174,8 @@ def load():
     lib.rmd_debug_kernel_launches.argtypes = [sim]
     lib.rmd_debug_kernel_launches.restype = C.c_int64
     lib.rmd_debug_set_nonbonded.argtypes = [sim, C.c_int32, C.c_int32]
+    lib.rmd_kernel_shapes.argtypes = [sim, _i32p, _dp]
+    lib.rmd_set_kernel_shapes.argtypes = [sim, C.c_int32, C.c_int32, C.c_int32]
     lib.rmd_bench_run.argtypes = [sim, C.c_int64, C.c_int32, C.c_int32, _dp]
     lib.rmd_debug_force_term.argtypes = [sim, C.c_int32, C.c_int32, _dp]
     lib.rmd_debug_read.argtypes = [sim, C.c_int32, C.c_int32, _dp]

@@ -40,6 +40,7 @@ struct DevSys {
   int cell_base;        // offset into per-cell arrays (count/cursor)
   int cell_start_base;  // offset into cell_start ((cells + 1) per system)
   int cell_capacity;    // cells allocated for this system
+  int group_base;       // first neighbour-search group slot of this system
   long long nbr_base;   // offset of row 0 in the neighbour array
   int nbr_capacity;
   int grid[3];

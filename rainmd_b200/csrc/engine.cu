@@ -6,7 +6,11 @@
 // reference's shared/ modules and cited where they appear. The step itself is a CUDA graph
 // per block of steps: one replay launches every kernel of every step of every system.
 #include <algorithm>
+#include <array>
 #include <cmath>
+#include <functional>
+#include <map>
+#include <mutex>
 #include <cstdio>
 #include <cstring>
 #include <map>
@@ -158,6 +162,8 @@ struct Engine {
   cudaStream_t stream = nullptr;
   std::string last_error;
   int nb_lanes = 32;
+  int group_atoms = 8;   // atoms per neighbour-search warp
+  int spread_atoms = 8;  // atoms per PME spreading block
   int pair_fixed = 1;
   int pme_order = 5;
   bool pme_on = true;
@@ -173,6 +179,8 @@ struct Engine {
   DevArray<float4> exc_param;
   DevArray<int> cell_of_atom, cell_count, cell_start, cell_atoms, cell_sys;
   int n_cells_total = 0;
+  DevArray<int> cell_gstart, group_order, group_sys;
+  int n_groups_total = 0;
   DevArray<int> nbr, nbr_count, required;
   DevArray<float4> spos, wrap;
   DevArray<int> sorted_orig, sorted_type, rank;
@@ -236,6 +244,11 @@ struct Engine {
   void evaluate(bool rebuild, bool energy);
   void set_state(int s, const double *pos, const double *vel, int64_t step, int supplied);
   void initialise();
+  // kernel-shape autotuner: which shapes were left to it, and what it measured
+  bool tune_group = false, tune_lanes = false, tune_spread = false;
+  double tune_ms[9] = {-1, -1, -1, -1, -1, -1, -1, -1, -1};
+  void autotune();
+  void drop_graphs();
   int check_capacity();  // returns max required; grows if needed
   void run(int64_t count, int block, const volatile int32_t *stop);
   void run_block(int n, bool barostat, bool energy_last);
@@ -308,6 +321,7 @@ void Engine::plan_system(HostSystem &h, const rmd_system &s) {
   const double slack = o.neighbour_slack > 0 ? o.neighbour_slack : 2.0;
   h.capacity = o.max_neighbours > 0 ? o.max_neighbours
                                     : std::max(32, (int)std::ceil(h.estimated_neighbours * slack));
+  h.capacity = (h.capacity + 3) & ~3;  // rows start on 16-byte boundaries
   // pmeParameters (parameters.js:227-252)
   const double tol = o.ewald_tolerance > 0 ? o.ewald_tolerance : 5e-4;
   h.alpha = o.alpha > 0 ? o.alpha : alpha_from_tolerance(h.cutoff, tol);
@@ -399,6 +413,16 @@ void Engine::build(int count, const rmd_system *systems, const rmd_options *opti
   }
   pme_order = hs[0].order;
   pair_fixed = options[0].force_accumulation == 1 ? 0 : 1;
+  {
+    const rmd_options &o = options[0];
+    auto pick = [](int v, int a, int b, int c, int dflt) { return v == a || v == b || v == c ? v : dflt; };
+    group_atoms = pick(o.neighbour_group_atoms, 8, 16, 32, 8);
+    nb_lanes = pick(o.nonbonded_lanes, 8, 16, 32, 32);
+    spread_atoms = pick(o.spread_atoms_per_block, 4, 8, 16, 8);
+    tune_group = o.neighbour_group_atoms == 0;
+    tune_lanes = o.nonbonded_lanes == 0;
+    tune_spread = o.spread_atoms_per_block == 0;
+  }
   for (auto &h : hs)
     if (h.order != pme_order) throw Error(RMD_ERR_INVALID, "every system of a batch must use the same PME order");
   CUDA_OK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
@@ -707,7 +731,7 @@ void Engine::upload_all(const std::vector<const rmd_system *> &src) {
   }
 
   // ---- cells
-  std::vector<int> h_cell_sys;
+  std::vector<int> h_cell_sys, h_group_sys;
   h_sys.resize(S);
   h_sysd.resize(S);
   int cell_base = 0, cell_start_base = 0;
@@ -735,6 +759,10 @@ void Engine::upload_all(const std::vector<const rmd_system *> &src) {
     d.cell_start_base = cell_start_base;
     d.cell_capacity = cells;
     for (int c = 0; c < cells; ++c) h_cell_sys.push_back(s);
+    // search groups: at most ceil(n / 32) full ones plus one partial group per cell
+    d.group_base = (int)h_group_sys.size();
+    const int groups = neighbour_group_slots(h.n, cells, 8);  // enough for every group size
+    for (int q = 0; q < groups; ++q) h_group_sys.push_back(s);
     cell_base += cells;
     cell_start_base += cells + 1;
     d.order = h.order;
@@ -755,6 +783,11 @@ void Engine::upload_all(const std::vector<const rmd_system *> &src) {
   cell_count.zero();
   cell_start.alloc(cell_start_base);
   cell_start.zero();
+  cell_gstart.alloc(cell_start_base);
+  cell_gstart.zero();
+  n_groups_total = (int)h_group_sys.size();
+  group_sys.upload(h_group_sys);
+  group_order.alloc(N);
   cell_atoms.alloc(N);
   cell_of_atom.alloc(N);
   spos.alloc(N);
@@ -939,6 +972,12 @@ LaunchCtx Engine::ctx() const {
   c.cell_atoms = cell_atoms.p;
   c.cell_sys = cell_sys.p;
   c.n_cells_total = n_cells_total;
+  c.cell_gstart = cell_gstart.p;
+  c.group_order = group_order.p;
+  c.group_sys = group_sys.p;
+  c.n_groups_total = n_groups_total;
+  c.group_atoms = group_atoms;
+  c.spread_atoms = spread_atoms;
   c.excl_start = excl_start.p;
   c.excl_partners = excl_partners.p;
   c.nbr = nbr.p;
@@ -1121,7 +1160,7 @@ int Engine::check_capacity() {
     hs[s].worst_required = std::max(hs[s].worst_required, req[s]);
     worst = std::max(worst, req[s]);
     if (req[s] > hs[s].capacity) {  // grownPlan (cells.js:282-288)
-      hs[s].capacity = std::max(hs[s].capacity + 32, (int)std::ceil(req[s] * 1.25));
+      hs[s].capacity = (std::max(hs[s].capacity + 32, (int)std::ceil(req[s] * 1.25)) + 3) & ~3;
       hs[s].neighbour_growths++;
       grow = true;
     }
@@ -1143,11 +1182,113 @@ int Engine::check_capacity() {
   return worst;
 }
 
+void Engine::drop_graphs() {
+  for (auto &kv : graphs) cudaGraphExecDestroy(kv.second);
+  graphs.clear();
+  graph_launches.clear();
+}
+
+namespace {
+// Shapes chosen per workload, kept for the life of the process so that engines of the same
+// shape (a benchmark's repeated runs, a batch rebuilt after a restart) tune once.
+std::mutex g_tune_mutex;
+std::map<std::string, std::array<int, 3>> g_tuned;
+}  // namespace
+
+// The kernel-shape autotuner. Three launch shapes change speed but not results (neighbour
+// rows are the same for every group size; fixed-point pair forces and the fixed-point charge
+// grid are independent of summation order): atoms per neighbour-search warp (8, 16, 32),
+// lanes per atom in the pair loop (8, 16, 32) and atoms per spreading block (4, 8, 16).
+// Each candidate is timed with CUDA events on the engine's stream over a few launches on the
+// engine's own current state, the fastest is kept, and the choice is cached by workload
+// shape (atoms, systems, cells, PME grids and order, accumulation mode).
+void Engine::autotune() {
+  if (!(tune_group || tune_lanes || tune_spread)) return;
+  std::string key = std::to_string(S) + ":" + std::to_string(N) + ":" + std::to_string(n_cells_total) + ":" +
+                    std::to_string(pme_order) + ":" + std::to_string(pair_fixed);
+  for (auto &h : hs) key += ":" + std::to_string(h.grid[0] * 100000LL + h.grid[1] * 1000LL + h.grid[2]);
+  {
+    std::lock_guard<std::mutex> lock(g_tune_mutex);
+    auto it = g_tuned.find(key);
+    if (it != g_tuned.end()) {
+      if (tune_group) group_atoms = it->second[0];
+      if (tune_lanes) nb_lanes = it->second[1];
+      if (tune_spread) spread_atoms = it->second[2];
+      drop_graphs();
+      return;
+    }
+  }
+  cudaEvent_t a, b;
+  CUDA_OK(cudaEventCreate(&a));
+  CUDA_OK(cudaEventCreate(&b));
+  auto time = [&](const std::function<void()> &one) {
+    constexpr int reps = 5;
+    one();  // warm
+    CUDA_OK(cudaEventRecord(a, stream));
+    for (int k = 0; k < reps; ++k) one();
+    CUDA_OK(cudaEventRecord(b, stream));
+    CUDA_OK(cudaEventSynchronize(b));
+    float ms = 0;
+    CUDA_OK(cudaEventElapsedTime(&ms, a, b));
+    return (double)ms / reps;
+  };
+  const int groups[3] = {8, 16, 32}, lanes[3] = {8, 16, 32}, spreads[3] = {4, 8, 16};
+  if (tune_group) {
+    double best = 1e30;
+    int pick = group_atoms;
+    for (int k = 0; k < 3; ++k) {
+      group_atoms = groups[k];
+      const LaunchCtx c = ctx();
+      tune_ms[k] = time([&]() { launch_rebuild(c, stream); });
+      if (tune_ms[k] < best) best = tune_ms[k], pick = groups[k];
+    }
+    group_atoms = pick;
+    // leave the lists as the chosen shape builds them (they are the same for every shape)
+    const LaunchCtx c = ctx();
+    launch_rebuild(c, stream);
+  }
+  if (tune_lanes) {
+    double best = 1e30;
+    int pick = nb_lanes;
+    const LaunchCtx c = ctx();
+    for (int k = 0; k < 3; ++k) {
+      tune_ms[3 + k] = time([&]() { launch_nonbonded(c, false, lanes[k], stream); });
+      if (tune_ms[3 + k] < best) best = tune_ms[3 + k], pick = lanes[k];
+    }
+    nb_lanes = pick;
+  }
+  if (tune_spread && pme_on) {
+    double best = 1e30;
+    int pick = spread_atoms;
+    for (int k = 0; k < 3; ++k) {
+      spread_atoms = spreads[k];
+      const LaunchCtx c = ctx();
+      tune_ms[6 + k] = time([&]() { launch_spread_only(c, stream); });
+      if (tune_ms[6 + k] < best) best = tune_ms[6 + k], pick = spreads[k];
+    }
+    spread_atoms = pick;
+    CUDA_OK(cudaMemsetAsync(fixed_grid.p, 0, fixed_grid.bytes(), stream));  // the z pass expects it clear
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  CUDA_OK(cudaGetLastError());
+  sync();
+  {
+    std::lock_guard<std::mutex> lock(g_tune_mutex);
+    g_tuned[key] = {group_atoms, nb_lanes, spread_atoms};
+  }
+  drop_graphs();
+}
+
 void Engine::initialise() {
   evaluate(true, false);
   sync();
   for (auto &h : hs) h.steps_since_rebuild = 0;
   check_capacity();
+  autotune();
+  // the forces (accumulated into by the timed pair-loop launches) from a clean evaluation
+  evaluate(false, false);
+  sync();
   // kinetic energies of the current velocities, for energy() before any step
   launch_integrate(iargs(0), INT_CLOSE_KINETIC, stream);
   kernel_launches += 1;
@@ -2021,6 +2162,33 @@ rmd_status rmd_debug_time_kernel(rmd_sim *sim, int32_t which, int32_t reps, doub
 }
 
 int64_t rmd_debug_kernel_launches(const rmd_sim *sim) { return sim ? sim->engine.kernel_launches : 0; }
+
+rmd_status rmd_kernel_shapes(const rmd_sim *sim, int32_t shapes[3], double tune_ms[9]) {
+  if (!sim) return RMD_ERR_INVALID;
+  const auto &e = sim->engine;
+  if (shapes) {
+    shapes[0] = e.group_atoms;
+    shapes[1] = e.nb_lanes;
+    shapes[2] = e.spread_atoms;
+  }
+  if (tune_ms)
+    for (int k = 0; k < 9; ++k) tune_ms[k] = e.tune_ms[k];
+  return RMD_OK;
+}
+
+rmd_status rmd_set_kernel_shapes(rmd_sim *sim, int32_t group_atoms, int32_t nonbonded_lanes,
+                                 int32_t spread_atoms) {
+  if (!sim) return RMD_ERR_INVALID;
+  auto ok = [](int v, int a, int b, int c) { return v == 0 || v == a || v == b || v == c; };
+  if (!ok(group_atoms, 8, 16, 32) || !ok(nonbonded_lanes, 8, 16, 32) || !ok(spread_atoms, 4, 8, 16))
+    return RMD_ERR_INVALID;
+  auto &e = sim->engine;
+  if (group_atoms) e.group_atoms = group_atoms;
+  if (nonbonded_lanes) e.nb_lanes = nonbonded_lanes;
+  if (spread_atoms) e.spread_atoms = spread_atoms;
+  e.drop_graphs();
+  return RMD_OK;
+}
 
 rmd_status rmd_debug_set_nonbonded(rmd_sim *sim, int32_t lanes, int32_t pair_fixed) {
   if (!sim || (lanes != 8 && lanes != 16 && lanes != 32)) return RMD_ERR_INVALID;

@@ -83,6 +83,12 @@ struct LaunchCtx {
   // lists
   int *cell_of_atom, *cell_count, *cell_start, *cell_atoms, *cell_sys;
   int n_cells_total;
+  // neighbour-search groups: per cell the first group (scan of ceil(count / 32), indexed like
+  // cell_start), the cell's slots in sub-cell order, and the system of each group slot
+  int *cell_gstart, *group_order;
+  const int *group_sys;
+  int n_groups_total;
+  int group_atoms;  // atoms per neighbour-search group: 8, 16 or 32
   const int *excl_start, *excl_partners;
   int *nbr, *nbr_count, *required;
   float4 *origin;
@@ -115,6 +121,7 @@ struct LaunchCtx {
   double *e_term;
   // pme
   int pme_on, pme_order;
+  int spread_atoms;  // atoms per spreading block: 4, 8 or 16
   unsigned long long *fixed_grid;
   float2 *half;
   float *real_grid;
@@ -127,6 +134,8 @@ struct LaunchCtx {
 };
 
 void launch_rebuild(const LaunchCtx &c, cudaStream_t stream);
+// group slots a system needs for a given group size (its search groups never exceed this)
+int neighbour_group_slots(int atoms, int cells, int group_atoms);
 void launch_nonbonded(const LaunchCtx &c, bool energy, int lanes, cudaStream_t stream);
 void launch_bonded(const LaunchCtx &c, bool energy, cudaStream_t stream);
 void launch_pme(const LaunchCtx &c, bool energy, cudaStream_t stream);

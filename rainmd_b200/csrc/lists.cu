@@ -8,9 +8,12 @@
 //   - the histogram and the scatter use integer atomics, and a per-cell block rank-sort
 //     (shared memory) restores the deterministic index order;
 //   - the scan is one block per system;
-//   - the neighbour search is one WARP per atom: lanes test 32 candidates of a cell at
-//     once and a ballot/popc prefix compacts the survivors in order, so the list order
-//     equals the sequential one without any per-atom serial loop.
+//   - the neighbour search is one WARP per group of 8, 16 or 32 spatially close atoms of a
+//     cell: the group's bounding box culls stencil cells and candidates once for all its
+//     atoms, the survivors are staged in shared memory, and each atom's lanes append its
+//     hits in candidate order, so every row's order equals the sequential one.
+#include <climits>
+
 #include "common.cuh"
 #include "kernels.h"
 
@@ -22,6 +25,7 @@ struct LaunchCtxView {
   float4 *spos;
   float4 *wrap;
   int *sorted_orig, *sorted_type, *rank;
+  int *group_order;
 };
 
 __global__ void k_cells_assign(const float4 *__restrict__ posq, const int *__restrict__ sys_of_atom,
@@ -37,47 +41,61 @@ __global__ void k_cells_assign(const float4 *__restrict__ posq, const int *__res
   atomicAdd(&cell_count[s.cell_base + cell], 1);
 }
 
-// One block per system: exclusive scan of the counts into cell_start, count -> 0.
-__global__ void k_cells_scan(const DevSys *__restrict__ sys, int *__restrict__ cell_count,
-                             int *__restrict__ cell_start) {
-  const DevSys &s = sys[blockIdx.x];
-  const int cells = s.cell_counts[0] * s.cell_counts[1] * s.cell_counts[2];
-  __shared__ int warp_totals[32];
-  __shared__ int running;
-  if (threadIdx.x == 0) running = 0;
-  __syncthreads();
+// Block-wide exclusive scan step over one chunk of blockDim.x values; returns the value's
+// exclusive prefix within the chunk and leaves the chunk total in *total.
+__device__ __forceinline__ int block_exclusive_scan(int v, int *warp_totals, int *total) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
-  for (int chunk = 0; chunk < cells; chunk += blockDim.x) {
-    int c = chunk + threadIdx.x;
-    int v = c < cells ? cell_count[s.cell_base + c] : 0;
-    int x = v;
+  int x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) warp_totals[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    int t = lane < warps ? warp_totals[lane] : 0;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
-      int y = __shfl_up_sync(0xffffffffu, x, o);
-      if (lane >= o) x += y;
+      int y = __shfl_up_sync(0xffffffffu, t, o);
+      if (lane >= o) t += y;
     }
-    if (lane == 31) warp_totals[warp] = x;
-    __syncthreads();
-    if (warp == 0) {
-      int t = lane < warps ? warp_totals[lane] : 0;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        int y = __shfl_up_sync(0xffffffffu, t, o);
-        if (lane >= o) t += y;
-      }
-      warp_totals[lane] = t;  // inclusive over warps
-    }
-    __syncthreads();
-    int before = (warp > 0 ? warp_totals[warp - 1] : 0) + x - v;
+    warp_totals[lane] = t;  // inclusive over warps
+  }
+  __syncthreads();
+  const int before = (warp > 0 ? warp_totals[warp - 1] : 0) + x - v;
+  *total = warp_totals[warps - 1];
+  __syncthreads();
+  return before;
+}
+
+// One block per system: exclusive scans of the counts into cell_start and of the number
+// of neighbour-search groups per cell (ceil(count / group_atoms)) into cell_gstart;
+// count -> 0.
+__global__ void k_cells_scan(const DevSys *__restrict__ sys, int *__restrict__ cell_count,
+                             int *__restrict__ cell_start, int *__restrict__ cell_gstart, int group_atoms) {
+  const DevSys &s = sys[blockIdx.x];
+  const int cells = s.cell_counts[0] * s.cell_counts[1] * s.cell_counts[2];
+  __shared__ int warp_totals[2][32];
+  int running = 0, running_groups = 0;
+  for (int chunk = 0; chunk < cells; chunk += blockDim.x) {
+    const int c = chunk + threadIdx.x;
+    const int v = c < cells ? cell_count[s.cell_base + c] : 0;
+    int total, total_groups;
+    const int before = block_exclusive_scan(v, warp_totals[0], &total);
+    const int before_groups = block_exclusive_scan((v + group_atoms - 1) / group_atoms, warp_totals[1], &total_groups);
     if (c < cells) {
       cell_start[s.cell_start_base + c] = running + before;
+      cell_gstart[s.cell_start_base + c] = running_groups + before_groups;
       cell_count[s.cell_base + c] = 0;
     }
-    __syncthreads();
-    if (threadIdx.x == 0) running += warp_totals[warps - 1];
-    __syncthreads();
+    running += total;
+    running_groups += total_groups;
   }
-  if (threadIdx.x == 0) cell_start[s.cell_start_base + cells] = running;
+  if (threadIdx.x == 0) {
+    cell_start[s.cell_start_base + cells] = running;
+    cell_gstart[s.cell_start_base + cells] = running_groups;
+  }
 }
 
 __global__ void k_cells_scatter(const int *__restrict__ sys_of_atom, const DevSys *__restrict__ sys,
@@ -94,13 +112,22 @@ __global__ void k_cells_scatter(const int *__restrict__ sys_of_atom, const DevSy
 
 // Write slot g's cell-ordered record for atom j: its position shifted into the box by
 // whole box vectors (the shift is kept per atom so the integrator can apply it every step).
-__device__ __forceinline__ void place_sorted(const LaunchCtxView &v, const DevSys &s, int g, int j) {
+// Returns the atom's sub-cell key: the Morton code of its position on a 4x4x4 grid inside
+// its cell (the order in which the neighbour search groups a cell's atoms).
+__device__ __forceinline__ int place_sorted(const LaunchCtxView &v, const DevSys &s, int g, int j,
+                                            const int cc[3]) {
   const float4 p = v.posq[j];
   // floor of the same exact-rounding fractional coordinate the cell assignment used, so the
   // wrapped copy lies in (the closure of) the cell the atom was counted in
   float fl[3];
+  int sub[3];
 #pragma unroll
-  for (int d = 0; d < 3; ++d) fl[d] = floorf(frac_exact(make_float3(p.x, p.y, p.z), s, d));
+  for (int d = 0; d < 3; ++d) {
+    const float f = frac_exact(make_float3(p.x, p.y, p.z), s, d);
+    fl[d] = floorf(f);
+    const float inside = (f - fl[d]) * (float)s.cell_counts[d] - (float)cc[d];
+    sub[d] = min(3, max(0, (int)(inside * 4.f)));
+  }
   const float wx = fl[0] * s.box[0] + fl[1] * s.box[3] + fl[2] * s.box[6];
   const float wy = fl[0] * s.box[1] + fl[1] * s.box[4] + fl[2] * s.box[7];
   const float wz = fl[0] * s.box[2] + fl[1] * s.box[5] + fl[2] * s.box[8];
@@ -109,10 +136,13 @@ __device__ __forceinline__ void place_sorted(const LaunchCtxView &v, const DevSy
   v.sorted_orig[g] = j;
   v.sorted_type[g] = v.atom_type[j];
   v.rank[j] = g;
+  auto spread = [](int b) { return (b & 1) | ((b & 2) << 2); };
+  return (spread(sub[0]) << 2) | (spread(sub[1]) << 1) | spread(sub[2]);
 }
 
-// One block per allocated cell: rank-sort the cell's slice ascending, zero the cursor, and
-// write the cell-ordered records of its atoms.
+// One block per allocated cell: rank-sort the cell's slice ascending, zero the cursor, write
+// the cell-ordered records of its atoms, and order the cell's slots by sub-cell key (ties by
+// slot) into group_order, so that 32 consecutive entries there are spatially compact.
 __global__ void k_cells_sort(const int *__restrict__ cell_sys, const DevSys *__restrict__ sys,
                              const int *__restrict__ cell_start, int *__restrict__ cell_cursor,
                              int *__restrict__ cell_atoms, LaunchCtxView v) {
@@ -125,10 +155,13 @@ __global__ void k_cells_sort(const int *__restrict__ cell_sys, const DevSys *__r
   const int begin = cell_start[s.cell_start_base + c], end = cell_start[s.cell_start_base + c + 1];
   const int n = end - begin;
   if (n <= 0) return;
+  const int cc[3] = {c / (s.cell_counts[1] * s.cell_counts[2]), (c / s.cell_counts[2]) % s.cell_counts[1],
+                     c % s.cell_counts[2]};
   int *slice = cell_atoms + s.atom_start + begin;
   const int gbase = s.atom_start + begin;
   constexpr int SMEM = 2048;
   __shared__ int keys[SMEM];
+  __shared__ int sub_keys[SMEM];
   if (n <= SMEM) {
     for (int k = threadIdx.x; k < n; k += blockDim.x) keys[k] = slice[k];
     __syncthreads();
@@ -136,10 +169,17 @@ __global__ void k_cells_sort(const int *__restrict__ cell_sys, const DevSys *__r
       int key = keys[k], rank = 0;
       for (int m = 0; m < n; ++m) rank += keys[m] < key;
       slice[rank] = key;
-      place_sorted(v, s, gbase + rank, key);
+      sub_keys[rank] = (place_sorted(v, s, gbase + rank, key, cc) << 11) | rank;
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < n; k += blockDim.x) {
+      int key = sub_keys[k], rank = 0;
+      for (int m = 0; m < n; ++m) rank += sub_keys[m] < key;
+      v.group_order[gbase + rank] = gbase + k;
     }
   } else {
-    // Oversized cell (only in pathological inputs): serial insertion sort by one thread.
+    // Oversized cell (only in pathological inputs): serial insertion sort by one thread;
+    // the groups then follow slot order.
     if (threadIdx.x == 0) {
       for (int a = 1; a < n; ++a) {
         int key = slice[a], b = a;
@@ -151,7 +191,10 @@ __global__ void k_cells_sort(const int *__restrict__ cell_sys, const DevSys *__r
       }
     }
     __syncthreads();
-    for (int k = threadIdx.x; k < n; k += blockDim.x) place_sorted(v, s, gbase + k, slice[k]);
+    for (int k = threadIdx.x; k < n; k += blockDim.x) {
+      place_sorted(v, s, gbase + k, slice[k], cc);
+      v.group_order[gbase + k] = gbase + k;
+    }
   }
 }
 
@@ -167,31 +210,83 @@ __device__ __forceinline__ bool is_excluded(const int *__restrict__ start, const
   return false;
 }
 
-// One warp per atom, atoms visited in cell order: the full neighbour row within the list
-// cutoff, in the reference's stencil order. Candidates of a cell are read as one coalesced
-// run of the cell-ordered records. With at least three cells per axis every stencil cell
-// is reached through one known lattice shift (no per-candidate minimum image) and, in a
-// rectangular box, cells entirely beyond the list cutoff are skipped. Membership near the
-// cutoff is decided by the exact-rounding test of the reference's WGSL on the original
-// coordinates, so rows are bit-identical to the reference's. An entry is the partner's
-// cell-ordered slot with the code of the lattice shift to its nearest image.
-__global__ void k_neighbours(const float4 *__restrict__ posq, const int *__restrict__ sys_of_atom,
-                             const DevSys *__restrict__ sys, const int *__restrict__ cell_start,
-                             const int *__restrict__ excl_start, const int *__restrict__ excl_partners,
-                             const float4 *__restrict__ spos, const int *__restrict__ sorted_orig,
-                             int *__restrict__ nbr, int *__restrict__ nbr_count, int *__restrict__ required,
-                             float4 *__restrict__ origin, int n_atoms) {
-  const int si = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+constexpr int NBR_WARPS = 4;
+
+// One WARP per search group of G atoms of one cell, taken in sub-cell order so the group is
+// spatially compact; lane l works for the group's atom l / J on candidate sub-lane l % J
+// (J = 32 / G). The group walks the reference's stencil once for all its atoms: per stencil
+// cell (skipped when the cell's box is beyond the list cutoff from the group's bounding
+// box), 32 candidates at a time are read as one coalesced run of the cell-ordered records,
+// those beyond the list cutoff from the bounding box are dropped, and the survivors are
+// staged in shared memory; then each atom's J lanes test J survivors at a time and append
+// the hits with a prefix count over those J lanes, so every row keeps the reference's
+// order: stencil cell by stencil cell, partners ascending by index within a cell. With at
+// least three cells per axis every stencil cell is reached through one known lattice shift
+// (no per-candidate minimum image). Membership near the cutoff is decided by the
+// exact-rounding test of the reference's WGSL on the original coordinates, so rows are
+// bit-identical to the reference's. An entry is the partner's cell-ordered slot with the
+// code of the lattice shift to its nearest image.
+template <int G>
+__global__ void __launch_bounds__(32 * NBR_WARPS)
+    k_neighbours(const float4 *__restrict__ posq, const int *__restrict__ group_sys,
+                 const DevSys *__restrict__ sys, const int *__restrict__ cell_start,
+                 const int *__restrict__ cell_gstart, const int *__restrict__ group_order,
+                 const int *__restrict__ excl_start, const int *__restrict__ excl_partners,
+                 const float4 *__restrict__ spos, const int *__restrict__ sorted_orig,
+                 int *__restrict__ nbr, int *__restrict__ nbr_count, int *__restrict__ required,
+                 float4 *__restrict__ origin, int n_groups) {
+  constexpr int J = 32 / G;
+  __shared__ float4 stage_pos[NBR_WARPS][32];
+  __shared__ int stage_orig[NBR_WARPS][32];
+  const int wib = threadIdx.x >> 5;
+  const int warp = blockIdx.x * NBR_WARPS + wib;
   const int lane = threadIdx.x & 31;
-  if (si >= n_atoms) return;
-  const int i = sorted_orig[si];
-  const int sidx = sys_of_atom[i];
+  const int a = lane / J, sub = lane % J;
+  if (warp >= n_groups) return;
+  const int sidx = group_sys[warp];
   const DevSys &s = sys[sidx];
-  const float4 po = posq[i];
-  const float4 pw = spos[si];
-  if (lane == 0) origin[i] = po;  // displacement origin for the skin check
-  const int3 c = cell_coord(make_float3(po.x, po.y, po.z), s);
+  const int q = warp - s.group_base;
   const int counts[3] = {s.cell_counts[0], s.cell_counts[1], s.cell_counts[2]};
+  const int cells = counts[0] * counts[1] * counts[2];
+  const int *gstart = cell_gstart + s.cell_start_base;
+  if (q >= gstart[cells]) return;
+  // the cell holding group q: gstart[c] <= q < gstart[c + 1]
+  int lo = 0, hi = cells;
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (gstart[mid] <= q) lo = mid; else hi = mid;
+  }
+  const int cell0 = lo;
+  const int cbegin = s.atom_start + cell_start[s.cell_start_base + cell0];
+  const int cend = s.atom_start + cell_start[s.cell_start_base + cell0 + 1];
+  const int k = cbegin + (q - gstart[cell0]) * G + a;
+  const bool valid = k < cend;
+  const int si = valid ? group_order[k] : -1;
+  const int i = valid ? sorted_orig[si] : 0;
+  const float4 pw = valid ? spos[si] : make_float4(0.f, 0.f, 0.f, 0.f);
+  const float4 po = valid ? posq[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+  if (valid && sub == 0) origin[i] = po;  // displacement origin for the skin check
+  // exclusions of this lane's atom: sorted partners; the range check skips the search
+  const int e_lo = valid ? excl_start[i] : 0, e_hi = valid ? excl_start[i + 1] : 0;
+  const int p_min = e_lo < e_hi ? excl_partners[e_lo] : INT_MAX;
+  const int p_max = e_lo < e_hi ? excl_partners[e_hi - 1] : INT_MIN;
+  // the group's bounding box (wrapped coordinates)
+  float blo[3], bhi[3];
+  {
+    const float c[3] = {pw.x, pw.y, pw.z};
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      float lo_d = valid ? c[d] : INFINITY, hi_d = valid ? c[d] : -INFINITY;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        lo_d = fminf(lo_d, __shfl_xor_sync(0xffffffffu, lo_d, o));
+        hi_d = fmaxf(hi_d, __shfl_xor_sync(0xffffffffu, hi_d, o));
+      }
+      blo[d] = lo_d;
+      bhi[d] = hi_d;
+    }
+  }
+  const int cc[3] = {cell0 / (counts[1] * counts[2]), (cell0 / counts[2]) % counts[1], cell0 % counts[2]};
   int base[3], count[3];
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
@@ -201,13 +296,17 @@ __global__ void k_neighbours(const float4 *__restrict__ posq, const int *__restr
   const bool stencil_shift = counts[0] >= 3 && counts[1] >= 3 && counts[2] >= 3;
   const bool rectangular = s.box[3] == 0.f && s.box[6] == 0.f && s.box[7] == 0.f;
   const float wcell[3] = {s.box[0] / counts[0], s.box[4] / counts[1], s.box[8] / counts[2]};
-  const int cc[3] = {c.x, c.y, c.z};
   const float lc2 = s.list_cutoff2;
-  const float band_hi = lc2 * 1.00001f, band_lo = lc2 * 0.99999f;
+  // the fast test below is within a few 1e-6 of lc2 relative: the band around it goes to the
+  // exact test; culling keeps a further margin
+  const float band_hi = lc2 * 1.00004f, band_lo = lc2 * 0.99996f, cull2 = band_hi * 1.0001f;
   const int cap = s.nbr_capacity;
-  int *row = nbr + s.nbr_base + (long long)(si - s.atom_start) * cap;
-  int stored = 0, found = 0;
-  const unsigned lt = (1u << lane) - 1u;
+  int *row = nbr + s.nbr_base + (long long)(valid ? si - s.atom_start : 0) * cap;
+  int found = 0;
+  const unsigned seg_mask = J == 32 ? 0xffffffffu : ((1u << J) - 1u);
+  const unsigned below = (1u << sub) - 1u;
+  float4 *st_pos = stage_pos[wib];
+  int *st_orig = stage_orig[wib];
   for (int ox = 0; ox < count[0]; ++ox) {
     const int rx = cc[0] + base[0] + ox;
     const int wx = rx < 0 ? -1 : (rx >= counts[0] ? 1 : 0);
@@ -226,83 +325,126 @@ __global__ void k_neighbours(const float4 *__restrict__ posq, const int *__restr
         if (stencil_shift) {
           code = shift_code(wx, wy, wz);
           S = s.shift[code];
-          if (rectangular) {  // skip a cell whose nearest point is beyond the list cutoff
-            const float lo[3] = {rx * wcell[0], ry * wcell[1], rz * wcell[2]};
-            const float p[3] = {pw.x, pw.y, pw.z};
+          if (rectangular) {  // skip a cell whose box is beyond the list cutoff from the group's
+            const float r[3] = {(float)rx, (float)ry, (float)rz};
             float d2 = 0.f;
 #pragma unroll
             for (int d = 0; d < 3; ++d) {
-              const float e = fmaxf(fmaxf(lo[d] - p[d], p[d] - (lo[d] + wcell[d])), 0.f);
+              const float clo = r[d] * wcell[d], chi = clo + wcell[d];
+              const float e = fmaxf(fmaxf(clo - bhi[d], blo[d] - chi), 0.f);
               d2 = fmaf(e, e, d2);
             }
-            if (d2 > band_hi * 1.0001f) continue;
+            if (d2 > cull2) continue;
           }
         }
+        // the bounding box seen from the unshifted copies of this cell's atoms
+        const float slo[3] = {blo[0] - S.x, blo[1] - S.y, blo[2] - S.z};
+        const float shi[3] = {bhi[0] - S.x, bhi[1] - S.y, bhi[2] - S.z};
         const int begin = s.atom_start + cell_start[s.cell_start_base + cell];
         const int end = s.atom_start + cell_start[s.cell_start_base + cell + 1];
         for (int b = begin; b < end; b += 32) {
           const int g = b + lane;
-          bool ok = g < end;
-          int j = -1, jcode = code;
-          if (ok) {
-            j = sorted_orig[g];
-            ok = j != i;
-          }
-          if (ok) {
-            const float4 pj = spos[g];
-            float3 d = make_float3(pw.x - pj.x - S.x, pw.y - pj.y - S.y, pw.z - pj.z - S.z);
-            if (!stencil_shift) {
-              const float kc = rintf(d.z * s.inv_diag[2]);
-              d.x = fmaf(-kc, s.box[6], d.x); d.y = fmaf(-kc, s.box[7], d.y); d.z = fmaf(-kc, s.box[8], d.z);
-              const float kb = rintf(d.y * s.inv_diag[1]);
-              d.x = fmaf(-kb, s.box[3], d.x); d.y = fmaf(-kb, s.box[4], d.y);
-              const float ka = rintf(d.x * s.inv_diag[0]);
-              d.x = fmaf(-ka, s.box[0], d.x);
-              jcode = shift_code(max(-1, min(1, (int)ka)), max(-1, min(1, (int)kb)), max(-1, min(1, (int)kc)));
-            }
-            const float r2 = fmaf(d.x, d.x, fmaf(d.y, d.y, d.z * d.z));
-            if (r2 > band_hi) ok = false;
-            else if (r2 < band_lo) ok = true;
-            else {
-              const float4 qj = posq[j];
-              const float3 d0 = make_float3(__fsub_rn(po.x, qj.x), __fsub_rn(po.y, qj.y), __fsub_rn(po.z, qj.z));
-              ok = !(dot_exact(min_image_exact(d0, s)) > lc2);
+          bool keep = g < end;
+          float4 pj = make_float4(0.f, 0.f, 0.f, 0.f);
+          if (keep) {
+            pj = spos[g];
+            if (stencil_shift) {  // drop candidates beyond the list cutoff from the bounding box
+              const float c[3] = {pj.x, pj.y, pj.z};
+              float d2 = 0.f;
+#pragma unroll
+              for (int d = 0; d < 3; ++d) {
+                const float e = fmaxf(fmaxf(slo[d] - c[d], c[d] - shi[d]), 0.f);
+                d2 = fmaf(e, e, d2);
+              }
+              keep = d2 <= cull2;
             }
           }
-          if (ok) ok = !is_excluded(excl_start, excl_partners, i, j);
-          const unsigned mask = __ballot_sync(0xffffffffu, ok);
-          const int rank = __popc(mask & lt);
-          if (ok && stored + rank < cap)
-            row[stored + rank] = (int)((unsigned)g | ((unsigned)jcode << NBR_SLOT_BITS));
-          const int total = __popc(mask);
-          found += total;
-          stored = min(cap, stored + total);
+          const unsigned mask = __ballot_sync(0xffffffffu, keep);
+          if (keep) {
+            const int at = __popc(mask & ((1u << lane) - 1u));
+            st_pos[at] = make_float4(pj.x + S.x, pj.y + S.y, pj.z + S.z, __int_as_float(g));
+            st_orig[at] = sorted_orig[g];
+          }
+          __syncwarp();
+          const int survivors = __popc(mask);
+          for (int t = 0; t < survivors; t += J) {
+            const int tt = t + sub;
+            bool in = valid && tt < survivors;
+            int entry = 0;
+            if (in) {
+              const float4 c = st_pos[tt];
+              const int j = st_orig[tt];
+              const int gj = __float_as_int(c.w);
+              float3 d = make_float3(pw.x - c.x, pw.y - c.y, pw.z - c.z);
+              int jcode = code;
+              if (!stencil_shift) {
+                const float kc = rintf(d.z * s.inv_diag[2]);
+                d.x = fmaf(-kc, s.box[6], d.x); d.y = fmaf(-kc, s.box[7], d.y); d.z = fmaf(-kc, s.box[8], d.z);
+                const float kb = rintf(d.y * s.inv_diag[1]);
+                d.x = fmaf(-kb, s.box[3], d.x); d.y = fmaf(-kb, s.box[4], d.y);
+                const float ka = rintf(d.x * s.inv_diag[0]);
+                d.x = fmaf(-ka, s.box[0], d.x);
+                jcode = shift_code(max(-1, min(1, (int)ka)), max(-1, min(1, (int)kb)), max(-1, min(1, (int)kc)));
+              }
+              const float r2 = fmaf(d.x, d.x, fmaf(d.y, d.y, d.z * d.z));
+              in = r2 <= band_hi && gj != si;
+              if (in && r2 >= band_lo) {
+                const float4 qj = posq[j];
+                const float3 d0 = make_float3(__fsub_rn(po.x, qj.x), __fsub_rn(po.y, qj.y), __fsub_rn(po.z, qj.z));
+                in = !(dot_exact(min_image_exact(d0, s)) > lc2);
+              }
+              if (in && j >= p_min && j <= p_max) in = !is_excluded(excl_start, excl_partners, i, j);
+              entry = (int)((unsigned)gj | ((unsigned)jcode << NBR_SLOT_BITS));
+            }
+            const unsigned hits = (__ballot_sync(0xffffffffu, in) >> (a * J)) & seg_mask;
+            if (in) {
+              const int pos = found + __popc(hits & below);
+              if (pos < cap) row[pos] = entry;
+            }
+            found += __popc(hits);
+          }
+          __syncwarp();
         }
       }
     }
   }
-  if (lane == 0) {
-    nbr_count[si] = stored;
-    atomicMax(&required[sidx], found);
-  }
+  if (valid && sub == 0) nbr_count[si] = min(found, cap);
+  int most = valid ? found : 0;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) most = max(most, __shfl_xor_sync(0xffffffffu, most, o));
+  if (lane == 0) atomicMax(&required[sidx], most);
+}
+
+int neighbour_group_slots(int atoms, int cells, int group_atoms) {
+  return (atoms + group_atoms - 1) / group_atoms + cells;
 }
 
 void launch_rebuild(const LaunchCtx &ctx, cudaStream_t stream) {
   const int n = ctx.n_atoms;
   const int tb = 128;
+  const int G = ctx.group_atoms;
   k_cells_assign<<<(n + tb - 1) / tb, tb, 0, stream>>>(ctx.posq, ctx.sys_of_atom, ctx.sys,
                                                         ctx.cell_of_atom, ctx.cell_count, n);
-  k_cells_scan<<<ctx.n_systems, 1024, 0, stream>>>(ctx.sys, ctx.cell_count, ctx.cell_start);
+  k_cells_scan<<<ctx.n_systems, 1024, 0, stream>>>(ctx.sys, ctx.cell_count, ctx.cell_start, ctx.cell_gstart, G);
   k_cells_scatter<<<(n + tb - 1) / tb, tb, 0, stream>>>(ctx.sys_of_atom, ctx.sys, ctx.cell_of_atom,
                                                          ctx.cell_start, ctx.cell_count,
                                                          ctx.cell_atoms, n);
-  LaunchCtxView v{ctx.posq, ctx.atom_type, ctx.spos, ctx.wrap, ctx.sorted_orig, ctx.sorted_type, ctx.rank};
+  LaunchCtxView v{ctx.posq, ctx.atom_type, ctx.spos, ctx.wrap, ctx.sorted_orig, ctx.sorted_type, ctx.rank,
+                  ctx.group_order};
   k_cells_sort<<<ctx.n_cells_total, 128, 0, stream>>>(ctx.cell_sys, ctx.sys, ctx.cell_start,
                                                       ctx.cell_count, ctx.cell_atoms, v);
-  const int warps_per_block = 4;
-  k_neighbours<<<(n + warps_per_block - 1) / warps_per_block, 32 * warps_per_block, 0, stream>>>(
-      ctx.posq, ctx.sys_of_atom, ctx.sys, ctx.cell_start, ctx.excl_start, ctx.excl_partners, ctx.spos,
-      ctx.sorted_orig, ctx.nbr, ctx.nbr_count, ctx.required, ctx.origin, n);
+  const int blocks = (ctx.n_groups_total + NBR_WARPS - 1) / NBR_WARPS;
+#define RMD_NBR_ARGS                                                                                      \
+  ctx.posq, ctx.group_sys, ctx.sys, ctx.cell_start, ctx.cell_gstart, ctx.group_order, ctx.excl_start,  \
+      ctx.excl_partners, ctx.spos, ctx.sorted_orig, ctx.nbr, ctx.nbr_count, ctx.required, ctx.origin, \
+      ctx.n_groups_total
+  if (G == 8)
+    k_neighbours<8><<<blocks, 32 * NBR_WARPS, 0, stream>>>(RMD_NBR_ARGS);
+  else if (G == 16)
+    k_neighbours<16><<<blocks, 32 * NBR_WARPS, 0, stream>>>(RMD_NBR_ARGS);
+  else
+    k_neighbours<32><<<blocks, 32 * NBR_WARPS, 0, stream>>>(RMD_NBR_ARGS);
+#undef RMD_NBR_ARGS
 }
 
 }  // namespace rmd

@@ -32,10 +32,11 @@ __device__ __forceinline__ double group_sum(double v) {
   return v;
 }
 
-// PAIR_FIXED (the precision form): each pair force is quantised to 64-bit fixed point
-// before it is summed, so the atom's force is an exact integer sum and does not depend on
-// the order of its neighbour row (a rebuilt list, a resumed run, a different batch all give
-// the same bits). Without it (the plain form) lanes sum in f32 and convert once.
+// PAIR_FIXED (the precision form): each pair force (and, in the ENERGY variant, each pair
+// energy) is quantised to 64-bit fixed point (2^32 per unit) before it is summed, so the
+// atom's sums are exact integers and do not depend on the order of its neighbour row or on
+// the lanes per atom (a rebuilt list, a resumed run, a different batch or launch shape all
+// give the same bits). Without it (the plain form) lanes sum in f32 and convert once.
 template <bool ENERGY, int LANES, bool PAIR_FIXED>
 __global__ void __launch_bounds__(128) k_nonbonded(
     const float4 *__restrict__ posq, const float4 *__restrict__ spos, const int *__restrict__ sorted_orig,
@@ -64,7 +65,7 @@ __global__ void __launch_bounds__(128) k_nonbonded(
   const int *row = nbr + s.nbr_base + (long long)(si - s.atom_start) * s.nbr_capacity;
 
   float fx = 0.f, fy = 0.f, fz = 0.f, elj = 0.f, ecoul = 0.f;
-  long long qx = 0, qy = 0, qz = 0;
+  long long qx = 0, qy = 0, qz = 0, qlj = 0, qcoul = 0;
   for (int k = lane; k < count; k += LANES) {
     const unsigned e = (unsigned)__ldg(row + k);
     const int g = (int)(e & NBR_SLOT_MASK);
@@ -94,8 +95,13 @@ __global__ void __launch_bounds__(128) k_nonbonded(
         fz = fmaf(scalar, d.z, fz);
       }
       if (ENERGY) {
-        elj += a12 - b6;
-        ecoul = fmaf(qq * screened, inv_r, ecoul);
+        if (PAIR_FIXED) {
+          qlj += (long long)to_fixed(a12 - b6);
+          qcoul += (long long)to_fixed(qq * screened * inv_r);
+        } else {
+          elj += a12 - b6;
+          ecoul = fmaf(qq * screened, inv_r, ecoul);
+        }
       }
     }
   }
@@ -103,6 +109,7 @@ __global__ void __launch_bounds__(128) k_nonbonded(
   const int eb = exc_start[i], ee = valid ? exc_start[i + 1] : eb;
   const float4 pi = posq[i];
   for (int e = eb + lane; e < ee; e += LANES) {
+    float pair_lj = 0.f, pair_coul = 0.f;
     const int j = exc_partner[e];
     const float4 prm = exc_param[e];  // chargeProduct, ljA, ljB, fullProduct
     const float4 pj = posq[j];
@@ -114,12 +121,12 @@ __global__ void __launch_bounds__(128) k_nonbonded(
     if (prm.y != 0.f || prm.z != 0.f) {
       const float a12 = prm.y * inv_r6 * inv_r6, b6 = prm.z * inv_r6;
       scalar += (12.0f * a12 - 6.0f * b6) * inv_r2;
-      if (ENERGY) elj += a12 - b6;
+      if (ENERGY) pair_lj += a12 - b6;
     }
     if (prm.x != 0.f) {
       const float qq = (float)ONE_4PI_EPS0 * prm.x;
       scalar += qq * inv_r * inv_r2;
-      if (ENERGY) ecoul += qq * inv_r;
+      if (ENERGY) pair_coul += qq * inv_r;
     }
     if (alpha > 0.f && prm.w != 0.f) {
       const float qq = (float)ONE_4PI_EPS0 * prm.w;
@@ -127,7 +134,16 @@ __global__ void __launch_bounds__(128) k_nonbonded(
       const float r = r2 * inv_r;
       const float unscreened = 1.0f - erfc_and_gauss(alpha * r, gauss);
       scalar -= qq * (unscreened * inv_r - gauss_k * gauss) * inv_r2;
-      if (ENERGY) ecoul -= qq * unscreened * inv_r;
+      if (ENERGY) pair_coul -= qq * unscreened * inv_r;
+    }
+    if (ENERGY) {
+      if (PAIR_FIXED) {
+        qlj += (long long)to_fixed(pair_lj);
+        qcoul += (long long)to_fixed(pair_coul);
+      } else {
+        elj += pair_lj;
+        ecoul += pair_coul;
+      }
     }
     if (PAIR_FIXED) {
       qx += (long long)to_fixed(scalar * d.x);
@@ -149,8 +165,13 @@ __global__ void __launch_bounds__(128) k_nonbonded(
   const long long gz = group_sum<LANES>(qz);
   double dl = 0, dc = 0;
   if (ENERGY) {
-    dl = group_sum<LANES>((double)elj);
-    dc = group_sum<LANES>((double)ecoul);
+    if (PAIR_FIXED) {  // exact integer sums: the energy, like the force, is order-independent
+      dl = (double)group_sum<LANES>(qlj) / FORCE_SCALE;
+      dc = (double)group_sum<LANES>(qcoul) / FORCE_SCALE;
+    } else {
+      dl = group_sum<LANES>((double)elj);
+      dc = group_sum<LANES>((double)ecoul);
+    }
   }
   if (lane == 0 && valid) {
     force[i] = (unsigned long long)gx;

@@ -397,12 +397,12 @@ __global__ void k_gather(const float4 *__restrict__ posq, const int *__restrict_
 void launch_pme(const LaunchCtx &c, bool energy, cudaStream_t stream) {
   if (!c.pme_on) return;
   const int n = c.n_atoms, tb = 128;
+  const int per_block = c.spread_atoms > 0 ? c.spread_atoms : 8;
+  const int blocks = (n + per_block - 1) / per_block;
   if (c.pme_order == 4)
-    k_spread<4><<<(int)(((long long)n * 16 + tb - 1) / tb), tb, 0, stream>>>(c.posq, c.sys_of_atom, c.sys,
-                                                                            c.fixed_grid, n);
+    k_spread<4><<<blocks, per_block * 16, 0, stream>>>(c.posq, c.sys_of_atom, c.sys, c.fixed_grid, n);
   else
-    k_spread<5><<<(int)(((long long)n * 25 + tb - 1) / tb), tb, 0, stream>>>(c.posq, c.sys_of_atom, c.sys,
-                                                                            c.fixed_grid, n);
+    k_spread<5><<<blocks, per_block * 25, 0, stream>>>(c.posq, c.sys_of_atom, c.sys, c.fixed_grid, n);
   k_fft_z_r2c<<<c.n_tasks_z, 256, 0, stream>>>(c.tasks_z, c.sys, c.fft_plans, c.twiddles,
                                                 c.fixed_grid, c.half);
   k_fft_y<<<c.n_tasks_y, 256, 0, stream>>>(c.tasks_y, c.sys, c.fft_plans, c.twiddles, c.half, 0);

@@ -54,7 +54,8 @@ _OPTION_NAMES = {
     "restraintForce": "restraint_force", "skin": "skin", "neighbourSlack": "neighbour_slack",
     "maxNeighbours": "max_neighbours", "ewaldTolerance": "ewald_tolerance", "alpha": "alpha",
     "pmeOrder": "pme_order", "waterSolver": "water_solver", "learnedBarostat": "learned_barostat",
-    "forceAccumulation": "force_accumulation",
+    "forceAccumulation": "force_accumulation", "neighbourGroupAtoms": "neighbour_group_atoms",
+    "nonbondedLanes": "nonbonded_lanes", "spreadAtomsPerBlock": "spread_atoms_per_block",
 }
 
 
@@ -328,6 +329,27 @@ class BatchSimulation:
 
     def setNonbonded(self, lanes: int = 32, pairFixed: bool = True):
         self._check(self._lib.rmd_debug_set_nonbonded(self._h, int(lanes), 1 if pairFixed else 0))
+
+    def kernelShapes(self) -> dict:
+        """The launch shapes in use and, for those the autotuner chose, its timings (ms)."""
+        shapes = np.zeros(3, np.int32)
+        ms = np.zeros(9)
+        self._check(self._lib.rmd_kernel_shapes(self._h, shapes.ctypes.data_as(C.POINTER(C.c_int32)),
+                                                ms.ctypes.data_as(C.POINTER(C.c_double))))
+
+        def table(row, keys):
+            return {k: float(v) for k, v in zip(keys, row) if v >= 0}
+
+        return {"neighbourGroupAtoms": int(shapes[0]), "nonbondedLanes": int(shapes[1]),
+                "spreadAtomsPerBlock": int(shapes[2]),
+                "tuned": {"neighbourGroupAtoms": table(ms[0:3], (8, 16, 32)),
+                          "nonbondedLanes": table(ms[3:6], (8, 16, 32)),
+                          "spreadAtomsPerBlock": table(ms[6:9], (4, 8, 16))}}
+
+    def setKernelShapes(self, neighbourGroupAtoms: int = 0, nonbondedLanes: int = 0,
+                        spreadAtomsPerBlock: int = 0):
+        self._check(self._lib.rmd_set_kernel_shapes(self._h, int(neighbourGroupAtoms), int(nonbondedLanes),
+                                                    int(spreadAtomsPerBlock)))
 
     def release(self):
         if getattr(self, "_h", None):

@@ -57,12 +57,14 @@ def symmetric_exclusions(system):
     return np.cumsum(start).astype(np.int32), b[order].astype(np.int32)
 
 
+@pytest.mark.parametrize("group", [8, 16, 32])
 @pytest.mark.parametrize("cutoff", [1.0, 0.7, 0.5])
-def test_cell_and_neighbour_lists_bit_exact(cutoff):
-    """check-nonbonded.mjs:12-19, 240-262 at three cell geometries, compared bit for bit
-    with the f32 restatement of the reference's assignment and search."""
+def test_cell_and_neighbour_lists_bit_exact(cutoff, group):
+    """check-nonbonded.mjs:12-19, 240-262 at three cell geometries and every search-group
+    size, compared bit for bit with the f32 restatement of the reference's assignment and
+    search."""
     s, pos, _ = system_for("ala-wat", cutoff=cutoff)
-    sim = engine_for(s, pos, alpha=None, grid=None)
+    sim = engine_for(s, pos, alpha=None, grid=None, neighbourGroupAtoms=group)
     counts, start, atoms = sim.debugCells()
     lc = np.float32(cutoff) + np.float32(0.1)
     P = oracle.pack_params(s["boxVectors"], cutoff, float(np.float32(cutoff + 0.1)), 1.0)
