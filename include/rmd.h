@@ -107,6 +107,10 @@ typedef struct {
   int32_t neighbour_group_atoms; /* atoms per neighbour-search warp: 8, 16 or 32 */
   int32_t nonbonded_lanes;       /* lanes per atom in the pair loop: 8, 16 or 32 */
   int32_t spread_atoms_per_block; /* atoms per PME charge-spreading block: 4, 8 or 16 */
+  /* learned barostat (learned_barostat = 1) */
+  int32_t learned_warmup_moves;  /* exact moves that train the surrogate before it screens; <= 0: 2000 */
+  int32_t learned_steps_per_move; /* Adam steps after each exact move; <= 0: 4 */
+  double learned_rate;           /* Adam learning rate; <= 0: 1e-3 */
 } rmd_options;
 
 #define RMD_NO_PRESSURE (-1.0e300)
@@ -125,6 +129,9 @@ typedef struct {
   int32_t kinetic_sampled_before_closing_kick; /* kineticSampledAt */
   double volume;
   double box_vectors[9];
+  /* dU/dlnV for molecules scaled rigidly about their centres of mass, from the virial of this
+   * evaluation (the learned barostat's first-order term; no reference counterpart) */
+  double volume_derivative;
 } rmd_energy_report;
 
 /* attemptVolumeChange() — webgpu/simulation.js:995-1070 */
@@ -284,6 +291,26 @@ rmd_status rmd_bench_run(rmd_sim *sim, int64_t count, int32_t block_size, int32_
                          double *device_ms);
 /* Kernels this handle has launched so far (graph replays included). */
 int64_t rmd_debug_kernel_launches(const rmd_sim *sim);
+/* The learned barostat's surrogate for system `system_index` (no reference counterpart). */
+typedef struct {
+  int64_t samples;             /* exact (inputs, energy change) pairs seen */
+  int64_t train_steps;         /* Adam steps taken */
+  double loss;                 /* running mean training loss (targets in kT / sqrt(N_mol)) */
+  double prediction_error_kT;  /* running mean |surrogate weight - exact weight| / kT */
+  int32_t screening;           /* 1 once the warm-up is over and stage 1 screens moves */
+  int64_t attempts, exact_evaluations, screened, accepted;
+  int64_t exact_passes, skipped_passes; /* batch-wide: moves that ran / skipped the exact evaluation */
+} rmd_surrogate_report;
+rmd_status rmd_surrogate_report_at(rmd_sim *sim, int32_t system_index, rmd_surrogate_report *out);
+/* The surrogate's FP32 master parameters (4801 floats: W1[64][8], b1[64], W2[64][64], b2[64],
+ * W3[64], b3), e.g. to check its predictions on the CPU. */
+rmd_status rmd_surrogate_weights(rmd_sim *sim, int32_t system_index, float *params);
+/* The surrogate's device forward pass and its mean-squared-error gradient on given data, for
+ * any parameters (host arrays; count <= 64 samples of 8 inputs). The weights go through BF16
+ * exactly as in training. `outputs` or `grads` may be NULL. */
+rmd_status rmd_surrogate_evaluate(const float *params, const float *inputs, const float *targets, int32_t count,
+                                  float *outputs, float *grads, double *loss);
+
 /* Kernel launch shapes in use: shapes = {atoms per neighbour-search warp, lanes per atom in
  * the pair loop, atoms per PME spreading block}. When the options left a shape at 0,
  * initialise() chose it by timing every candidate (the engine's autotuner); tune_ms (may be

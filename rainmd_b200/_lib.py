@@ -53,6 +53,17 @@ class RmdOptions(C.Structure):
         ("pme_order", C.c_int32), ("water_solver", C.c_int32), ("learned_barostat", C.c_int32),
         ("force_accumulation", C.c_int32), ("neighbour_group_atoms", C.c_int32),
         ("nonbonded_lanes", C.c_int32), ("spread_atoms_per_block", C.c_int32),
+        ("learned_warmup_moves", C.c_int32), ("learned_steps_per_move", C.c_int32),
+        ("learned_rate", C.c_double),
+    ]
+
+
+class RmdSurrogateReport(C.Structure):
+    _fields_ = [
+        ("samples", C.c_int64), ("train_steps", C.c_int64), ("loss", C.c_double),
+        ("prediction_error_kT", C.c_double), ("screening", C.c_int32), ("attempts", C.c_int64),
+        ("exact_evaluations", C.c_int64), ("screened", C.c_int64), ("accepted", C.c_int64),
+        ("exact_passes", C.c_int64), ("skipped_passes", C.c_int64),
     ]
 
 
@@ -66,7 +77,7 @@ class RmdEnergyReport(C.Structure):
         ("restrained_atoms", C.c_int32), ("potential", C.c_double), ("kinetic", C.c_double),
         ("total", C.c_double), ("temperature", C.c_double), ("kinetic_for_temperature", C.c_double),
         ("kinetic_sampled_before_closing_kick", C.c_int32), ("volume", C.c_double),
-        ("box_vectors", C.c_double * 9),
+        ("box_vectors", C.c_double * 9), ("volume_derivative", C.c_double),
     ]
 
 
@@ -117,7 +128,8 @@ EXPORTS = [
     "rmd_debug_neighbours", "rmd_debug_evaluate", "rmd_debug_charge_grid", "rmd_debug_fft",
     "rmd_debug_time_kernel", "rmd_debug_kernel_launches", "rmd_debug_set_nonbonded",
     "rmd_bench_run", "rmd_debug_force_term", "rmd_debug_read", "rmd_spread_charges_noalloc",
-    "rmd_kernel_shapes", "rmd_set_kernel_shapes",
+    "rmd_kernel_shapes", "rmd_set_kernel_shapes", "rmd_surrogate_report_at", "rmd_surrogate_weights",
+    "rmd_surrogate_evaluate",
 ]
 
 _lib = None
@@ -176,6 +188,9 @@ def load():
     lib.rmd_debug_set_nonbonded.argtypes = [sim, C.c_int32, C.c_int32]
     lib.rmd_kernel_shapes.argtypes = [sim, _i32p, _dp]
     lib.rmd_set_kernel_shapes.argtypes = [sim, C.c_int32, C.c_int32, C.c_int32]
+    lib.rmd_surrogate_report_at.argtypes = [sim, C.c_int32, C.POINTER(RmdSurrogateReport)]
+    lib.rmd_surrogate_weights.argtypes = [sim, C.c_int32, _fp]
+    lib.rmd_surrogate_evaluate.argtypes = [_fp, _fp, _fp, C.c_int32, _fp, _fp, _dp]
     lib.rmd_bench_run.argtypes = [sim, C.c_int64, C.c_int32, C.c_int32, _dp]
     lib.rmd_debug_force_term.argtypes = [sim, C.c_int32, C.c_int32, _dp]
     lib.rmd_debug_read.argtypes = [sim, C.c_int32, C.c_int32, _dp]

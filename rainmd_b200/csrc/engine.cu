@@ -62,6 +62,12 @@ struct DevArray {
 };
 
 // -------------------------------------------------------------- host-side derivations
+static unsigned short bf16_round_bits(float v) {  // round to nearest even (finite inputs)
+  uint32_t u;
+  memcpy(&u, &v, 4);
+  u += 0x7fffu + ((u >> 16) & 1u);
+  return (unsigned short)(u >> 16);
+}
 static double alpha_from_tolerance(double cutoff, double tol) {  // parameters.js:43-49
   return std::sqrt(-std::log(2.0 * tol)) / cutoff;
 }
@@ -173,7 +179,7 @@ struct Engine {
   DevArray<int> atom_type, sys_of_atom, sys_atom_start;
   DevArray<float> masses, noise;
   DevArray<unsigned long long> force, saved_force;
-  DevArray<double> e_lj, e_coul, ke_post, ke_early, e_term, e_pme;
+  DevArray<double> e_lj, e_coul, e_vir, ke_post, ke_early, e_term, e_pme, e_pme_vir;
   DevArray<float2> lj;
   DevArray<int> excl_start, excl_partners, exc_start, exc_partner;
   DevArray<float4> exc_param;
@@ -215,6 +221,8 @@ struct Engine {
   DevArray<DevSettle> settle_param;
   int n_free = 0, n_clusters = 0, n_settle = 0;
   DevArray<int> mol_start, mol_atoms;
+  DevArray<double> mol_vir, e_term_vir;
+  std::vector<int> mol_base;  // first molecule of each system (S + 1)
   int n_molecules_total = 0;
   bool any_pressure = false;
   bool supplied_noise_any = false;
@@ -237,6 +245,16 @@ struct Engine {
   LaunchCtx ctx() const;
   IntegrateArgs iargs(int step_offset) const;
   BaroArgs bargs() const;
+  // learned barostat (surrogate.cu)
+  bool learned = false;
+  DevArray<float> mlp_master, mlp_m, mlp_v, mlp_replay;
+  DevArray<unsigned short> mlp_wbf;
+  int learned_steps = 4;
+  float learned_lr = 1e-3f;
+  long long exact_passes = 0, skipped_passes = 0;
+  SurrogateArgs sargs();
+  bool surrogate_stage1();  // true when some system's move needs the exact evaluation
+  void surrogate_train();
 
   // ---------------------------------------------------------------- operations
   void record_forces(bool rebuild, bool energy);
@@ -465,7 +483,7 @@ void Engine::upload_all(const std::vector<const rmd_system *> &src) {
   force.zero();
   saved_force.alloc(3 * (size_t)N);
   saved_force.zero();
-  for (auto *a : {&e_lj, &e_coul, &ke_post, &ke_early}) {
+  for (auto *a : {&e_lj, &e_coul, &e_vir, &ke_post, &ke_early}) {
     a->alloc(N);
     a->zero();
   }
@@ -576,6 +594,8 @@ void Engine::upload_all(const std::vector<const rmd_system *> &src) {
   rest_param.upload(hrp);
   e_term.alloc(std::max(1, n_bonds + n_angles + n_tors + n_rest));
   e_term.zero();
+  e_term_vir.alloc(std::max(1, n_bonds + n_angles + n_tors + n_rest));
+  e_term_vir.zero();
 
   // ---- constraint clusters (buildConstraintClusters, clusters.js:20-57) and SETTLE waters
   std::vector<int> h_free, h_cl_as, h_cl_atoms, h_cl_cs;
@@ -710,8 +730,10 @@ void Engine::upload_all(const std::vector<const rmd_system *> &src) {
   // ---- molecules (global CSR over all systems)
   {
     std::vector<int> ms(1, 0), ma;
+    mol_base.assign(1, 0);
     for (int s = 0; s < S; ++s) {
       const rmd_system &r = *src[s];
+      mol_base.push_back(mol_base.back() + r.molecule_count);
       const int base = hs[s].atom_start;
       std::vector<std::vector<int>> mol(r.molecule_count);
       for (int a = 0; a < r.atom_count; ++a) {
@@ -725,6 +747,8 @@ void Engine::upload_all(const std::vector<const rmd_system *> &src) {
       }
     }
     n_molecules_total = (int)ms.size() - 1;
+    mol_vir.alloc(std::max(1, n_molecules_total));
+    mol_vir.zero();
     if (ma.empty()) ma.push_back(0);
     mol_start.upload(ms);
     mol_atoms.upload(ma);
@@ -863,6 +887,8 @@ void Engine::upload_all(const std::vector<const rmd_system *> &src) {
     tasks_x.upload(tx);
     e_pme.alloc(tx.size());
     e_pme.zero();
+    e_pme_vir.alloc(tx.size());
+    e_pme_vir.zero();
   }
 
   // ---- per-system device state
@@ -905,6 +931,44 @@ void Engine::upload_all(const std::vector<const rmd_system *> &src) {
       b[B_KT] = BOLTZMANN * h.opt.temperature;
       b[B_NMOL] = h.n_molecules;
       b[B_SEED] = (double)h.opt.seed;
+      const bool lb = h.has_pressure && h.opt.learned_barostat != 0;
+      learned = learned || lb;
+      b[B_LEARNED] = lb ? 1.0 : 0.0;
+      b[B_WARMUP] = h.opt.learned_warmup_moves > 0 ? h.opt.learned_warmup_moves : 2000;
+      b[B_VOL_REF] = std::fabs(h.box[0] * h.box[4] * h.box[8]);
+      b[B_DOF] = h.dof;
+    }
+    if (learned) {
+      // Xavier-uniform weights (the output layer scaled down), zero biases, from the seed
+      std::vector<float> w((size_t)S * MLP_STRIDE, 0.f);
+      for (int s = 0; s < S; ++s) {
+        uint64_t state = 0x9e3779b97f4a7c15ULL ^ (uint64_t)hs[s].opt.seed * 0xbf58476d1ce4e5b9ULL;
+        auto uniform = [&state]() {
+          state ^= state << 13;
+          state ^= state >> 7;
+          state ^= state << 17;
+          return (double)(state >> 11) * (1.0 / 9007199254740992.0);
+        };
+        float *p = w.data() + (size_t)s * MLP_STRIDE;
+        const double l1 = std::sqrt(6.0 / (MLP_IN + MLP_H)), l2 = std::sqrt(6.0 / (2 * MLP_H)),
+                     l3 = 0.1 * std::sqrt(6.0 / (MLP_H + 1));
+        for (int k = 0; k < MLP_H * MLP_IN; ++k) p[MLP_W1 + k] = (float)((2 * uniform() - 1) * l1);
+        for (int k = 0; k < MLP_H * MLP_H; ++k) p[MLP_W2 + k] = (float)((2 * uniform() - 1) * l2);
+        for (int k = 0; k < MLP_H; ++k) p[MLP_W3 + k] = (float)((2 * uniform() - 1) * l3);
+      }
+      std::vector<unsigned short> wb(w.size());
+      for (size_t k = 0; k < w.size(); ++k) wb[k] = bf16_round_bits(w[k]);
+      mlp_master.upload(w);
+      mlp_wbf.upload(wb);
+      mlp_m.alloc(w.size());
+      mlp_m.zero();
+      mlp_v.alloc(w.size());
+      mlp_v.zero();
+      mlp_replay.alloc((size_t)S * MLP_REPLAY * (MLP_IN + 1));
+      mlp_replay.zero();
+      const rmd_options &o0 = hs[0].opt;
+      if (o0.learned_steps_per_move > 0) learned_steps = o0.learned_steps_per_move;
+      if (o0.learned_rate > 0) learned_lr = (float)o0.learned_rate;
     }
     std::vector<double> tmp = hb;
     baro.upload(tmp);
@@ -924,6 +988,15 @@ void Engine::upload_all(const std::vector<const rmd_system *> &src) {
       seg.push_back(Segment{s, E_LJ, e_lj.p, a0, a1, nullptr});
       seg.push_back(Segment{s, E_COUL_DIRECT, e_coul.p, a0, a1, nullptr});
       seg.push_back(Segment{s, E_RECIP, e_pme.p, task_x_start[s], task_x_start[s + 1], nullptr});
+      seg.push_back(Segment{s, E_VIR_SR, e_vir.p, a0, a1, nullptr});
+      seg.push_back(Segment{s, E_VIR_SR, e_term_vir.p, bstart[s], bstart[s + 1], nullptr});
+      seg.push_back(Segment{s, E_VIR_SR, e_term_vir.p, n_bonds + astart[s], n_bonds + astart[s + 1], nullptr});
+      seg.push_back(Segment{s, E_VIR_SR, e_term_vir.p, n_bonds + n_angles + tstart[s],
+                            n_bonds + n_angles + tstart[s + 1], nullptr});
+      seg.push_back(Segment{s, E_VIR_SR, e_term_vir.p, n_bonds + n_angles + n_tors + rstart[s],
+                            n_bonds + n_angles + n_tors + rstart[s + 1], nullptr});
+      seg.push_back(Segment{s, E_VIR_MOL, mol_vir.p, mol_base[s], mol_base[s + 1], nullptr});
+      seg.push_back(Segment{s, E_VIR_REC, e_pme_vir.p, task_x_start[s], task_x_start[s + 1], nullptr});
       seg.push_back(Segment{s, E_KINETIC, ke_post.p, a0, a1, nullptr});
       seg.push_back(Segment{s, E_KINETIC_EARLY, ke_early.p, a0, a1, nullptr});
     }
@@ -996,6 +1069,7 @@ LaunchCtx Engine::ctx() const {
   c.force = force.p;
   c.e_lj = e_lj.p;
   c.e_coul = e_coul.p;
+  c.e_vir = e_vir.p;
   c.pair_fixed = pair_fixed;
   c.bond_atoms = bond_atoms.p;
   c.bond_param = bond_param.p;
@@ -1010,6 +1084,12 @@ LaunchCtx Engine::ctx() const {
   c.rest_param = rest_param.p;
   c.n_rest = n_rest;
   c.e_term = e_term.p;
+  c.e_term_vir = e_term_vir.p;
+  c.mol_start = mol_start.p;
+  c.mol_atoms = mol_atoms.p;
+  c.masses = masses.p;
+  c.mol_vir = mol_vir.p;
+  c.n_molecules = n_molecules_total;
   c.pme_on = pme_on ? 1 : 0;
   c.pme_order = pme_order;
   c.fixed_grid = fixed_grid.p;
@@ -1025,6 +1105,7 @@ LaunchCtx Engine::ctx() const {
   c.n_tasks_y = (int)tasks_y.n;
   c.n_tasks_x = (int)tasks_x.n;
   c.e_pme = e_pme.p;
+  c.e_pme_vir = e_pme_vir.p;
   return c;
 }
 
@@ -1065,6 +1146,46 @@ IntegrateArgs Engine::iargs(int step_offset) const {
   return a;
 }
 
+SurrogateArgs Engine::sargs() {
+  SurrogateArgs m{};
+  m.n_systems = S;
+  m.master = mlp_master.p;
+  m.adam_m = mlp_m.p;
+  m.adam_v = mlp_v.p;
+  m.wbf = mlp_wbf.p;
+  m.replay = mlp_replay.p;
+  m.baro = baro.p;
+  m.energies = energies.p;
+  m.sysd = sysd.p;
+  m.lr = learned_lr;
+  m.steps = learned_steps;
+  return m;
+}
+
+// Stage 1 of the learned barostat on every system (after the energy evaluation of the
+// current state); whether any system's move still needs the exact evaluation.
+bool Engine::surrogate_stage1() {
+  launch_surrogate_stage1(bargs(), sargs(), stream);
+  kernel_launches += 1;
+  std::vector<double> b((size_t)S * N_BARO);
+  CUDA_OK(cudaMemcpyAsync(b.data(), baro.p, sizeof(double) * b.size(), cudaMemcpyDeviceToHost, stream));
+  sync();
+  bool exact = false;
+  for (int s = 0; s < S; ++s) {
+    const double *x = b.data() + (size_t)s * N_BARO;
+    if (x[B_ACTIVE] == 0.0) continue;
+    if (x[B_LEARNED] == 0.0 || (x[B_REFUSED] == 0.0 && x[B_SCREENED] == 0.0)) exact = true;
+  }
+  if (exact) exact_passes++;
+  else skipped_passes++;
+  return exact;
+}
+
+void Engine::surrogate_train() {
+  launch_surrogate_train(sargs(), stream);
+  kernel_launches += 1;
+}
+
 BaroArgs Engine::bargs() const {
   BaroArgs a{};
   a.n_systems = S;
@@ -1100,8 +1221,9 @@ void Engine::record_forces(bool rebuild, bool energy) {
   launch_pme(c, energy, stream);
   recorded += 1 + (n_bonds + n_angles + n_tors + n_rest > 0 ? 1 : 0) + (pme_on ? 7 : 0);
   if (energy) {
+    launch_molecular_virial(c, stream);
     launch_energy_reduce(segments.p, n_segments, seg_out.p, energies.p, sysd.p, S, stream);
-    recorded += 2;
+    recorded += 3;
   }
 }
 
@@ -1424,11 +1546,16 @@ void Engine::run(int64_t count, int block, const volatile int32_t *stop) {
     bool next_due = false;
     for (auto &h : hs)
       if (h.has_pressure && (due ? 0 : h.steps_since_barostat) + n >= h.barostat_interval) next_due = true;
+    bool exact_move = due;
     if (due) {
       // the move needs the energy at the current positions
       evaluate(false, true);
+      // with the learned barostat, stage 1 may screen every system's move out: the block
+      // then runs without the exact trial evaluation
+      if (learned) exact_move = surrogate_stage1();
     }
-    run_block(n, due, next_due);
+    run_block(n, exact_move, next_due);
+    if (due && learned && exact_move) surrogate_train();
     sync();
     if (due) {
       for (auto &h : hs) h.steps_since_barostat = 0;
@@ -1440,8 +1567,9 @@ void Engine::run(int64_t count, int block, const volatile int32_t *stop) {
         if (!h.has_pressure) continue;
         rmd_volume_move &m = h.last_move;
         m.attempted = 1;
-        m.accepted = bb[B_ACCEPT] != 0.0 && bb[B_REFUSED] == 0.0;
+        m.screened = bb[B_SCREENED] != 0.0;
         m.refused = bb[B_REFUSED] != 0.0;
+        m.accepted = exact_move && bb[B_ACCEPT] != 0.0 && !m.refused && !m.screened;
         m.weight = bb[B_WEIGHT];
         m.delta_volume = bb[B_DV];
         m.length_scale = bb[B_LSCALE];
@@ -1502,6 +1630,7 @@ void Engine::energy(int s, rmd_energy_report *out) {
   out->temperature = 2.0 * kt / (h.dof * BOLTZMANN);
   out->volume = d.volume;
   for (int k = 0; k < 9; ++k) out->box_vectors[k] = d.box[k];
+  out->volume_derivative = e[E_DUDLNV];
   if (!std::isfinite(out->potential) || !std::isfinite(out->kinetic))
     throw Error(RMD_ERR_NON_FINITE, std::string("the simulation is no longer a number: the ") +
                                         (!std::isfinite(out->potential) ? "potential" : "kinetic") +
@@ -1512,7 +1641,11 @@ void Engine::attempt_volume_change() {
   // energy at the current positions, then one device-side move on every system
   evaluate(false, true);
   const BaroArgs b = bargs();
-  record_barostat();
+  const bool exact_move = learned ? surrogate_stage1() : true;
+  if (exact_move) {
+    record_barostat();
+    if (learned) surrogate_train();
+  }
   CUDA_OK(cudaGetLastError());
   sync();
   for (auto &h : hs) h.steps_since_rebuild = 1LL << 40;
@@ -1529,7 +1662,8 @@ void Engine::attempt_volume_change() {
     if (!h.has_pressure) continue;
     m.attempted = 1;
     m.refused = x[B_REFUSED] != 0.0;
-    m.accepted = !m.refused && x[B_ACCEPT] != 0.0;
+    m.screened = x[B_SCREENED] != 0.0;
+    m.accepted = exact_move && !m.refused && !m.screened && x[B_ACCEPT] != 0.0;
     m.weight = x[B_WEIGHT];
     m.delta_volume = x[B_DV];
     m.length_scale = x[B_LSCALE];
@@ -2162,6 +2296,71 @@ rmd_status rmd_debug_time_kernel(rmd_sim *sim, int32_t which, int32_t reps, doub
 }
 
 int64_t rmd_debug_kernel_launches(const rmd_sim *sim) { return sim ? sim->engine.kernel_launches : 0; }
+
+rmd_status rmd_surrogate_report_at(rmd_sim *sim, int32_t s, rmd_surrogate_report *out) {
+  if (rmd_status c = check_index(sim, s)) return c;
+  if (!out) return RMD_ERR_INVALID;
+  return guarded(sim, [&]() {
+    auto &e = sim->engine;
+    e.sync();
+    std::vector<double> b(rmd::N_BARO);
+    CUDA_OK(cudaMemcpy(b.data(), e.baro.p + (size_t)s * rmd::N_BARO, sizeof(double) * rmd::N_BARO,
+                       cudaMemcpyDeviceToHost));
+    memset(out, 0, sizeof *out);
+    out->samples = (int64_t)b[rmd::B_REPLAY_N];
+    out->train_steps = (int64_t)b[rmd::B_TRAIN_STEPS];
+    out->loss = b[rmd::B_LOSS];
+    out->prediction_error_kT = b[rmd::B_PRED_ERR];
+    out->screening = b[rmd::B_LEARNED] != 0.0 && b[rmd::B_REPLAY_N] >= b[rmd::B_WARMUP];
+    out->attempts = (int64_t)b[rmd::B_ATTEMPTS];
+    out->exact_evaluations = (int64_t)b[rmd::B_EXACT_EVALS];
+    out->screened = (int64_t)b[rmd::B_SCREENED_TOTAL];
+    out->accepted = (int64_t)b[rmd::B_ACCEPTED];
+    out->exact_passes = e.exact_passes;
+    out->skipped_passes = e.skipped_passes;
+  });
+}
+
+rmd_status rmd_surrogate_weights(rmd_sim *sim, int32_t s, float *params) {
+  if (rmd_status c = check_index(sim, s)) return c;
+  if (!params) return RMD_ERR_INVALID;
+  return guarded(sim, [&]() {
+    auto &e = sim->engine;
+    if (!e.learned) throw rmd::Error(RMD_ERR_INVALID, "the learned barostat is not enabled");
+    e.sync();
+    CUDA_OK(cudaMemcpy(params, e.mlp_master.p + (size_t)s * rmd::MLP_STRIDE, sizeof(float) * rmd::MLP_PARAMS,
+                       cudaMemcpyDeviceToHost));
+  });
+}
+
+rmd_status rmd_surrogate_evaluate(const float *params, const float *inputs, const float *targets, int32_t count,
+                                  float *outputs, float *grads, double *loss) {
+  if (!params || !inputs || count <= 0 || count > rmd::MLP_BATCH || (grads && (!targets || !loss)))
+    return RMD_ERR_INVALID;
+  return guarded(nullptr, [&]() {
+    rmd::DevArray<float> p, x, t, o, g, l;
+    p.upload(std::vector<float>(params, params + rmd::MLP_PARAMS));
+    x.upload(std::vector<float>(inputs, inputs + (size_t)count * rmd::MLP_IN));
+    if (targets) t.upload(std::vector<float>(targets, targets + count));
+    o.alloc(count);
+    if (grads) {
+      g.alloc(rmd::MLP_PARAMS);
+      l.alloc(1);
+    }
+    rmd::surrogate_predict(p.p, x.p, count, o.p, nullptr);
+    if (grads) rmd::surrogate_gradients(p.p, x.p, t.p, count, g.p, l.p, nullptr);
+    CUDA_OK(cudaGetLastError());
+    CUDA_OK(cudaDeviceSynchronize());
+    if (outputs) CUDA_OK(cudaMemcpy(outputs, o.p, sizeof(float) * count, cudaMemcpyDeviceToHost));
+    if (grads) {
+      CUDA_OK(cudaMemcpy(grads, g.p, sizeof(float) * rmd::MLP_PARAMS, cudaMemcpyDeviceToHost));
+      float lf = 0;
+      CUDA_OK(cudaMemcpy(&lf, l.p, sizeof(float), cudaMemcpyDeviceToHost));
+      *loss = lf;
+    }
+    for (auto *a : {&p, &x, &t, &o, &g, &l}) a->release();
+  });
+}
 
 rmd_status rmd_kernel_shapes(const rmd_sim *sim, int32_t shapes[3], double tune_ms[9]) {
   if (!sim) return RMD_ERR_INVALID;

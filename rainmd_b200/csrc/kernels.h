@@ -103,7 +103,12 @@ struct LaunchCtx {
   const int *exc_start, *exc_partner;
   const float4 *exc_param;
   unsigned long long *force;
-  double *e_lj, *e_coul;
+  double *e_lj, *e_coul, *e_vir;
+  // molecules, for the molecular virial correction (energy evaluations only)
+  const int *mol_start, *mol_atoms;
+  const float *masses;
+  double *mol_vir;
+  int n_molecules;
   int pair_fixed;  // 1: per-pair fixed-point accumulation (precision form), 0: per-lane f32
   // bonded
   const int2 *bond_atoms;
@@ -118,7 +123,7 @@ struct LaunchCtx {
   const int *rest_atom;
   const float4 *rest_param;
   int n_rest;
-  double *e_term;
+  double *e_term, *e_term_vir;
   // pme
   int pme_on, pme_order;
   int spread_atoms;  // atoms per spreading block: 4, 8 or 16
@@ -130,7 +135,7 @@ struct LaunchCtx {
   const FftPlan *fft_plans;
   const FftTask *tasks_z, *tasks_y, *tasks_x;
   int n_tasks_z, n_tasks_y, n_tasks_x;
-  double *e_pme;
+  double *e_pme, *e_pme_vir;
 };
 
 void launch_rebuild(const LaunchCtx &c, cudaStream_t stream);
@@ -138,6 +143,7 @@ void launch_rebuild(const LaunchCtx &c, cudaStream_t stream);
 int neighbour_group_slots(int atoms, int cells, int group_atoms);
 void launch_nonbonded(const LaunchCtx &c, bool energy, int lanes, cudaStream_t stream);
 void launch_bonded(const LaunchCtx &c, bool energy, cudaStream_t stream);
+void launch_molecular_virial(const LaunchCtx &c, cudaStream_t stream);
 void launch_pme(const LaunchCtx &c, bool energy, cudaStream_t stream);
 void launch_fft_forward(const LaunchCtx &c, cudaStream_t stream);
 void launch_spread_only(const LaunchCtx &c, cudaStream_t stream);
@@ -148,7 +154,12 @@ void launch_integrate(const IntegrateArgs &a, int mode, cudaStream_t stream);
 // per-item FP64 array; the result lands in energies[sys * N_ENERGY + term].
 enum EnergyTerm {
   E_BOND = 0, E_ANGLE, E_TORSION, E_LJ, E_COUL_DIRECT, E_RECIP, E_RESTRAINT, E_KINETIC,
-  E_KINETIC_EARLY, E_SELF, E_NET, E_DISPERSION, E_POTENTIAL, N_ENERGY
+  E_KINETIC_EARLY, E_SELF, E_NET, E_DISPERSION, E_POTENTIAL,
+  // not energies: the atomic virial sum F.r of the pair, exception and bonded terms; the
+  // reciprocal-space sum sum_k E_k (1 + pi^2 m^2 / alpha^2); sum_i F_i.(r_i - R_mol(i)) over
+  // atoms with R the molecule's centre of mass; and from them dU/dlnV when molecules are
+  // scaled rigidly about their centres (the barostat's move)
+  E_VIR_SR, E_VIR_REC, E_VIR_MOL, E_DUDLNV, N_ENERGY
 };
 struct Segment {
   int sys, term;
@@ -178,10 +189,41 @@ struct BaroArgs {
 enum BaroSlot {
   B_ACTIVE = 0, B_PRESSURE, B_KT, B_NMOL, B_SEED, B_ATTEMPTS, B_ACCEPTED, B_WINDOW_ATT, B_WINDOW_ACC,
   B_SCALE, B_DV, B_LSCALE, B_OLD_E, B_NEW_E, B_WEIGHT, B_ACCEPT, B_REFUSED, B_REFUSALS,
-  B_OLD_VOL, B_MAX_SHRINK, B_MIN_LIST_WIDTH, B_SCREENED, B_SCREENED_TOTAL, B_EXACT_EVALS,
-  B_PRED, B_PRED_REV, B_FEATURE0, B_LEARNED, B_VOL_REF, N_BARO = 48
+  B_OLD_VOL, B_SCREENED, B_SCREENED_TOTAL, B_EXACT_EVALS,
+  // learned barostat (surrogate.cu): on/off, moves before screening starts, the reference
+  // volume of the inputs, degrees of freedom, the last four exact energy changes, the
+  // surrogate's weights for the forward and reverse move, dU/dlnV of the move's start,
+  // replay fill, training steps, running loss and prediction error, and the move's inputs
+  B_LEARNED, B_WARMUP, B_VOL_REF, B_DOF, B_HIST0, B_HIST1, B_HIST2, B_HIST3, B_PRED, B_PRED_REV,
+  B_DUDLNV, B_REPLAY_N, B_TRAIN_STEPS, B_LOSS, B_PRED_ERR, B_SCREENING, B_FEATURE0,
+  N_BARO = B_FEATURE0 + 8 + 4
 };
 void launch_baro_propose(const BaroArgs &a, cudaStream_t stream);
+// Learned barostat (surrogate.cu). The MLP: 8 inputs, two tanh layers of 64, one output;
+// FP32 master weights with Adam moments, BF16 copies for every forward pass.
+constexpr int MLP_IN = 8, MLP_H = 64;
+constexpr int MLP_W1 = 0, MLP_B1 = MLP_W1 + MLP_H * MLP_IN, MLP_W2 = MLP_B1 + MLP_H,
+              MLP_B2 = MLP_W2 + MLP_H * MLP_H, MLP_W3 = MLP_B2 + MLP_H, MLP_B3 = MLP_W3 + MLP_H,
+              MLP_PARAMS = MLP_B3 + 1, MLP_STRIDE = 4864;
+constexpr int MLP_REPLAY = 4096;  // (inputs, target) samples kept per system
+constexpr int MLP_BATCH = 64;     // training minibatch
+struct SurrogateArgs {
+  int n_systems;
+  float *master, *adam_m, *adam_v;  // [system][MLP_STRIDE]
+  unsigned short *wbf;              // BF16 bits of the master weights, [system][MLP_STRIDE]
+  float *replay;                    // [system][MLP_REPLAY][MLP_IN + 1]
+  double *baro;
+  double *energies;
+  DevSysD *sysd;
+  float lr;
+  int steps;                        // gradient steps per training launch
+};
+void launch_surrogate_stage1(const BaroArgs &a, const SurrogateArgs &m, cudaStream_t stream);
+void launch_surrogate_train(const SurrogateArgs &m, cudaStream_t stream);
+// standalone forward and gradient of one network on given data (for the gradient check)
+void surrogate_predict(const float *params, const float *x, int count, float *out, cudaStream_t stream);
+void surrogate_gradients(const float *params, const float *x, const float *target, int count,
+                         float *grads, float *loss, cudaStream_t stream);
 void launch_baro_scale(const BaroArgs &a, cudaStream_t stream);
 void launch_baro_decide(const BaroArgs &a, cudaStream_t stream);
 void launch_baro_restore(const BaroArgs &a, cudaStream_t stream);

@@ -13,7 +13,8 @@
 // once per pair and shared by erfc and the Gaussian. Per-lane partial forces are converted
 // to 64-bit fixed point and reduced with integer shuffles, so the sum is exact and
 // order-independent; lane 0 stores the atom's force (this kernel is the first writer of
-// the force array in every evaluation). Energies are only computed in the ENERGY variant.
+// the force array in every evaluation). Energies, and the pair virial sum F.r over the
+// list pairs (the barostat surrogate's input), are only computed in the ENERGY variant.
 #include "common.cuh"
 #include "kernels.h"
 
@@ -44,7 +45,7 @@ __global__ void __launch_bounds__(128) k_nonbonded(
     const float2 *__restrict__ lj, const int *__restrict__ nbr, const int *__restrict__ nbr_count,
     const int *__restrict__ exc_start, const int *__restrict__ exc_partner,
     const float4 *__restrict__ exc_param, unsigned long long *__restrict__ force,
-    double *__restrict__ e_lj, double *__restrict__ e_coul, int n_atoms) {
+    double *__restrict__ e_lj, double *__restrict__ e_coul, double *__restrict__ e_vir, int n_atoms) {
   const int gid = blockIdx.x * blockDim.x + threadIdx.x;
   // A warp may hold a group past the last atom (LANES < 32): it works on a clamped atom
   // with an empty row and stores nothing, so every lane reaches the shuffles.
@@ -64,8 +65,8 @@ __global__ void __launch_bounds__(128) k_nonbonded(
   const int count = valid ? nbr_count[si] : 0;
   const int *row = nbr + s.nbr_base + (long long)(si - s.atom_start) * s.nbr_capacity;
 
-  float fx = 0.f, fy = 0.f, fz = 0.f, elj = 0.f, ecoul = 0.f;
-  long long qx = 0, qy = 0, qz = 0, qlj = 0, qcoul = 0;
+  float fx = 0.f, fy = 0.f, fz = 0.f, elj = 0.f, ecoul = 0.f, evir = 0.f;
+  long long qx = 0, qy = 0, qz = 0, qlj = 0, qcoul = 0, qvir = 0;
   for (int k = lane; k < count; k += LANES) {
     const unsigned e = (unsigned)__ldg(row + k);
     const int g = (int)(e & NBR_SLOT_MASK);
@@ -98,9 +99,11 @@ __global__ void __launch_bounds__(128) k_nonbonded(
         if (PAIR_FIXED) {
           qlj += (long long)to_fixed(a12 - b6);
           qcoul += (long long)to_fixed(qq * screened * inv_r);
+          qvir += (long long)to_fixed(scalar * r2);
         } else {
           elj += a12 - b6;
           ecoul = fmaf(qq * screened, inv_r, ecoul);
+          evir = fmaf(scalar, r2, evir);
         }
       }
     }
@@ -140,9 +143,11 @@ __global__ void __launch_bounds__(128) k_nonbonded(
       if (PAIR_FIXED) {
         qlj += (long long)to_fixed(pair_lj);
         qcoul += (long long)to_fixed(pair_coul);
+        qvir += (long long)to_fixed(scalar * r2);
       } else {
         elj += pair_lj;
         ecoul += pair_coul;
+        evir = fmaf(scalar, r2, evir);
       }
     }
     if (PAIR_FIXED) {
@@ -163,14 +168,16 @@ __global__ void __launch_bounds__(128) k_nonbonded(
   const long long gx = group_sum<LANES>(qx);
   const long long gy = group_sum<LANES>(qy);
   const long long gz = group_sum<LANES>(qz);
-  double dl = 0, dc = 0;
+  double dl = 0, dc = 0, dv = 0;
   if (ENERGY) {
     if (PAIR_FIXED) {  // exact integer sums: the energy, like the force, is order-independent
       dl = (double)group_sum<LANES>(qlj) / FORCE_SCALE;
       dc = (double)group_sum<LANES>(qcoul) / FORCE_SCALE;
+      dv = (double)group_sum<LANES>(qvir) / FORCE_SCALE;
     } else {
       dl = group_sum<LANES>((double)elj);
       dc = group_sum<LANES>((double)ecoul);
+      dv = group_sum<LANES>((double)evir);
     }
   }
   if (lane == 0 && valid) {
@@ -180,6 +187,7 @@ __global__ void __launch_bounds__(128) k_nonbonded(
     if (ENERGY) {
       e_lj[i] = 0.5 * dl;
       e_coul[i] = 0.5 * dc;
+      e_vir[i] = 0.5 * dv;
     }
   }
 }
@@ -191,7 +199,7 @@ static void launch_nb(const LaunchCtx &c, cudaStream_t stream) {
   const int blocks = (int)((total + threads - 1) / threads);
   k_nonbonded<ENERGY, LANES, PAIR_FIXED><<<blocks, threads, 0, stream>>>(
       c.posq, c.spos, c.sorted_orig, c.sorted_type, c.sys_of_atom, c.sys, c.lj, c.nbr, c.nbr_count, c.exc_start,
-      c.exc_partner, c.exc_param, c.force, c.e_lj, c.e_coul, c.n_atoms);
+      c.exc_partner, c.exc_param, c.force, c.e_lj, c.e_coul, c.e_vir, c.n_atoms);
 }
 
 template <bool PAIR_FIXED>
@@ -225,12 +233,12 @@ __global__ void k_bonded(const float4 *__restrict__ posq, const int *__restrict_
                          const float4 *__restrict__ tor_param, int n_tors,
                          const int *__restrict__ rest_atom, const float4 *__restrict__ rest_param,
                          int n_rest, unsigned long long *__restrict__ force,
-                         double *__restrict__ e_term, int n_atoms) {
+                         double *__restrict__ e_term, double *__restrict__ e_term_vir, int n_atoms) {
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   unsigned long long *fxp = force, *fyp = force + n_atoms, *fzp = force + 2 * (long long)n_atoms;
   const int total = n_bonds + n_angles + n_tors + n_rest;
   if (t >= total) return;
-  float energy = 0.f;
+  float energy = 0.f, virial = 0.f;  // virial: sum_k F_k.(r_k - r_ref) over the term's atoms
   if (t < n_bonds) {
     const int2 a = bond_atoms[t];
     const float2 p = bond_param[t];
@@ -240,6 +248,7 @@ __global__ void k_bonded(const float4 *__restrict__ posq, const int *__restrict_
     const float stretch = r - p.y;
     energy = 0.5f * p.x * stretch * stretch;
     const float sc = r > 0.f ? p.x * stretch / r : 0.f;
+    virial = -sc * r * r;
     add_fixed(fxp + a.x, -sc * dx); add_fixed(fyp + a.x, -sc * dy); add_fixed(fzp + a.x, -sc * dz);
     add_fixed(fxp + a.y, sc * dx); add_fixed(fyp + a.y, sc * dy); add_fixed(fzp + a.y, sc * dz);
   } else if ((t -= n_bonds) < n_angles) {
@@ -258,6 +267,7 @@ __global__ void k_bonded(const float4 *__restrict__ posq, const int *__restrict_
     const float s1 = -dE / (n1 * safe), s2 = dE / (n2 * safe);
     const float fax = s1 * (v1y * nz - v1z * ny), fay = s1 * (v1z * nx - v1x * nz), faz = s1 * (v1x * ny - v1y * nx);
     const float fcx = s2 * (v2y * nz - v2z * ny), fcy = s2 * (v2z * nx - v2x * nz), fcz = s2 * (v2x * ny - v2y * nx);
+    virial = fax * v1x + fay * v1y + faz * v1z + fcx * v2x + fcy * v2y + fcz * v2z;
     add_fixed(fxp + a.x, fax); add_fixed(fyp + a.x, fay); add_fixed(fzp + a.x, faz);
     add_fixed(fxp + a.z, fcx); add_fixed(fyp + a.z, fcy); add_fixed(fzp + a.z, fcz);
     add_fixed(fxp + a.y, -(fax + fcx)); add_fixed(fyp + a.y, -(fay + fcy)); add_fixed(fzp + a.y, -(faz + fcz));
@@ -288,6 +298,11 @@ __global__ void k_bonded(const float4 *__restrict__ posq, const int *__restrict_
       const float uu = (b3x * b2x + b3y * b2y + b3z * b2z) * inv;
       const float fax = fA * n1x, fay = fA * n1y, faz = fA * n1z;
       const float fdx = fD * n2x, fdy = fD * n2y, fdz = fD * n2z;
+      const float fcx = tt * fax - (1.f + uu) * fdx, fcy = tt * fay - (1.f + uu) * fdy,
+                  fcz = tt * faz - (1.f + uu) * fdz;
+      // about atom B: r_A - r_B = -b1, r_C - r_B = b2, r_D - r_B = b2 + b3
+      virial = -(fax * b1x + fay * b1y + faz * b1z) + fcx * b2x + fcy * b2y + fcz * b2z +
+               fdx * (b2x + b3x) + fdy * (b2y + b3y) + fdz * (b2z + b3z);
       add_fixed(fxp + a.x, fax); add_fixed(fyp + a.x, fay); add_fixed(fzp + a.x, faz);
       add_fixed(fxp + a.w, fdx); add_fixed(fyp + a.w, fdy); add_fixed(fzp + a.w, fdz);
       add_fixed(fxp + a.y, -(1.f + tt) * fax + uu * fdx);
@@ -307,8 +322,12 @@ __global__ void k_bonded(const float4 *__restrict__ posq, const int *__restrict_
     energy = p.w * (d.x * d.x + d.y * d.y + d.z * d.z);
     const float sc = -2.0f * p.w;
     add_fixed(fxp + atom, sc * d.x); add_fixed(fyp + atom, sc * d.y); add_fixed(fzp + atom, sc * d.z);
+    virial = sc * (d.x * A.x + d.y * A.y + d.z * A.z);  // F.r: not translation invariant
   }
-  if (ENERGY) e_term[blockIdx.x * blockDim.x + threadIdx.x] = (double)energy;
+  if (ENERGY) {
+    e_term[blockIdx.x * blockDim.x + threadIdx.x] = (double)energy;
+    e_term_vir[blockIdx.x * blockDim.x + threadIdx.x] = (double)virial;
+  }
 }
 
 void launch_bonded(const LaunchCtx &c, bool energy, cudaStream_t stream) {
@@ -319,12 +338,65 @@ void launch_bonded(const LaunchCtx &c, bool energy, cudaStream_t stream) {
     k_bonded<true><<<(total + tb - 1) / tb, tb, 0, stream>>>(
         c.posq, c.sys_of_atom, c.sys, c.bond_atoms, c.bond_param, c.n_bonds, c.angle_atoms,
         c.angle_param, c.n_angles, c.tor_atoms, c.tor_param, c.n_tors, c.rest_atom, c.rest_param,
-        c.n_rest, c.force, c.e_term, c.n_atoms);
+        c.n_rest, c.force, c.e_term, c.e_term_vir, c.n_atoms);
   else
     k_bonded<false><<<(total + tb - 1) / tb, tb, 0, stream>>>(
         c.posq, c.sys_of_atom, c.sys, c.bond_atoms, c.bond_param, c.n_bonds, c.angle_atoms,
         c.angle_param, c.n_angles, c.tor_atoms, c.tor_param, c.n_tors, c.rest_atom, c.rest_param,
-        c.n_rest, c.force, c.e_term, c.n_atoms);
+        c.n_rest, c.force, c.e_term, c.e_term_vir, c.n_atoms);
+}
+
+// ------------------------------------------------------------------ molecular virial
+// One warp per molecule, after every force term: sum_i F_i.(r_i - R) over the molecule's
+// atoms, R its centre of mass (positions are never wrapped, so molecules are whole).
+// Added to the atomic virial it turns dU/dlnV for atoms scaled with the box into dU/dlnV
+// for molecules scaled rigidly about their centres.
+__global__ void k_molecular_virial(const float4 *__restrict__ posq, const float *__restrict__ masses,
+                                   const int *__restrict__ mol_start, const int *__restrict__ mol_atoms,
+                                   const unsigned long long *__restrict__ force, double *__restrict__ mol_vir,
+                                   int n_molecules, int n_atoms) {
+  const int m = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (m >= n_molecules) return;
+  const int begin = mol_start[m], end = mol_start[m + 1];
+  const int i0 = mol_atoms[begin];
+  const float4 r0 = posq[i0];
+  double cx = 0, cy = 0, cz = 0, mt = 0;
+  for (int k = begin + lane; k < end; k += 32) {
+    const int i = mol_atoms[k];
+    const float4 p = posq[i];
+    const double w = masses[i];
+    cx += w * (double)(p.x - r0.x);
+    cy += w * (double)(p.y - r0.y);
+    cz += w * (double)(p.z - r0.z);
+    mt += w;
+  }
+  cx = warp_sum(cx);
+  cy = warp_sum(cy);
+  cz = warp_sum(cz);
+  mt = warp_sum(mt);
+  if (mt > 0) {
+    cx /= mt;
+    cy /= mt;
+    cz /= mt;
+  }
+  double v = 0;
+  for (int k = begin + lane; k < end; k += 32) {
+    const int i = mol_atoms[k];
+    const float4 p = posq[i];
+    const double fx = (double)(long long)force[i] / FORCE_SCALE;
+    const double fy = (double)(long long)force[n_atoms + i] / FORCE_SCALE;
+    const double fz = (double)(long long)force[2 * (long long)n_atoms + i] / FORCE_SCALE;
+    v += fx * ((double)(p.x - r0.x) - cx) + fy * ((double)(p.y - r0.y) - cy) + fz * ((double)(p.z - r0.z) - cz);
+  }
+  v = warp_sum(v);
+  if (lane == 0) mol_vir[m] = v;
+}
+
+void launch_molecular_virial(const LaunchCtx &c, cudaStream_t stream) {
+  if (c.n_molecules <= 0) return;
+  const int tb = 128;
+  k_molecular_virial<<<(int)(((long long)c.n_molecules * 32 + tb - 1) / tb), tb, 0, stream>>>(
+      c.posq, c.masses, c.mol_start, c.mol_atoms, c.force, c.mol_vir, c.n_molecules, c.n_atoms);
 }
 
 }  // namespace rmd

@@ -285,9 +285,10 @@ __global__ void __launch_bounds__(256) k_fft_x_convolve(const FftTask *__restric
                                                         const float2 *__restrict__ twiddles,
                                                         const float *__restrict__ moduli,
                                                         float2 *__restrict__ half,
-                                                        double *__restrict__ e_pme) {
+                                                        double *__restrict__ e_pme,
+                                                        double *__restrict__ e_pme_vir) {
   __shared__ float2 bufa[FFT_SMEM], bufb[FFT_SMEM];
-  __shared__ double red[256 / 32];
+  __shared__ double red[2][256 / 32];
   const FftTask t = tasks[blockIdx.x];
   const DevSys &s = sys[t.sys];
   const FftPlan &pl = plans[t.sys];
@@ -306,7 +307,7 @@ __global__ void __launch_bounds__(256) k_fft_x_convolve(const FftTask *__restric
   const float two_pref = (float)(2.0 * ONE_4PI_EPS0 / (2.0 * M_PI * volume));
   const float *modx = moduli + s.moduli_base, *mody = modx + nx, *modz = mody + ny;
   const int ky = y <= ny / 2 ? y : y - ny;
-  double energy = 0.0;
+  double energy = 0.0, virial = 0.0;
   for (int idx = threadIdx.x; idx < nx * M; idx += blockDim.x) {
     const int m = idx / nx, mx = idx - m * nx;
     const int kz = kz0 + m;
@@ -324,7 +325,9 @@ __global__ void __launch_bounds__(256) k_fft_x_convolve(const FftTask *__restric
     const float kernel = __expf(-factor * m2) / (m2 * modx[mx] * mody[y] * modz[kz]);
     if (ENERGY) {
       const double weight = (kz == 0 || 2 * kz == nz) ? 1.0 : 2.0;
-      energy += weight * 0.5 * (double)two_pref * (double)kernel * ((double)v.x * v.x + (double)v.y * v.y);
+      const double ek = weight * 0.5 * (double)two_pref * (double)kernel * ((double)v.x * v.x + (double)v.y * v.y);
+      energy += ek;
+      virial += ek * (1.0 + (double)factor * (double)m2);
     }
     const float sc = kernel * two_pref;
     r[idx] = make_float2(v.x * sc, v.y * sc);
@@ -337,12 +340,20 @@ __global__ void __launch_bounds__(256) k_fft_x_convolve(const FftTask *__restric
   }
   if (ENERGY) {
     energy = warp_sum(energy);
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = energy;
+    virial = warp_sum(virial);
+    if ((threadIdx.x & 31) == 0) {
+      red[0][threadIdx.x >> 5] = energy;
+      red[1][threadIdx.x >> 5] = virial;
+    }
     __syncthreads();
     if (threadIdx.x == 0) {
-      double total = 0;
-      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) total += red[w];
+      double total = 0, total_vir = 0;
+      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+        total += red[0][w];
+        total_vir += red[1][w];
+      }
       e_pme[blockIdx.x] = total;
+      e_pme_vir[blockIdx.x] = total_vir;
     }
   }
 }
@@ -408,10 +419,12 @@ void launch_pme(const LaunchCtx &c, bool energy, cudaStream_t stream) {
   k_fft_y<<<c.n_tasks_y, 256, 0, stream>>>(c.tasks_y, c.sys, c.fft_plans, c.twiddles, c.half, 0);
   if (energy)
     k_fft_x_convolve<true><<<c.n_tasks_x, 256, 0, stream>>>(c.tasks_x, c.sys, c.sysd, c.fft_plans,
-                                                            c.twiddles, c.moduli, c.half, c.e_pme);
+                                                            c.twiddles, c.moduli, c.half, c.e_pme,
+                                                            c.e_pme_vir);
   else
     k_fft_x_convolve<false><<<c.n_tasks_x, 256, 0, stream>>>(c.tasks_x, c.sys, c.sysd, c.fft_plans,
-                                                             c.twiddles, c.moduli, c.half, c.e_pme);
+                                                             c.twiddles, c.moduli, c.half, c.e_pme,
+                                                             c.e_pme_vir);
   k_fft_y<<<c.n_tasks_y, 256, 0, stream>>>(c.tasks_y, c.sys, c.fft_plans, c.twiddles, c.half, 1);
   k_fft_z_c2r<<<c.n_tasks_z, 256, 0, stream>>>(c.tasks_z, c.sys, c.fft_plans, c.twiddles, c.half,
                                                 c.real_grid);

@@ -57,6 +57,14 @@ __global__ void k_energy_finalize(const Segment *__restrict__ segs, int n_segmen
   }
   e[E_POTENTIAL] = e[E_BOND] + e[E_ANGLE] + e[E_TORSION] + e[E_LJ] + e[E_COUL_DIRECT] +
                    e[E_RECIP] + e[E_SELF] + e[E_NET] + e[E_DISPERSION] + e[E_RESTRAINT];
+  // dU/dlnV with every coordinate scaled with the box: -(1/3) sum F.r for the pair,
+  // exception and bonded terms (F.r about any atom of a term); for the reciprocal sum
+  // E = sum_k f(m^2) |S(m)|^2 / V with m^2 ~ V^(-2/3), -E + (2/3) sum_k E_k (1 + pi^2 m^2 /
+  // alpha^2); the 1/V terms (dispersion, net charge) give -E each. Scaling molecules rigidly
+  // about their centres instead moves atom i by (lambda - 1) R_mol(i) rather than
+  // (lambda - 1) r_i, which adds (1/3) sum_i F_i.(r_i - R_mol(i)).
+  e[E_DUDLNV] = (-e[E_VIR_SR] + e[E_VIR_MOL]) / 3.0 - e[E_RECIP] + (2.0 / 3.0) * e[E_VIR_REC] -
+                e[E_DISPERSION] - e[E_NET];
   for (int k = 0; k < N_ENERGY; ++k) energies[s * N_ENERGY + k] = e[k];
 }
 
@@ -127,37 +135,48 @@ __global__ void k_baro_propose(BaroArgs a) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= a.n_systems) return;
   double *b = a.baro + (long long)s * N_BARO;
-  b[B_ACCEPT] = 1.0;
-  b[B_REFUSED] = 0.0;
-  b[B_LSCALE] = 1.0;
+  const bool learned = b[B_LEARNED] != 0.0;
+  if (!learned) {
+    b[B_ACCEPT] = 1.0;
+    b[B_REFUSED] = 0.0;
+    b[B_LSCALE] = 1.0;
+  }
   if (b[B_ACTIVE] == 0.0) return;
   DevSysD &d = a.sysd[s];
   const double volume = d.volume;
-  if (b[B_SCALE] == 0.0) b[B_SCALE] = 0.01 * volume;
-  b[B_ATTEMPTS] += 1.0;
-  b[B_WINDOW_ATT] += 1.0;
-  const uint32_t seed = ((uint32_t)b[B_SEED]) ^ 0x5a17u;
-  const uint32_t attempt = (uint32_t)b[B_ATTEMPTS];
-  const double u = uniform_d(seed, attempt, 0, 0);
-  const double dv = b[B_SCALE] * 2.0 * (u - 0.5);
-  const double nv = volume + dv;
-  b[B_DV] = dv;
-  b[B_OLD_VOL] = volume;
   for (int k = 0; k < N_ENERGY; ++k) a.saved_energies[s * N_ENERGY + k] = a.energies[s * N_ENERGY + k];
   b[B_OLD_E] = a.energies[s * N_ENERGY + E_POTENTIAL];
-  if (!(nv > 0)) {
-    b[B_REFUSED] = 1.0;
-    b[B_REFUSALS] += 1.0;
-    return;
+  b[B_OLD_VOL] = volume;
+  double ls;
+  if (learned) {
+    // the move was drawn (and refused or screened) by the surrogate's stage 1
+    b[B_ACCEPT] = 1.0;
+    if (b[B_REFUSED] != 0.0 || b[B_SCREENED] != 0.0) return;
+    ls = b[B_LSCALE];
+  } else {
+    if (b[B_SCALE] == 0.0) b[B_SCALE] = 0.01 * volume;
+    b[B_ATTEMPTS] += 1.0;
+    b[B_WINDOW_ATT] += 1.0;
+    const uint32_t seed = ((uint32_t)b[B_SEED]) ^ 0x5a17u;
+    const uint32_t attempt = (uint32_t)b[B_ATTEMPTS];
+    const double u = uniform_d(seed, attempt, 0, 0);
+    const double dv = b[B_SCALE] * 2.0 * (u - 0.5);
+    const double nv = volume + dv;
+    b[B_DV] = dv;
+    if (!(nv > 0)) {
+      b[B_REFUSED] = 1.0;
+      b[B_REFUSALS] += 1.0;
+      return;
+    }
+    ls = cbrt(nv / volume);
+    const double smallest = ls * fmin(fabs(d.box[0]), fmin(fabs(d.box[4]), fabs(d.box[8])));
+    if (d.cutoff > 0.5 * smallest) {  // simulation.js:1016-1035
+      b[B_REFUSED] = 1.0;
+      b[B_REFUSALS] += 1.0;
+      return;
+    }
+    b[B_LSCALE] = ls;
   }
-  const double ls = cbrt(nv / volume);
-  const double smallest = ls * fmin(fabs(d.box[0]), fmin(fabs(d.box[4]), fabs(d.box[8])));
-  if (d.cutoff > 0.5 * smallest) {  // simulation.js:1016-1035
-    b[B_REFUSED] = 1.0;
-    b[B_REFUSALS] += 1.0;
-    return;
-  }
-  b[B_LSCALE] = ls;
   for (int k = 0; k < 9; ++k) d.saved_box[k] = d.box[k];
   d.saved_volume = volume;
   for (int k = 0; k < 3; ++k) d.saved_counts[k] = a.sys[s].cell_counts[k];
@@ -231,14 +250,16 @@ __global__ void k_baro_decide(BaroArgs a) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= a.n_systems) return;
   double *b = a.baro + (long long)s * N_BARO;
-  if (b[B_ACTIVE] == 0.0 || b[B_REFUSED] != 0.0) {
+  if (b[B_ACTIVE] == 0.0 || b[B_REFUSED] != 0.0 || b[B_SCREENED] != 0.0) {
     b[B_ACCEPT] = 1.0;  // nothing moved; nothing to restore
     if (b[B_ACTIVE] != 0.0) {
       b[B_ACCEPT] = 0.0;
       b[B_NEW_E] = b[B_OLD_E];
+      b[B_WEIGHT] = b[B_SCREENED] != 0.0 ? b[B_PRED] : 0.0;
     }
     return;
   }
+  const bool learned = b[B_LEARNED] != 0.0;
   DevSysD &d = a.sysd[s];
   const double kT = b[B_KT];
   const double new_e = a.energies[s * N_ENERGY + E_POTENTIAL];
@@ -248,8 +269,19 @@ __global__ void k_baro_decide(BaroArgs a) {
   b[B_WEIGHT] = w;
   const uint32_t seed = ((uint32_t)b[B_SEED]) ^ 0x5a17u;
   const uint32_t attempt = (uint32_t)b[B_ATTEMPTS];
-  const bool accept = w <= 0.0 || uniform_d(seed, attempt, 1, 0) < exp(-w / kT);
+  bool accept;
+  if (learned && b[B_SCREENING] != 0.0) {
+    // stage 2 of delayed acceptance: min(1, exp(-w/kT) a1(reverse) / a1(forward))
+    const double log_a2 = -w / kT + fmin(0.0, -b[B_PRED_REV] / kT) - fmin(0.0, -b[B_PRED] / kT);
+    accept = log_a2 >= 0.0 || uniform_d(seed, attempt, 1, 0) < exp(log_a2);
+  } else {
+    accept = w <= 0.0 || uniform_d(seed, attempt, 1, 0) < exp(-w / kT);
+  }
   b[B_EXACT_EVALS] += 1.0;
+  if (learned) {  // the exact sample, appended to the surrogate's replay by its training kernel
+    b[B_FEATURE0 + 8] = new_e - b[B_OLD_E];
+    b[B_FEATURE0 + 9] = 1.0;
+  }
   b[B_ACCEPT] = accept ? 1.0 : 0.0;
   if (accept) {
     b[B_ACCEPTED] += 1.0;
@@ -262,7 +294,7 @@ __global__ void k_baro_decide(BaroArgs a) {
     for (int k = 0; k < 3; ++k) a.sys[s].cell_counts[k] = d.saved_counts[k];
     for (int k = 0; k < N_ENERGY; ++k) a.energies[s * N_ENERGY + k] = a.saved_energies[s * N_ENERGY + k];
   }
-  if (b[B_WINDOW_ATT] >= 10.0) {  // simulation.js:1058-1063
+  if (!learned && b[B_WINDOW_ATT] >= 10.0) {  // simulation.js:1058-1063 (stage 1 does it when learned)
     const double rate = b[B_WINDOW_ACC] / b[B_WINDOW_ATT];
     if (rate < 0.25) b[B_SCALE] /= 1.1;
     else if (rate > 0.75) b[B_SCALE] = fmin(b[B_SCALE] * 1.1, 0.3 * d.volume);

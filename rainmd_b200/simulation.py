@@ -56,6 +56,8 @@ _OPTION_NAMES = {
     "pmeOrder": "pme_order", "waterSolver": "water_solver", "learnedBarostat": "learned_barostat",
     "forceAccumulation": "force_accumulation", "neighbourGroupAtoms": "neighbour_group_atoms",
     "nonbondedLanes": "nonbonded_lanes", "spreadAtomsPerBlock": "spread_atoms_per_block",
+    "learnedWarmupMoves": "learned_warmup_moves", "learnedStepsPerMove": "learned_steps_per_move",
+    "learnedRate": "learned_rate",
 }
 
 
@@ -142,6 +144,27 @@ def _struct_dict(obj) -> dict:
     return out
 
 
+SURROGATE_PARAMS = 4801  # W1[64][8], b1[64], W2[64][64], b2[64], W3[64], b3
+
+
+def surrogate_evaluate(params, inputs, targets=None, gradients=False):
+    """The learned barostat's device forward pass (and MSE gradient) on given data:
+    (outputs, gradients or None, loss or None). At most 64 samples of 8 inputs."""
+    lib = L.load()
+    p = np.ascontiguousarray(params, np.float32)
+    x = np.ascontiguousarray(inputs, np.float32).reshape(-1, 8)
+    count = x.shape[0]
+    t = None if targets is None else np.ascontiguousarray(targets, np.float32)
+    out = np.zeros(count, np.float32)
+    grads = np.zeros(SURROGATE_PARAMS, np.float32) if gradients else None
+    loss = C.c_double(0)
+    fp = lambda a: None if a is None else a.ctypes.data_as(C.POINTER(C.c_float))  # noqa: E731
+    status = lib.rmd_surrogate_evaluate(fp(p), fp(x), fp(t), count, fp(out), fp(grads), C.byref(loss))
+    if status != L.RMD_OK:
+        raise _ERRORS.get(status, RainMDError)(lib.rmd_last_error(None).decode())
+    return out, grads, (loss.value if gradients else None)
+
+
 class BatchSimulation:
     """Many independent systems advanced together; every call takes a system index."""
 
@@ -213,6 +236,7 @@ class BatchSimulation:
             "kineticSampledAt": ("before the closing half kick"
                                  if e["kinetic_sampled_before_closing_kick"] else "after the step"),
             "volume": e["volume"], "boxVectors": np.array(e["box_vectors"]),
+            "volumeDerivative": e["volume_derivative"],
         }
 
     def readState(self, index=0) -> dict:
@@ -345,6 +369,16 @@ class BatchSimulation:
                 "tuned": {"neighbourGroupAtoms": table(ms[0:3], (8, 16, 32)),
                           "nonbondedLanes": table(ms[3:6], (8, 16, 32)),
                           "spreadAtomsPerBlock": table(ms[6:9], (4, 8, 16))}}
+
+    def surrogateReport(self, index=0) -> dict:
+        out = L.RmdSurrogateReport()
+        self._check(self._lib.rmd_surrogate_report_at(self._h, index, C.byref(out)))
+        return _struct_dict(out)
+
+    def surrogateWeights(self, index=0) -> np.ndarray:
+        w = np.zeros(SURROGATE_PARAMS, np.float32)
+        self._check(self._lib.rmd_surrogate_weights(self._h, index, w.ctypes.data_as(C.POINTER(C.c_float))))
+        return w
 
     def setKernelShapes(self, neighbourGroupAtoms: int = 0, nonbondedLanes: int = 0,
                         spreadAtomsPerBlock: int = 0):
