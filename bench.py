@@ -77,6 +77,84 @@ def options_for(grid, seed):
             "dispersionCorrection": True}
 
 
+def batch_workload(seed: int = 0, count: int = 64):
+    """64 solvated random-walk chains (20-400 chain atoms), totals log-uniform in 1,000-12,000
+    atoms, each with its own PME grid at <= 1 A spacing."""
+    from rainmd_b200 import synthetic
+    from rainmd_b200.topology import build_system
+
+    out = []
+    for topo, pos in synthetic.batch(count, seed=seed):
+        system = build_system(topo, cutoff=0.9)
+        box = system["boxVectors"]
+        grid = [smooth_at_least(math.ceil(box[4 * d] / 0.1)) for d in range(3)]
+        out.append((system, pos, grid))
+    return out
+
+
+def batched_block(steps: int, seed: int, single_steps: int = 200):
+    """Batched aggregate ns/day of the 64 uneven systems advanced together (one set of launches
+    per step, CUDA-graph blocks of 100 steps): the sum over systems of each one's ns/day in the
+    batch. Beside it the plain path for the same work: the same 64 systems run one after
+    another on this GPU, each alone (aggregate = 64 x ns/day at the summed per-system step
+    time), and the ratio of the two, which is the summed single-system step time over the
+    batch's step time."""
+    from rainmd_b200.simulation import BatchSimulation, GpuSimulation
+
+    items = batch_workload(seed)
+    systems = [s for s, _, _ in items]
+    options = [options_for(g, seed=11 + k) for k, (_, _, g) in enumerate(items)]
+    atoms = [s["topology"]["atomCount"] for s in systems]
+    batch = BatchSimulation(systems, options)
+    for k, (_, pos, _) in enumerate(items):
+        batch.setState(k, pos)
+    batch.initialise()
+    batch.minimise(maxIterations=100, forceTolerance=1000.0)
+    batch.run(500, blockSize=100)
+    batch.benchRun(100, 100, flushL2=True)
+    ms = batch.benchRun(steps, 100, flushL2=True)
+    batch_ns = len(systems) * ns_per_day(ms * 1e-3 / steps)
+    shapes = batch.kernelShapes()
+    batch.release()
+    single_ms = []
+    for k, (system, pos, _) in enumerate(items):
+        sim = GpuSimulation(system, options[k])
+        sim.setState(pos)
+        sim.initialise()
+        sim.minimise(maxIterations=100, forceTolerance=1000.0)
+        sim.run(200, blockSize=100)
+        single_ms.append(sim.benchRun(single_steps, 100, flushL2=True) / single_steps)
+        sim.release()
+    sequential_ms = float(sum(single_ms))
+    sequential_ns = len(systems) * ns_per_day(sequential_ms * 1e-3)
+    return {"systems": len(systems), "atoms_total": int(sum(atoms)), "atoms_min": int(min(atoms)),
+            "atoms_max": int(max(atoms)), "steps": steps, "ms_per_step": ms / steps,
+            "aggregate_ns_per_day": batch_ns,
+            "sequential_single_ms_per_step_summed": sequential_ms,
+            "sequential_single_aggregate_ns_per_day": sequential_ns,
+            "ratio_vs_sequential_singles": batch_ns / sequential_ns,
+            "single_ns_per_day_min": ns_per_day(max(single_ms) * 1e-3),
+            "single_ns_per_day_max": ns_per_day(min(single_ms) * 1e-3),
+            "single_steps": single_steps,
+            "kernel_shapes": {k: shapes[k] for k in ("neighbourGroupAtoms", "nonbondedLanes",
+                                                     "spreadAtomsPerBlock")},
+            "seed": seed}
+
+
+def measured_traffic(kernel: str, workload_name: str):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary of this workload
+    (profiles/<kernel>_<workload>.md, line 'dram_bytes_per_launch: N'), else None."""
+    path = os.path.join(ROOT, "profiles", f"{kernel}_{workload_name}.md")
+    try:
+        with open(path) as handle:
+            for line in handle:
+                if line.strip().startswith("dram_bytes_per_launch:"):
+                    return float(line.split(":", 1)[1].split()[0])
+    except OSError:
+        return None
+    return None
+
+
 def unique_pairs_within(positions, box_length, cutoff):
     from scipy.spatial import cKDTree
 
@@ -214,6 +292,8 @@ def main():
     parser.add_argument("--no-cpu-baseline", action="store_true")
     parser.add_argument("--minimise", type=int, default=200, help="minimiser iterations before dynamics")
     parser.add_argument("--equilibrate", type=int, default=3000, help="untimed steps before warm-up")
+    parser.add_argument("--no-batched", action="store_true", help="skip the 64-system batch measurement")
+    parser.add_argument("--batch-steps", type=int, default=500)
     args = parser.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -292,9 +372,10 @@ def main():
     # CUDA-event launch time on the engine's stream
     pairs = unique_pairs_within(out["positions"].astype(np.float64), system["boxVectors"][0], 0.9)
     nb_ms = sim.timeKernel("nonbonded", reps=50)
-    sim.setNonbonded(32, pairFixed=False)
+    shapes = sim.kernelShapes()
+    sim.setNonbonded(shapes["nonbondedLanes"], pairFixed=False)
     nb_plain_ms = sim.timeKernel("nonbonded", reps=50)
-    sim.setNonbonded(32, pairFixed=True)
+    sim.setNonbonded(shapes["nonbondedLanes"], pairFixed=True)
     pme_ms = sim.timeKernel("pme", reps=50)
     integ_ms = sim.timeKernel("integrate", reps=50)
     rebuild_ms = sim.timeKernel("rebuild", reps=20)
@@ -305,9 +386,11 @@ def main():
     peak, peak_kind = measured_peaks()
     achieved = bytes_nb / (nb_ms * 1e-3) / 1e9
 
+    batched = None if args.no_batched else batched_block(args.batch_steps, seed=rank)
     if rank != 0:
         return
     base = None if args.no_cpu_baseline else cpu_baseline(system, pos, grid, seed=1)
+    traffic = measured_traffic("k_nonbonded", args.workload)
     line = {
         "metric": METRIC, "value": value, "unit": "ns/day", "n_gpus": world, "steps": args.steps,
         "warmup": max(3, args.warmup), "ms_per_step": seconds_per_step * 1e3, "higher_is_better": True,
@@ -319,7 +402,7 @@ def main():
                 "path": "setState(host f64) + initialise + run(K) + readState(host f32)"},
         "gpu_launches": launches,
         "roofline": {"bound": "hbm", "kernel": "k_nonbonded", "achieved": achieved, "peak": peak,
-                     "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                     "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                      "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
                      "algorithmic_bytes": bytes_nb, "unique_pairs_within_cutoff": pairs,
                      "ms_per_launch": nb_ms},
@@ -327,6 +410,9 @@ def main():
                        "pme_7_kernels": pme_ms, "integrate": integ_ms,
                        "rebuild_5_kernels": rebuild_ms,
                        "pme_roofline_frac": bytes_pme / (pme_ms * 1e-3) / 1e9 / peak},
+        "kernel_shapes": {k: shapes[k] for k in ("neighbourGroupAtoms", "nonbondedLanes", "spreadAtomsPerBlock")},
+        "autotune_ms": shapes["tuned"],
+        "batched": batched,
         "clocks": clocks.summary(),
         "physics": {"temperature": e["temperature"], "potential": e["potential"],
                     "rebuild_interval": diag["rebuild_interval"], "skin_violations": diag["skin_violations"],

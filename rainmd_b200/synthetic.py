@@ -75,29 +75,52 @@ def _water_template():
                      [-O_H * math.sin(half), O_H * math.cos(half), 0.0]])
 
 
-def _chain(rng, count):
-    """A self-avoiding-ish random walk with bond lengths 1.0-1.5 Å and 109.5° angles."""
+def _cross(a, b):
+    return (a[1] * b[2] - a[2] * b[1], a[2] * b[0] - a[0] * b[2], a[0] * b[1] - a[1] * b[0])
+
+
+def _unit(v):
+    n = math.sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2])
+    return (v[0] / n, v[1] / n, v[2] / n), n
+
+
+def _chain(rng, count, box=None):
+    """A self-avoiding random walk with bond lengths 1.0-1.5 Å and 109.5° angles: every atom
+    at least 3 Å from all but its two predecessors, by minimum image when `box` is given (a
+    long chain in a small periodic box must not meet its own images). Of up to 200 random
+    dihedrals per step the first that clears is taken, else the one that comes closest."""
     pos = np.zeros((count, 3))
     lengths = rng.uniform(0.10, 0.15, size=max(count - 1, 1))
     theta = math.radians(109.5)
-    direction = np.array([1.0, 0.0, 0.0])
-    previous = np.array([0.0, 1.0, 0.0])
+    c_t, s_t = math.cos(math.pi - theta), math.sin(math.pi - theta)
+    direction = (1.0, 0.0, 0.0)
+    previous = (0.0, 1.0, 0.0)
     for k in range(1, count):
-        for _ in range(50):
+        best, best_d2 = None, -1.0
+        for _ in range(200):
             # rotate `direction` to make the bond angle with the previous bond, random dihedral
-            axis = np.cross(direction, previous)
-            if np.linalg.norm(axis) < 1e-8:
-                axis = np.cross(direction, rng.normal(size=3))
-            axis /= np.linalg.norm(axis)
+            axis = _cross(direction, previous)
+            axis, norm = _unit(axis) if any(axis) else (axis, 0.0)
+            if norm < 1e-8:
+                axis, _ = _unit(_cross(direction, tuple(rng.normal(size=3))))
             phi = rng.uniform(-math.pi, math.pi)
             # new direction: at angle (pi - theta) from current direction, azimuth phi
-            perp = np.cross(axis, direction)
-            new = (math.cos(math.pi - theta) * direction + math.sin(math.pi - theta)
-                   * (math.cos(phi) * axis + math.sin(phi) * perp))
-            new /= np.linalg.norm(new)
-            candidate = pos[k - 1] + lengths[k - 1] * new
-            if k < 3 or np.min(np.linalg.norm(pos[:k - 2] - candidate, axis=1)) > 0.3:
+            perp = _cross(axis, direction)
+            cp, sp = math.cos(phi), math.sin(phi)
+            new, _ = _unit(tuple(c_t * direction[d] + s_t * (cp * axis[d] + sp * perp[d]) for d in range(3)))
+            candidate = pos[k - 1] + lengths[k - 1] * np.array(new)
+            if k < 3:
+                best = (new, candidate)
                 break
+            d = pos[:k - 2] - candidate
+            if box is not None:
+                d -= box * np.round(d / box)
+            d2 = float(np.min(np.sum(d * d, axis=1)))
+            if d2 > best_d2:
+                best, best_d2 = (new, candidate), d2
+            if d2 > 0.09:
+                break
+        new, candidate = best
         previous, direction = direction, new
         pos[k] = candidate
     return pos - pos.mean(axis=0), lengths
@@ -274,7 +297,7 @@ def solvated_chain(n_atoms: int, chain_atoms: int, density: float = 0.997, seed:
     mass = n_water * sum(WATER_MASS) + chain_atoms * TYPES["C"][0] + TYPES["NA"][0]
     box = box_length if box_length is not None else _box_for(mass, density)
     b = _Builder()
-    chain, lengths = _chain(rng, chain_atoms)
+    chain, lengths = _chain(rng, chain_atoms, box)
     chain = chain + box / 2
     b.add_chain(rng, chain, lengths)
     _fill(b, rng, box, n_water, ["NA"], chain, clearance=0.3)
