@@ -156,6 +156,16 @@ __device__ __forceinline__ float erfc_and_gauss(float z, float &gauss) {
   return t * p * gauss;
 }
 
+// 1/sqrt(x) for x > 0: the hardware approximation plus one Newton-Raphson step
+// y <- y (1.5 - 0.5 x y^2), which leaves only the unbiased rounding of three f32 operations.
+// The pair kernel raises this to the 6th and 12th power and sums millions of LJ terms whose
+// repulsive and dispersive halves nearly cancel, so the approximation's own bias (not its
+// size) would otherwise set the error of the LJ total.
+__device__ __forceinline__ float rsqrt_refined(float x) {
+  const float y = rsqrtf(x);
+  return y * fmaf(-0.5f * x * y, y, 1.5f);
+}
+
 // ---------------------------------------------------------------- geometry
 // Minimum image for a reduced box, c then b then a (cpu/forces/geometry.js:27-43). The
 // force kernels use rint(d/L); at an exact half-box tie it may pick the other image of an

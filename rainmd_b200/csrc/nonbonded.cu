@@ -75,7 +75,7 @@ __global__ void __launch_bounds__(128) k_nonbonded(
     const float3 d = make_float3(pw.x - pj.x - S.x, pw.y - pj.y - S.y, pw.z - pj.z - S.z);
     const float r2 = fmaf(d.x, d.x, fmaf(d.y, d.y, d.z * d.z));
     if (r2 <= cut2) {
-      const float inv_r = rsqrtf(r2);
+      const float inv_r = rsqrt_refined(r2);
       const float inv_r2 = inv_r * inv_r;
       const float inv_r6 = inv_r2 * inv_r2 * inv_r2;
       const float2 ab = __ldg(ljrow + __ldg(sorted_type + g));
@@ -118,7 +118,7 @@ __global__ void __launch_bounds__(128) k_nonbonded(
     const float4 pj = posq[j];
     float3 d = min_image(make_float3(pi.x - pj.x, pi.y - pj.y, pi.z - pj.z), s);
     const float r2 = fmaf(d.x, d.x, fmaf(d.y, d.y, d.z * d.z));
-    const float inv_r = rsqrtf(r2);
+    const float inv_r = rsqrt_refined(r2);
     const float inv_r2 = inv_r * inv_r, inv_r6 = inv_r2 * inv_r2 * inv_r2;
     float scalar = 0.f;
     if (prm.y != 0.f || prm.z != 0.f) {
