@@ -141,6 +141,150 @@ def batched_block(steps: int, seed: int, single_steps: int = 200):
             "seed": seed}
 
 
+def learned_barostat_study(ps: float, seed: int = 3, warmup_moves: int = 2000):
+    """23,558 atoms (a 300-atom chain and TIP3P water) started underdense at 0.60 g/cm^3, NPT
+    at 1 bar and 300 K with a volume move every 25 steps, run twice from the same start: the
+    plain exact barostat and the learned one (pre-trained on the first `warmup_moves` exact
+    moves, then screening and training online). Density and isothermal compressibility from
+    the final quarter of each run (the density trajectory by tenths shows the relaxation from
+    the underdense start); exact evaluations and wall time of each."""
+    from rainmd_b200 import synthetic
+    from rainmd_b200.simulation import GpuSimulation
+    from rainmd_b200.topology import build_system
+
+    topo, pos = synthetic.solvated_chain(23558, 300, density=0.60, seed=seed)
+    system = build_system(topo, cutoff=0.9)
+    box = system["boxVectors"]
+    grid = [smooth_at_least(math.ceil(box[4 * d] / 0.1)) for d in range(3)]
+    mass = float(np.sum(system["topology"]["masses"]))
+    steps = int(round(ps / TIMESTEP_PS))
+    moves = steps // 25
+    kT = 0.0083144626 * 300.0
+    out = {"study": "learned-barostat", "atoms": system["topology"]["atomCount"], "grid": grid,
+           "start_density_g_cm3": 0.60, "ps": ps, "moves": moves, "warmup_moves": warmup_moves,
+           "seed": seed}
+    for learned in (False, True):
+        options = options_for(grid, seed=seed)
+        options.update({"pressure": 1.0, "barostatInterval": 25, "learnedBarostat": 1 if learned else 0,
+                        "learnedWarmupMoves": warmup_moves})
+        sim = GpuSimulation(system, options)
+        sim.setState(pos)
+        sim.initialise()
+        sim.minimise(maxIterations=200, forceTolerance=1000.0)
+        volumes = []
+        t0 = time.perf_counter()
+        for _ in range(moves):
+            sim.run(25)
+            volumes.append(sim.diagnostics()["volume"])
+        wall = time.perf_counter() - t0
+        trajectory = mass / np.array(volumes) * 1.66053906660e-3  # g/cm^3 per move
+        v = np.array(volumes[3 * len(volumes) // 4:])  # the final quarter (after the relaxation)
+        density = mass / v * 1.66053906660e-3
+        blocks = np.array([b.mean() for b in np.array_split(density, 20)])
+        d = sim.diagnostics()
+        arm = {"density_by_tenth_of_run": [round(float(x.mean()), 4) for x in np.array_split(trajectory, 10)],
+               "density_g_cm3": float(density.mean()),
+               "density_se": float(blocks.std(ddof=1) / math.sqrt(len(blocks))),
+               # kappa_T = <dV^2> / (kT <V>): nm^3 / (kJ/mol) -> 1/bar is x 6.0221e-2
+               "compressibility_per_bar": float(v.var() / (kT * v.mean()) * 6.02214076e-2),
+               "attempts": d["barostat_attempts"], "accepted": d["barostat_accepted"],
+               "exact_evaluations": d["barostat_exact_evaluations"], "screened": d["barostat_screened"],
+               "window_nm3": d["volume_scale"], "wall_s": wall,
+               "ns_per_day_wall": ns_per_day(wall / (moves * 25))}
+        if learned:
+            r = sim.surrogateReport()
+            after = max(1, r["attempts"] - warmup_moves)
+            arm.update({"surrogate_prediction_error_kT": r["prediction_error_kT"],
+                        "surrogate_train_steps": r["train_steps"],
+                        "exact_saved_after_warmup": 1.0 - (r["exact_evaluations"] - warmup_moves) / after,
+                        "exact_saved_overall": 1.0 - r["exact_evaluations"] / max(1, r["attempts"])})
+        out["learned" if learned else "plain"] = arm
+        sim.release()
+    p, l = out["plain"], out["learned"]
+    out["density_difference_sigma"] = abs(p["density_g_cm3"] - l["density_g_cm3"]) / math.hypot(
+        p["density_se"], l["density_se"])
+    return out
+
+
+def large_combined_study(steps: int, seed: int = 5):
+    """250,000 atoms (a 4,000-atom chain in TIP3P water, PME order 4 on 128^3) advanced in one
+    batch with 16 solvated systems of 5,000-20,000 atoms, all NPT at 1 bar with the learned
+    barostat. Reports ns/day, each kernel group's algorithmic HBM bytes per launch over its
+    CUDA-event time against the measured peak, and the large system's energy terms against
+    the FP64 oracle at the positions and box the run ends with."""
+    import oracle
+    from rainmd_b200 import synthetic
+    from rainmd_b200.simulation import BatchSimulation
+    from rainmd_b200.topology import build_system
+
+    rng = np.random.default_rng(seed)
+    topo, pos = synthetic.solvated_chain(250000, 4000, seed=seed)
+    items = [(build_system(topo, cutoff=0.9), pos, [128, 128, 128])]
+    for k, size in enumerate(np.exp(rng.uniform(math.log(5000), math.log(20000), size=16)).astype(int)):
+        t, p = synthetic.solvated_chain(int(size), int(rng.integers(20, 401)), seed=seed * 100 + k)
+        system = build_system(t, cutoff=0.9)
+        box = system["boxVectors"]
+        items.append((system, p, [smooth_at_least(math.ceil(box[4 * d] / 0.1)) for d in range(3)]))
+    systems = [s for s, _, _ in items]
+    options = []
+    for k, (_, _, grid) in enumerate(items):
+        o = options_for(grid, seed=seed + k)
+        o.update({"pressure": 1.0, "barostatInterval": 25, "learnedBarostat": 1, "learnedWarmupMoves": 200})
+        options.append(o)
+    batch = BatchSimulation(systems, options)
+    for k, (_, p, _) in enumerate(items):
+        batch.setState(k, p)
+    batch.initialise()
+    batch.minimise(maxIterations=100, forceTolerance=1000.0)
+    batch.run(1000, blockSize=100)
+    batch.benchRun(100, 100, flushL2=True)
+    ms = batch.benchRun(steps, 100, flushL2=True)
+    atoms = [s["topology"]["atomCount"] for s in systems]
+    n = sum(atoms)
+    per_step_ns = ns_per_day(ms * 1e-3 / steps)
+    peak, peak_kind = measured_peaks()
+    # algorithmic bytes per launch over the whole batch (the same formulas as the main line;
+    # P from the neighbour estimate rho 4/3 pi rc^3 / 2 per atom)
+    pairs = sum(a * (a / float(s["boxVectors"][0] * s["boxVectors"][4] * s["boxVectors"][8])) *
+                (4.0 / 3.0) * math.pi * 0.9 ** 3 / 2 for a, s in zip(atoms, systems))
+    k3 = sum(g[0] * g[1] * g[2] for _, _, g in items)
+    half = sum(g[0] * g[1] * (g[2] // 2 + 1) for _, _, g in items)
+    kernels = {}
+    for name, nbytes in (("nonbonded", 20 * n + 4 * pairs + 24 * n), ("pme", 32 * n + 24 * n + 16 * k3 + 32 * half),
+                         ("integrate", (52 + 24) * n)):
+        t = batch.timeKernel(name, reps=20)
+        kernels[name] = {"ms": t, "gb_per_s": nbytes / (t * 1e-3) / 1e9, "frac_of_peak": nbytes / (t * 1e-3) / 1e9 / peak}
+    # the large system against the FP64 oracle, at the run's final positions and box
+    state = batch.readState(0)
+    held = state["positions"].astype(np.float64)
+    energy, _ = batch.debugEvaluate(0)
+    ref_system = dict(systems[0])
+    ref_system["boxVectors"] = np.array(state["boxVectors"], dtype=np.float64)
+    alpha = math.sqrt(-math.log(2.0 * 5e-4)) / 0.9
+    expect, _ = oracle.Oracle(ref_system).potential(held, method="PME", alpha=alpha, grid=[128, 128, 128], order=4)
+    errors = {
+        "lennardJones": abs(energy["lennard_jones"] - expect["lennardJones"]) / abs(expect["lennardJones"]),
+        "coulombDirect": abs(energy["coulomb_direct"] - expect["coulombDirect"]) / abs(expect["coulombDirect"]),
+        "coulombReciprocal": abs(energy["coulomb_reciprocal"] - expect["coulombReciprocal"]) / abs(expect["coulombReciprocal"]),
+        "bonded": abs(energy["bonded"] - expect["bonded"]) / abs(expect["bonded"]),
+        "potential_without_dispersion": abs(energy["potential"] - energy["dispersion"] - expect["total"]) / abs(expect["total"]),
+    }
+    reports = [batch.surrogateReport(k) for k in range(len(systems))]
+    out = {"study": "large-combined", "systems": len(systems), "atoms_large": atoms[0], "atoms_total": n,
+           "small_atoms": atoms[1:], "steps": steps, "ms_per_step": ms / steps,
+           "large_ns_per_day": per_step_ns, "aggregate_ns_per_day": per_step_ns * len(systems),
+           "kernels": kernels, "peak_gb_per_s": peak, "peak_source": peak_kind,
+           "large_energy_relative_error_vs_fp64_oracle": errors,
+           "barostat": {"attempts": int(sum(r["attempts"] for r in reports)),
+                        "exact_evaluations": int(sum(r["exact_evaluations"] for r in reports)),
+                        "screened": int(sum(r["screened"] for r in reports)),
+                        "exact_passes": reports[0]["exact_passes"], "skipped_passes": reports[0]["skipped_passes"]},
+           "kernel_shapes": {k: v for k, v in batch.kernelShapes().items() if k != "tuned"},
+           "seed": seed}
+    batch.release()
+    return out
+
+
 def measured_traffic(kernel: str, workload_name: str):
     """DRAM bytes per launch of `kernel` from the committed ncu summary of this workload
     (profiles/<kernel>_<workload>.md, line 'dram_bytes_per_launch: N'), else None."""
@@ -293,6 +437,9 @@ def main():
     parser.add_argument("--minimise", type=int, default=200, help="minimiser iterations before dynamics")
     parser.add_argument("--equilibrate", type=int, default=3000, help="untimed steps before warm-up")
     parser.add_argument("--no-batched", action="store_true", help="skip the 64-system batch measurement")
+    parser.add_argument("--study", choices=["learned-barostat", "large-combined"], default=None,
+                        help="run a study instead of the benchmark and print its JSON line")
+    parser.add_argument("--ps", type=float, default=500.0, help="length of a study run")
     parser.add_argument("--batch-steps", type=int, default=500)
     args = parser.parse_args()
 
@@ -301,6 +448,14 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         run_reference(args, rank, world)
+        return
+    if args.study == "learned-barostat":
+        if rank == 0:
+            print(json.dumps(learned_barostat_study(args.ps)), flush=True)
+        return
+    if args.study == "large-combined":
+        if rank == 0:
+            print(json.dumps(large_combined_study(args.steps)), flush=True)
         return
     # one GPU per process: make this rank's GPU device 0 before any CUDA initialisation
     if world > 1:

@@ -165,24 +165,35 @@ __device__ void settle_positions(UnitState<3> &u, const DevSettle &w, float inv_
   const float mO = w.m_o, mH = w.m_h;
   const float wt = mO + 2.f * mH;
   const float ra = w.ra, rb = w.rb, rc = w.rc;  // geometry constants
-  // centre of mass of the new positions
+  // Everything below is relative to the old apex position o: the new positions are within
+  // a drift of it, so x - o is exact and the centre of mass, the frame and the rebuilt
+  // triangle are all formed from numbers of ~0.1 nm. Formed from absolute coordinates
+  // (several nm) instead, the f32 rounding of the centre of mass and the frame feeds back
+  // through the velocity correction into a kinetic energy that grows exponentially.
+  float o[3], xl[3][3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    o[c] = u.ref[0][c];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) xl[k][c] = u.x[k][c] - o[c];
+  }
   float com[3], b0[3], c0[3], a1[3], b1[3], c1[3];
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
-    b0[c] = u.ref[1][c] - u.ref[0][c];
-    c0[c] = u.ref[2][c] - u.ref[0][c];
-    com[c] = (mO * u.x[0][c] + mH * (u.x[1][c] + u.x[2][c])) / wt;
-    a1[c] = u.x[0][c] - com[c];
-    b1[c] = u.x[1][c] - com[c];
-    c1[c] = u.x[2][c] - com[c];
+    b0[c] = u.ref[1][c] - o[c];
+    c0[c] = u.ref[2][c] - o[c];
+    com[c] = (mO * xl[0][c] + mH * (xl[1][c] + xl[2][c])) / wt;
+    a1[c] = xl[0][c] - com[c];
+    b1[c] = xl[1][c] - com[c];
+    c1[c] = xl[2][c] - com[c];
   }
   // frame: Z along the normal of the old plane, X in the new apex direction
   float n0[3] = {b0[1] * c0[2] - b0[2] * c0[1], b0[2] * c0[0] - b0[0] * c0[2], b0[0] * c0[1] - b0[1] * c0[0]};
   float ax[3] = {a1[1] * n0[2] - a1[2] * n0[1], a1[2] * n0[0] - a1[0] * n0[2], a1[0] * n0[1] - a1[1] * n0[0]};
   float ay[3] = {n0[1] * ax[2] - n0[2] * ax[1], n0[2] * ax[0] - n0[0] * ax[2], n0[0] * ax[1] - n0[1] * ax[0]};
-  const float nz = rsqrtf(n0[0] * n0[0] + n0[1] * n0[1] + n0[2] * n0[2]);
-  const float nx = rsqrtf(ax[0] * ax[0] + ax[1] * ax[1] + ax[2] * ax[2]);
-  const float ny = rsqrtf(ay[0] * ay[0] + ay[1] * ay[1] + ay[2] * ay[2]);
+  const float nz = rsqrt_refined(n0[0] * n0[0] + n0[1] * n0[1] + n0[2] * n0[2]);
+  const float nx = rsqrt_refined(ax[0] * ax[0] + ax[1] * ax[1] + ax[2] * ax[2]);
+  const float ny = rsqrt_refined(ay[0] * ay[0] + ay[1] * ay[1] + ay[2] * ay[2]);
 #pragma unroll
   for (int c = 0; c < 3; ++c) { n0[c] *= nz; ax[c] *= nx; ay[c] *= ny; }
   auto proj = [&](const float *v, const float *e) { return v[0] * e[0] + v[1] * e[1] + v[2] * e[2]; };
@@ -219,8 +230,10 @@ __device__ void settle_positions(UnitState<3> &u, const DevSettle &w, float inv_
   }
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
-    const float da = na[c] - u.x[0][c], db = nb[c] - u.x[1][c], dc = nc[c] - u.x[2][c];
-    u.x[0][c] = na[c]; u.x[1][c] = nb[c]; u.x[2][c] = nc[c];
+    const float da = na[c] - xl[0][c], db = nb[c] - xl[1][c], dc = nc[c] - xl[2][c];
+    u.x[0][c] = o[c] + na[c];
+    u.x[1][c] = o[c] + nb[c];
+    u.x[2][c] = o[c] + nc[c];
     u.v[0][c] = fmaf(da, inv_h, u.v[0][c]);
     u.v[1][c] = fmaf(db, inv_h, u.v[1][c]);
     u.v[2][c] = fmaf(dc, inv_h, u.v[2][c]);
@@ -236,7 +249,7 @@ __device__ void settle_velocities(UnitState<3> &u, const DevSettle &w) {
   for (int k = 0; k < 3; ++k) {
     const int a = P[k][0], b = P[k][1];
     float d[3] = {u.x[a][0] - u.x[b][0], u.x[a][1] - u.x[b][1], u.x[a][2] - u.x[b][2]};
-    const float inv = rsqrtf(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+    const float inv = rsqrt_refined(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
 #pragma unroll
     for (int c = 0; c < 3; ++c) e[k][c] = d[c] * inv;
     rhs[k] = -(e[k][0] * (u.v[a][0] - u.v[b][0]) + e[k][1] * (u.v[a][1] - u.v[b][1]) +

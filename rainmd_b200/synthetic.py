@@ -87,41 +87,45 @@ def _unit(v):
 def _chain(rng, count, box=None):
     """A self-avoiding random walk with bond lengths 1.0-1.5 Å and 109.5° angles: every atom
     at least 3 Å from all but its two predecessors, by minimum image when `box` is given (a
-    long chain in a small periodic box must not meet its own images). Of up to 200 random
-    dihedrals per step the first that clears is taken, else the one that comes closest."""
+    long chain in a small periodic box must not meet its own images). Random dihedrals are
+    tried 16 at a time, up to 192 per step: the first that clears is taken, else the one that
+    comes closest."""
     pos = np.zeros((count, 3))
     lengths = rng.uniform(0.10, 0.15, size=max(count - 1, 1))
     theta = math.radians(109.5)
     c_t, s_t = math.cos(math.pi - theta), math.sin(math.pi - theta)
-    direction = (1.0, 0.0, 0.0)
-    previous = (0.0, 1.0, 0.0)
+    direction = np.array([1.0, 0.0, 0.0])
+    previous = np.array([0.0, 1.0, 0.0])
     for k in range(1, count):
+        axis = np.cross(direction, previous)
+        norm = np.linalg.norm(axis)
+        if norm < 1e-8:
+            axis = np.cross(direction, rng.normal(size=3))
+            norm = np.linalg.norm(axis)
+        axis /= norm
+        perp = np.cross(axis, direction)
         best, best_d2 = None, -1.0
-        for _ in range(200):
-            # rotate `direction` to make the bond angle with the previous bond, random dihedral
-            axis = _cross(direction, previous)
-            axis, norm = _unit(axis) if any(axis) else (axis, 0.0)
-            if norm < 1e-8:
-                axis, _ = _unit(_cross(direction, tuple(rng.normal(size=3))))
-            phi = rng.uniform(-math.pi, math.pi)
-            # new direction: at angle (pi - theta) from current direction, azimuth phi
-            perp = _cross(axis, direction)
-            cp, sp = math.cos(phi), math.sin(phi)
-            new, _ = _unit(tuple(c_t * direction[d] + s_t * (cp * axis[d] + sp * perp[d]) for d in range(3)))
-            candidate = pos[k - 1] + lengths[k - 1] * np.array(new)
+        for _ in range(12):
+            phi = rng.uniform(-math.pi, math.pi, size=16)
+            # new directions at angle (pi - theta) from the current one, azimuths phi
+            new = c_t * direction + s_t * (np.cos(phi)[:, None] * axis + np.sin(phi)[:, None] * perp)
+            new /= np.linalg.norm(new, axis=1)[:, None]
+            cand = pos[k - 1] + lengths[k - 1] * new
             if k < 3:
-                best = (new, candidate)
+                best = (new[0], cand[0])
                 break
-            d = pos[:k - 2] - candidate
+            d = pos[None, :k - 2, :] - cand[:, None, :]
             if box is not None:
                 d -= box * np.round(d / box)
-            d2 = float(np.min(np.sum(d * d, axis=1)))
-            if d2 > best_d2:
-                best, best_d2 = (new, candidate), d2
-            if d2 > 0.09:
+            d2 = np.min(np.einsum("cka,cka->ck", d, d), axis=1)
+            clear = np.nonzero(d2 > 0.09)[0]
+            pick = int(clear[0]) if len(clear) else int(np.argmax(d2))
+            if d2[pick] > best_d2:
+                best, best_d2 = (new[pick], cand[pick]), float(d2[pick])
+            if len(clear):
                 break
-        new, candidate = best
-        previous, direction = direction, new
+        new_dir, candidate = best
+        previous, direction = direction, new_dir
         pos[k] = candidate
     return pos - pos.mean(axis=0), lengths
 
@@ -253,10 +257,11 @@ def _fill(builder, rng, box, n_water, ions, occupied, clearance=0.25):
         g = (np.arange(n) + 0.5) * spacing
         sites = np.array(np.meshgrid(g, g, g, indexing="ij")).reshape(3, -1).T
         if len(occupied):
-            d = sites[:, None, :] - occupied[None, :, :]
-            d -= box * np.round(d / box)
-            keep = np.min(np.linalg.norm(d, axis=-1), axis=1) > clearance
-            sites = sites[keep]
+            from scipy.spatial import cKDTree
+
+            tree = cKDTree(np.mod(occupied, box), boxsize=box)
+            nearest, _ = tree.query(np.mod(sites, box), k=1, distance_upper_bound=clearance * 1.0001)
+            sites = sites[nearest > clearance]
         if len(sites) >= sites_needed:
             break
         n += 1
