@@ -281,7 +281,9 @@ rmd_status rmd_debug_fft(rmd_sim *sim, int32_t system_index, const double *data,
 /* Average device time of one launch of a kernel group on the engine's own stream, by CUDA
  * events over `reps` back-to-back launches: 0 nonbonded (no energy), 1 the seven PME
  * kernels, 2 the fused integrator, 3 bonded, 4 the five list-rebuild kernels, 5 nonbonded
- * with energies. For roofline measurement; no reference counterpart. */
+ * with energies. Positions and velocities are put back afterwards and the forces
+ * re-evaluated, so the simulation continues from where it was. For roofline measurement;
+ * no reference counterpart. */
 rmd_status rmd_debug_time_kernel(rmd_sim *sim, int32_t which, int32_t reps, double *ms_per_launch);
 /* run() with every block's CUDA graph bracketed by CUDA events on the engine's stream;
  * `device_ms` receives the summed device time of the blocks (host bookkeeping between

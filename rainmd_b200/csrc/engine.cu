@@ -2278,6 +2278,15 @@ rmd_status rmd_debug_time_kernel(rmd_sim *sim, int32_t which, int32_t reps, doub
       }
     };
     e.sync();
+    // the timed launches move atoms (integrator) or add into the force array (PME, bonded):
+    // keep the state and put it back afterwards, with forces from a clean evaluation
+    rmd::DevArray<float4> keep_pos, keep_vel, keep_spos;
+    keep_pos.alloc(e.N);
+    keep_vel.alloc(e.N);
+    keep_spos.alloc(e.N);
+    CUDA_OK(cudaMemcpyAsync(keep_pos.p, e.posq.p, sizeof(float4) * e.N, cudaMemcpyDeviceToDevice, e.stream));
+    CUDA_OK(cudaMemcpyAsync(keep_vel.p, e.vel.p, sizeof(float4) * e.N, cudaMemcpyDeviceToDevice, e.stream));
+    CUDA_OK(cudaMemcpyAsync(keep_spos.p, e.spos.p, sizeof(float4) * e.N, cudaMemcpyDeviceToDevice, e.stream));
     one();  // warm
     cudaEvent_t a, b;
     CUDA_OK(cudaEventCreate(&a));
@@ -2292,6 +2301,15 @@ rmd_status rmd_debug_time_kernel(rmd_sim *sim, int32_t which, int32_t reps, doub
     cudaEventDestroy(b);
     CUDA_OK(cudaGetLastError());
     *ms_per_launch = ms / reps;
+    CUDA_OK(cudaMemcpyAsync(e.posq.p, keep_pos.p, sizeof(float4) * e.N, cudaMemcpyDeviceToDevice, e.stream));
+    CUDA_OK(cudaMemcpyAsync(e.vel.p, keep_vel.p, sizeof(float4) * e.N, cudaMemcpyDeviceToDevice, e.stream));
+    CUDA_OK(cudaMemcpyAsync(e.spos.p, keep_spos.p, sizeof(float4) * e.N, cudaMemcpyDeviceToDevice, e.stream));
+    e.evaluate(true, false);
+    e.sync();
+    for (auto &h : e.hs) h.steps_since_rebuild = 0;
+    keep_pos.release();
+    keep_vel.release();
+    keep_spos.release();
   });
 }
 
