@@ -166,6 +166,10 @@ struct Engine {
   std::vector<HostSystem> hs;
   int S = 0, N = 0;
   cudaStream_t stream = nullptr;
+  // the reciprocal-space branch of a force evaluation runs on `side`, forked from and joined
+  // back to `stream` with events (inside a captured graph these become parallel branches)
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   std::string last_error;
   int nb_lanes = 32;
   int group_atoms = 8;   // atoms per neighbour-search warp
@@ -234,6 +238,9 @@ struct Engine {
 
   ~Engine() {
     for (auto &kv : graphs) cudaGraphExecDestroy(kv.second);
+    if (ev_fork) cudaEventDestroy(ev_fork);
+    if (ev_join) cudaEventDestroy(ev_join);
+    if (side) cudaStreamDestroy(side);
     if (stream) cudaStreamDestroy(stream);
   }
 
@@ -443,7 +450,19 @@ void Engine::build(int count, const rmd_system *systems, const rmd_options *opti
   }
   for (auto &h : hs)
     if (h.order != pme_order) throw Error(RMD_ERR_INVALID, "every system of a batch must use the same PME order");
-  CUDA_OK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+  // A blocking stream: work on it is ordered after the legacy default stream's, which is
+  // where the host-side uploads (cudaMemcpy from pageable memory, which may return before
+  // its DMA lands; cudaMemset, which is asynchronous) go. A non-blocking stream would let a
+  // kernel read a buffer before such an upload had finished.
+  CUDA_OK(cudaStreamCreateWithFlags(&stream, cudaStreamDefault));
+  // the reciprocal branch is a chain of small latency-bound kernels next to one large pair
+  // kernel: at higher priority its blocks take SM slots as they free instead of after the
+  // pair kernel's last wave
+  int lowest = 0, highest = 0;
+  CUDA_OK(cudaDeviceGetStreamPriorityRange(&lowest, &highest));
+  CUDA_OK(cudaStreamCreateWithPriority(&side, cudaStreamDefault, highest));
+  CUDA_OK(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
+  CUDA_OK(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
   upload_all(src);
 }
 
@@ -865,11 +884,11 @@ void Engine::upload_all(const std::vector<const rmd_system *> &src) {
       const int lines = nx * ny, pairs = (lines + 1) / 2;
       const int mz = lines_per_block(pairs, nz, 64);
       for (int p = 0; p < pairs; p += mz) tz.push_back(FftTask{s, 0, p, std::min(mz, pairs - p)});
-      const int my = lines_per_block(nx * nzh, ny, nzh);
+      const int my = lines_per_block(nx * nzh, ny + 1, nzh);  // y and x lines are padded to n + 1
       for (int x = 0; x < nx; ++x)
         for (int k = 0; k < nzh; k += my) ty.push_back(FftTask{s, x, k, std::min(my, nzh - k)});
       task_x_start[s] = (int)tx.size();
-      const int mx = lines_per_block(ny * nzh, nx, nzh);
+      const int mx = lines_per_block(ny * nzh, nx + 1, nzh);
       for (int y = 0; y < ny; ++y)
         for (int k = 0; k < nzh; k += mx) tx.push_back(FftTask{s, y, k, std::min(mx, nzh - k)});
     }
@@ -1216,10 +1235,22 @@ void Engine::record_forces(bool rebuild, bool energy) {
     launch_rebuild(c, stream);
     recorded += 5;
   }
+  // The reciprocal-space chain up to the convolved grid only reads positions, so it runs
+  // concurrently with the pair and bonded kernels; the gather, which adds into the force
+  // array the pair kernel stores, waits for both branches.
+  if (pme_on) {
+    CUDA_OK(cudaEventRecord(ev_fork, stream));
+    CUDA_OK(cudaStreamWaitEvent(side, ev_fork, 0));
+    launch_pme_grid(c, energy, side);
+    CUDA_OK(cudaEventRecord(ev_join, side));
+  }
   launch_nonbonded(c, energy, nb_lanes, stream);
   launch_bonded(c, energy, stream);
-  launch_pme(c, energy, stream);
-  recorded += 1 + (n_bonds + n_angles + n_tors + n_rest > 0 ? 1 : 0) + (pme_on ? 7 : 0);
+  if (pme_on) {
+    CUDA_OK(cudaStreamWaitEvent(stream, ev_join, 0));
+    launch_pme_gather(c, stream);
+  }
+  recorded += 1 + (n_bonds + n_angles + n_tors + n_rest > 0 ? 1 : 0) + pme_launches(c);
   if (energy) {
     launch_molecular_virial(c, stream);
     launch_energy_reduce(segments.p, n_segments, seg_out.p, energies.p, sysd.p, S, stream);
@@ -2429,8 +2460,9 @@ rmd_status rmd_debug_fft(rmd_sim *sim, int32_t s, const double *data, double *ha
     e.sync();
     std::vector<long long> fx(pts);
     for (size_t k = 0; k < pts; ++k) fx[k] = (long long)std::llround(data[k] * rmd::FORCE_SCALE);
-    CUDA_OK(cudaMemset(e.fixed_grid.p, 0, e.fixed_grid.bytes()));
-    CUDA_OK(cudaMemcpy(e.fixed_grid.p + ds.grid_base, fx.data(), sizeof(long long) * pts, cudaMemcpyHostToDevice));
+    CUDA_OK(cudaMemsetAsync(e.fixed_grid.p, 0, e.fixed_grid.bytes(), e.stream));
+    CUDA_OK(cudaMemcpyAsync(e.fixed_grid.p + ds.grid_base, fx.data(), sizeof(long long) * pts,
+                            cudaMemcpyHostToDevice, e.stream));
     const rmd::LaunchCtx c = e.ctx();
     rmd::launch_fft_forward(c, e.stream);
     e.sync();

@@ -145,6 +145,10 @@ void launch_nonbonded(const LaunchCtx &c, bool energy, int lanes, cudaStream_t s
 void launch_bonded(const LaunchCtx &c, bool energy, cudaStream_t stream);
 void launch_molecular_virial(const LaunchCtx &c, cudaStream_t stream);
 void launch_pme(const LaunchCtx &c, bool energy, cudaStream_t stream);
+// launch_pme split in two: the grid chain (spread .. inverse transform) and the force gather
+void launch_pme_grid(const LaunchCtx &c, bool energy, cudaStream_t stream);
+void launch_pme_gather(const LaunchCtx &c, cudaStream_t stream);
+int pme_launches(const LaunchCtx &c);  // kernels launch_pme issues
 void launch_fft_forward(const LaunchCtx &c, cudaStream_t stream);
 void launch_spread_only(const LaunchCtx &c, cudaStream_t stream);
 void launch_fft_inverse(const LaunchCtx &c, cudaStream_t stream);

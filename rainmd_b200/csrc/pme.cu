@@ -7,14 +7,15 @@
 // force gather. The spline order is a template parameter (4 or 5).
 //
 // B200 design (not the reference's pass structure):
-//   spread   one thread per atom, 64-bit fixed-point integer atomics (deterministic);
+//   spread   ORDER^2 threads per atom, 64-bit fixed-point integer atomics (deterministic);
 //   z pass   R2C: two real z-lines packed as one complex line, FFT in shared memory,
 //            split into two half spectra; also converts fixed point -> f32 and zeroes the
 //            fixed grid for the next step (no separate clear/convert kernels);
 //   y pass   complex FFT along y on the half spectrum, in place;
 //   x pass   forward FFT along x, the Ewald convolution and the FP64 energy partial, and
 //            the inverse FFT along x, all while the lines are in shared memory;
-//   y pass   inverse; z pass C2R back to a real f32 grid; gather one thread per atom.
+//   y pass   inverse; z pass C2R back to a real f32 grid; gather four threads per atom.
+// Lines filled by a transpose (y and x passes) are padded to n + 1 in shared memory.
 // The FFT is a mixed-radix (4, 2, 3, 5) Stockham autosort over lines held in shared
 // memory; a host-built task table gives each block a set of lines of one system, so
 // systems with different grid sizes run in the same launch.
@@ -73,13 +74,13 @@ __device__ __forceinline__ void dft_small(float2 *v, bool inv) {
 
 template <int R>
 __device__ __forceinline__ void stockham_stage(const float2 *__restrict__ in, float2 *__restrict__ out,
-                                               int lines, int N, int Ns, const float2 *__restrict__ tw,
+                                               int lines, int N, int ld, int Ns, const float2 *__restrict__ tw,
                                                bool inv) {
   const int per_line = N / R;
   const int stride_tw = N / (Ns * R);
   for (int idx = threadIdx.x; idx < lines * per_line; idx += blockDim.x) {
     const int line = idx / per_line, j = idx - line * per_line;
-    const float2 *src = in + line * N;
+    const float2 *src = in + line * ld;
     float2 v[R];
     const int k = j % Ns;
 #pragma unroll
@@ -91,23 +92,25 @@ __device__ __forceinline__ void stockham_stage(const float2 *__restrict__ in, fl
       v[r] = cmul(v[r], w);
     }
     dft_small<R>(v, inv);
-    float2 *dst = out + line * N + (j / Ns) * Ns * R + k;
+    float2 *dst = out + line * ld + (j / Ns) * Ns * R + k;
 #pragma unroll
     for (int r = 0; r < R; ++r) dst[r * Ns] = v[r];
   }
 }
 
-// Transform `lines` lines of length N held in a; returns the buffer holding the result.
-__device__ float2 *fft_lines(float2 *a, float2 *b, int lines, int N, const FftAxis &ax,
+// Transform `lines` lines of length N held in a, line l starting at a + l * ld (ld >= N;
+// lines filled by a transpose use ld = N + 1 so that the transposing accesses, which step
+// by ld, fall in different shared-memory banks); returns the buffer holding the result.
+__device__ float2 *fft_lines(float2 *a, float2 *b, int lines, int N, int ld, const FftAxis &ax,
                              const float2 *__restrict__ tw, bool inv) {
   int Ns = 1;
   for (int st = 0; st < ax.nstages; ++st) {
     const int R = ax.radix[st];
     __syncthreads();
-    if (R == 4) stockham_stage<4>(a, b, lines, N, Ns, tw, inv);
-    else if (R == 2) stockham_stage<2>(a, b, lines, N, Ns, tw, inv);
-    else if (R == 3) stockham_stage<3>(a, b, lines, N, Ns, tw, inv);
-    else stockham_stage<5>(a, b, lines, N, Ns, tw, inv);
+    if (R == 4) stockham_stage<4>(a, b, lines, N, ld, Ns, tw, inv);
+    else if (R == 2) stockham_stage<2>(a, b, lines, N, ld, Ns, tw, inv);
+    else if (R == 3) stockham_stage<3>(a, b, lines, N, ld, Ns, tw, inv);
+    else stockham_stage<5>(a, b, lines, N, ld, Ns, tw, inv);
     Ns *= R;
     float2 *t = a;
     a = b;
@@ -191,7 +194,7 @@ __global__ void __launch_bounds__(256) k_fft_z_r2c(const FftTask *__restrict__ t
     }
     bufa[idx] = make_float2(re, im);
   }
-  float2 *r = fft_lines(bufa, bufb, M, N, pl.axis[2], twiddles + pl.axis[2].tw_base, false);
+  float2 *r = fft_lines(bufa, bufb, M, N, N, pl.axis[2], twiddles + pl.axis[2].tw_base, false);
   float2 *h = half + s.half_base;
   for (int idx = threadIdx.x; idx < M * nzh; idx += blockDim.x) {
     const int p = idx / nzh, k = idx - p * nzh;
@@ -241,7 +244,7 @@ __global__ void __launch_bounds__(256) k_fft_z_c2r(const FftTask *__restrict__ t
     }
     bufa[idx] = make_float2(a.x - b.y, a.y + b.x);  // A + iB
   }
-  float2 *r = fft_lines(bufa, bufb, M, N, pl.axis[2], twiddles + pl.axis[2].tw_base, true);
+  float2 *r = fft_lines(bufa, bufb, M, N, N, pl.axis[2], twiddles + pl.axis[2].tw_base, true);
   float *g = real_grid + s.grid_base;
   for (int idx = threadIdx.x; idx < M * N; idx += blockDim.x) {
     const int p = idx / N, k = idx - p * N;
@@ -265,14 +268,15 @@ __global__ void __launch_bounds__(256) k_fft_y(const FftTask *__restrict__ tasks
   const int ny = s.grid[1], nzh = s.grid[2] / 2 + 1;
   const int x = t.fixed, kz0 = t.first, M = t.count;
   float2 *h = half + s.half_base + (long long)x * ny * nzh + kz0;
+  const int ld = ny + 1;  // padded lines (bank-conflict-free transpose)
   for (int idx = threadIdx.x; idx < ny * M; idx += blockDim.x) {
     const int y = idx / M, m = idx - y * M;
-    bufa[m * ny + y] = h[(long long)y * nzh + m];
+    bufa[m * ld + y] = h[(long long)y * nzh + m];
   }
-  float2 *r = fft_lines(bufa, bufb, M, ny, pl.axis[1], twiddles + pl.axis[1].tw_base, inverse != 0);
+  float2 *r = fft_lines(bufa, bufb, M, ny, ld, pl.axis[1], twiddles + pl.axis[1].tw_base, inverse != 0);
   for (int idx = threadIdx.x; idx < ny * M; idx += blockDim.x) {
     const int y = idx / M, m = idx - y * M;
-    h[(long long)y * nzh + m] = r[m * ny + y];
+    h[(long long)y * nzh + m] = r[m * ld + y];
   }
 }
 
@@ -296,11 +300,12 @@ __global__ void __launch_bounds__(256) k_fft_x_convolve(const FftTask *__restric
   const int y = t.fixed, kz0 = t.first, M = t.count;
   const long long stride = (long long)ny * nzh;
   float2 *h = half + s.half_base + (long long)y * nzh + kz0;
+  const int ld = nx + 1;  // padded lines (bank-conflict-free transpose)
   for (int idx = threadIdx.x; idx < nx * M; idx += blockDim.x) {
     const int x = idx / M, m = idx - x * M;
-    bufa[m * nx + x] = h[x * stride + m];
+    bufa[m * ld + x] = h[x * stride + m];
   }
-  float2 *r = fft_lines(bufa, bufb, M, nx, pl.axis[0], twiddles + pl.axis[0].tw_base, false);
+  float2 *r = fft_lines(bufa, bufb, M, nx, ld, pl.axis[0], twiddles + pl.axis[0].tw_base, false);
   const double volume = sysd[t.sys].volume;
   const double alpha = sysd[t.sys].alpha;
   const float factor = (float)(M_PI * M_PI / (alpha * alpha));
@@ -312,9 +317,10 @@ __global__ void __launch_bounds__(256) k_fft_x_convolve(const FftTask *__restric
     const int m = idx / nx, mx = idx - m * nx;
     const int kz = kz0 + m;
     const int kx = mx <= nx / 2 ? mx : mx - nx;
-    float2 v = r[idx];
+    const int at = m * ld + mx;
+    float2 v = r[at];
     if (kx == 0 && ky == 0 && kz == 0) {
-      r[idx] = make_float2(0.f, 0.f);
+      r[at] = make_float2(0.f, 0.f);
       continue;
     }
     const float fx = (float)kx, fy = (float)ky, fz = (float)kz;
@@ -330,13 +336,13 @@ __global__ void __launch_bounds__(256) k_fft_x_convolve(const FftTask *__restric
       virial += ek * (1.0 + (double)factor * (double)m2);
     }
     const float sc = kernel * two_pref;
-    r[idx] = make_float2(v.x * sc, v.y * sc);
+    r[at] = make_float2(v.x * sc, v.y * sc);
   }
   float2 *other = (r == bufa) ? bufb : bufa;
-  float2 *q = fft_lines(r, other, M, nx, pl.axis[0], twiddles + pl.axis[0].tw_base, true);
+  float2 *q = fft_lines(r, other, M, nx, ld, pl.axis[0], twiddles + pl.axis[0].tw_base, true);
   for (int idx = threadIdx.x; idx < nx * M; idx += blockDim.x) {
     const int x = idx / M, m = idx - x * M;
-    h[x * stride + m] = q[m * nx + x];
+    h[x * stride + m] = q[m * ld + x];
   }
   if (ENERGY) {
     energy = warp_sum(energy);
@@ -405,18 +411,105 @@ __global__ void k_gather(const float4 *__restrict__ posq, const int *__restrict_
   add_fixed(force + 2 * (long long)n_atoms + i, -(su * s.recip[6] + sv * s.recip[7] + sw * s.recip[8]));
 }
 
-void launch_pme(const LaunchCtx &c, bool energy, cudaStream_t stream) {
-  if (!c.pme_on) return;
+// Force gather with four threads per atom (atoms in cell order, for locality of the grid
+// reads): thread q sums the x-planes kx = q, q + 4 (< ORDER), the four partial gradients are
+// combined with shuffles, and the first thread adds the force. One thread per atom leaves
+// most of the GPU idle at these sizes (23,558 atoms are 185 blocks of 128).
+template <int ORDER>
+__global__ void k_gather4(const float4 *__restrict__ posq, const int *__restrict__ sorted_orig,
+                          const int *__restrict__ sys_of_atom, const DevSys *__restrict__ sys,
+                          const float *__restrict__ real_grid, unsigned long long *__restrict__ force,
+                          int n_atoms) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int slot = t >> 2, q = t & 3;
+  const bool valid = slot < n_atoms;
+  const int i = valid ? sorted_orig[slot] : 0;
+  const float4 p = valid ? posq[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+  float gu = 0.f, gv = 0.f, gw = 0.f;
+  const DevSys &s = sys[sys_of_atom[i]];
+  if (valid && p.w != 0.f) {
+    float w[3][ORDER], dw[3][ORDER];
+    int base[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const float f = p.x * s.recip[d] + p.y * s.recip[3 + d] + p.z * s.recip[6 + d];
+      const float scaled = (f - floorf(f)) * (float)s.grid[d];
+      const float fl = floorf(scaled);
+      base[d] = (int)fl;
+      bspline<ORDER>(scaled - fl, w[d], dw[d]);
+    }
+    const int nx = s.grid[0], ny = s.grid[1], nz = s.grid[2];
+    const float *g = real_grid + s.grid_base;
+    int iz[ORDER];
+#pragma unroll
+    for (int kz = 0; kz < ORDER; ++kz) iz[kz] = wrap_index(base[2] + kz - ORDER + 1, nz);
+    // this thread's x-planes: kx = q (and q + 4 for order 5), weights selected without
+    // branching so the four threads of an atom run the y and z loops in step
+    for (int kx = q; kx < ORDER; kx += 4) {
+      float wx = w[0][0], dwx = dw[0][0];
+#pragma unroll
+      for (int k = 1; k < ORDER; ++k) {
+        wx = (kx == k) ? w[0][k] : wx;
+        dwx = (kx == k) ? dw[0][k] : dwx;
+      }
+      const int ix = wrap_index(base[0] + kx - ORDER + 1, nx);
+#pragma unroll
+      for (int ky = 0; ky < ORDER; ++ky) {
+        const int iy = wrap_index(base[1] + ky - ORDER + 1, ny);
+        const float *rowp = g + ((long long)ix * ny + iy) * nz;
+        const float wxy = wx * w[1][ky], dxy = dwx * w[1][ky], wdy = wx * dw[1][ky];
+#pragma unroll
+        for (int kz = 0; kz < ORDER; ++kz) {
+          const float v = __ldg(rowp + iz[kz]);
+          gu = fmaf(dxy * w[2][kz], v, gu);
+          gv = fmaf(wdy * w[2][kz], v, gv);
+          gw = fmaf(wxy * dw[2][kz], v, gw);
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int o = 1; o < 4; o <<= 1) {
+    gu += __shfl_xor_sync(0xffffffffu, gu, o);
+    gv += __shfl_xor_sync(0xffffffffu, gv, o);
+    gw += __shfl_xor_sync(0xffffffffu, gw, o);
+  }
+  if (!valid || q != 0 || p.w == 0.f) return;
+  // the convolved grid already carries the Coulomb prefactor (and the factor 2)
+  const float su = gu * (float)s.grid[0] * p.w, sv = gv * (float)s.grid[1] * p.w, sw = gw * (float)s.grid[2] * p.w;
+  add_fixed(force + i, -(su * s.recip[0] + sv * s.recip[1] + sw * s.recip[2]));
+  add_fixed(force + n_atoms + i, -(su * s.recip[3] + sv * s.recip[4] + sw * s.recip[5]));
+  add_fixed(force + 2 * (long long)n_atoms + i, -(su * s.recip[6] + sv * s.recip[7] + sw * s.recip[8]));
+}
+
+static void launch_gather(const LaunchCtx &c, cudaStream_t stream) {
   const int n = c.n_atoms, tb = 128;
-  const int per_block = c.spread_atoms > 0 ? c.spread_atoms : 8;
-  const int blocks = (n + per_block - 1) / per_block;
+  const int blocks = (int)(((long long)n * 4 + tb - 1) / tb);
   if (c.pme_order == 4)
-    k_spread<4><<<blocks, per_block * 16, 0, stream>>>(c.posq, c.sys_of_atom, c.sys, c.fixed_grid, n);
+    k_gather4<4><<<blocks, tb, 0, stream>>>(c.posq, c.sorted_orig, c.sys_of_atom, c.sys, c.real_grid, c.force, n);
   else
-    k_spread<5><<<blocks, per_block * 25, 0, stream>>>(c.posq, c.sys_of_atom, c.sys, c.fixed_grid, n);
-  k_fft_z_r2c<<<c.n_tasks_z, 256, 0, stream>>>(c.tasks_z, c.sys, c.fft_plans, c.twiddles,
-                                                c.fixed_grid, c.half);
+    k_gather4<5><<<blocks, tb, 0, stream>>>(c.posq, c.sorted_orig, c.sys_of_atom, c.sys, c.real_grid, c.force, n);
+}
+
+// Forward transform of the spread grid to the half spectrum (z and y; x is left to the caller).
+static void launch_forward_zy(const LaunchCtx &c, cudaStream_t stream) {
+  k_fft_z_r2c<<<c.n_tasks_z, 256, 0, stream>>>(c.tasks_z, c.sys, c.fft_plans, c.twiddles, c.fixed_grid, c.half);
   k_fft_y<<<c.n_tasks_y, 256, 0, stream>>>(c.tasks_y, c.sys, c.fft_plans, c.twiddles, c.half, 0);
+}
+
+static void launch_inverse_yz(const LaunchCtx &c, cudaStream_t stream) {
+  k_fft_y<<<c.n_tasks_y, 256, 0, stream>>>(c.tasks_y, c.sys, c.fft_plans, c.twiddles, c.half, 1);
+  k_fft_z_c2r<<<c.n_tasks_z, 256, 0, stream>>>(c.tasks_z, c.sys, c.fft_plans, c.twiddles, c.half, c.real_grid);
+}
+
+int pme_launches(const LaunchCtx &c) { return c.pme_on ? 7 : 0; }
+
+// Everything up to the convolved real grid: spreading, forward transform, convolution (and
+// energy), inverse transform.
+void launch_pme_grid(const LaunchCtx &c, bool energy, cudaStream_t stream) {
+  if (!c.pme_on) return;
+  launch_spread_only(c, stream);
+  launch_forward_zy(c, stream);
   if (energy)
     k_fft_x_convolve<true><<<c.n_tasks_x, 256, 0, stream>>>(c.tasks_x, c.sys, c.sysd, c.fft_plans,
                                                             c.twiddles, c.moduli, c.half, c.e_pme,
@@ -425,13 +518,27 @@ void launch_pme(const LaunchCtx &c, bool energy, cudaStream_t stream) {
     k_fft_x_convolve<false><<<c.n_tasks_x, 256, 0, stream>>>(c.tasks_x, c.sys, c.sysd, c.fft_plans,
                                                              c.twiddles, c.moduli, c.half, c.e_pme,
                                                              c.e_pme_vir);
-  k_fft_y<<<c.n_tasks_y, 256, 0, stream>>>(c.tasks_y, c.sys, c.fft_plans, c.twiddles, c.half, 1);
-  k_fft_z_c2r<<<c.n_tasks_z, 256, 0, stream>>>(c.tasks_z, c.sys, c.fft_plans, c.twiddles, c.half,
-                                                c.real_grid);
-  if (c.pme_order == 4)
-    k_gather<4><<<(n + tb - 1) / tb, tb, 0, stream>>>(c.posq, c.sys_of_atom, c.sys, c.real_grid, c.force, n);
+  launch_inverse_yz(c, stream);
+}
+
+void launch_pme_gather(const LaunchCtx &c, cudaStream_t stream) {
+  if (c.pme_on) launch_gather(c, stream);
+}
+
+void launch_pme(const LaunchCtx &c, bool energy, cudaStream_t stream) {
+  if (!c.pme_on) return;
+  launch_spread_only(c, stream);
+  launch_forward_zy(c, stream);
+  if (energy)
+    k_fft_x_convolve<true><<<c.n_tasks_x, 256, 0, stream>>>(c.tasks_x, c.sys, c.sysd, c.fft_plans,
+                                                            c.twiddles, c.moduli, c.half, c.e_pme,
+                                                            c.e_pme_vir);
   else
-    k_gather<5><<<(n + tb - 1) / tb, tb, 0, stream>>>(c.posq, c.sys_of_atom, c.sys, c.real_grid, c.force, n);
+    k_fft_x_convolve<false><<<c.n_tasks_x, 256, 0, stream>>>(c.tasks_x, c.sys, c.sysd, c.fft_plans,
+                                                             c.twiddles, c.moduli, c.half, c.e_pme,
+                                                             c.e_pme_vir);
+  launch_inverse_yz(c, stream);
+  launch_gather(c, stream);
 }
 
 // Debug: forward R2C then C2R of a given real grid (already in real_grid as f32 values
@@ -448,39 +555,36 @@ __global__ void k_fft_x_plain(const FftTask *__restrict__ tasks, const DevSys *_
   const int y = t.fixed, kz0 = t.first, M = t.count;
   const long long stride = (long long)ny * nzh;
   float2 *h = half + s.half_base + (long long)y * nzh + kz0;
+  const int ld = nx + 1;
   for (int idx = threadIdx.x; idx < nx * M; idx += blockDim.x) {
     const int x = idx / M, m = idx - x * M;
-    bufa[m * nx + x] = h[x * stride + m];
+    bufa[m * ld + x] = h[x * stride + m];
   }
-  float2 *r = fft_lines(bufa, bufb, M, nx, pl.axis[0], twiddles + pl.axis[0].tw_base, inverse != 0);
+  float2 *r = fft_lines(bufa, bufb, M, nx, ld, pl.axis[0], twiddles + pl.axis[0].tw_base, inverse != 0);
   for (int idx = threadIdx.x; idx < nx * M; idx += blockDim.x) {
     const int x = idx / M, m = idx - x * M;
-    h[x * stride + m] = r[m * nx + x];
+    h[x * stride + m] = r[m * ld + x];
   }
 }
 
 void launch_spread_only(const LaunchCtx &c, cudaStream_t stream) {
-  const int n = c.n_atoms, tb = 128;
+  const int n = c.n_atoms;
+  const int per_block = c.spread_atoms > 0 ? c.spread_atoms : 8;
+  const int blocks = (n + per_block - 1) / per_block;
   if (c.pme_order == 4)
-    k_spread<4><<<(int)(((long long)n * 16 + tb - 1) / tb), tb, 0, stream>>>(c.posq, c.sys_of_atom, c.sys,
-                                                                            c.fixed_grid, n);
+    k_spread<4><<<blocks, per_block * 16, 0, stream>>>(c.posq, c.sys_of_atom, c.sys, c.fixed_grid, n);
   else
-    k_spread<5><<<(int)(((long long)n * 25 + tb - 1) / tb), tb, 0, stream>>>(c.posq, c.sys_of_atom, c.sys,
-                                                                            c.fixed_grid, n);
+    k_spread<5><<<blocks, per_block * 25, 0, stream>>>(c.posq, c.sys_of_atom, c.sys, c.fixed_grid, n);
 }
 
 void launch_fft_forward(const LaunchCtx &c, cudaStream_t stream) {
-  k_fft_z_r2c<<<c.n_tasks_z, 256, 0, stream>>>(c.tasks_z, c.sys, c.fft_plans, c.twiddles,
-                                                c.fixed_grid, c.half);
-  k_fft_y<<<c.n_tasks_y, 256, 0, stream>>>(c.tasks_y, c.sys, c.fft_plans, c.twiddles, c.half, 0);
+  launch_forward_zy(c, stream);
   k_fft_x_plain<<<c.n_tasks_x, 256, 0, stream>>>(c.tasks_x, c.sys, c.fft_plans, c.twiddles, c.half, 0);
 }
 
 void launch_fft_inverse(const LaunchCtx &c, cudaStream_t stream) {
   k_fft_x_plain<<<c.n_tasks_x, 256, 0, stream>>>(c.tasks_x, c.sys, c.fft_plans, c.twiddles, c.half, 1);
-  k_fft_y<<<c.n_tasks_y, 256, 0, stream>>>(c.tasks_y, c.sys, c.fft_plans, c.twiddles, c.half, 1);
-  k_fft_z_c2r<<<c.n_tasks_z, 256, 0, stream>>>(c.tasks_z, c.sys, c.fft_plans, c.twiddles, c.half,
-                                                c.real_grid);
+  launch_inverse_yz(c, stream);
 }
 
 }  // namespace rmd
