@@ -141,9 +141,18 @@ __device__ __forceinline__ float3 rng_gaussian3(uint32_t seed, uint32_t atom, ui
 // erfc(z) = t * P(t) * exp(-z^2), t = 1/(1 + z/2). P is this project's own degree-8 fit
 // (rainmd_b200/fit_erfc.py: relative error 2.0e-8 in exact arithmetic over z in [0, 5],
 // 3e-7 at f32 evaluation). Returns erfc and leaves exp(-z^2) in `gauss` for the force.
+// Hardware approximate reciprocal (one MUFU instruction, within 1 ulp).
+__device__ __forceinline__ float rcp_approx(float x) {
+  float y;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
 __device__ __forceinline__ float erfc_and_gauss(float z, float &gauss) {
   gauss = __expf(-z * z);
-  float t = __frcp_rn(fmaf(0.5f, z, 1.0f));
+  // t in (0, 1]: a 1-ulp reciprocal moves erfc by ~1e-7 relative, well inside the f32 pair
+  // arithmetic's own error, at a fraction of the correctly rounded division's cost
+  float t = rcp_approx(fmaf(0.5f, z, 1.0f));
   float p = -4.967514911e-02f;
   p = fmaf(p, t, 2.366592171e-01f);
   p = fmaf(p, t, -3.827331461e-01f);
