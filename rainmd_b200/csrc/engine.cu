@@ -1082,6 +1082,7 @@ LaunchCtx Engine::ctx() const {
   c.sorted_type = sorted_type.p;
   c.rank = rank.p;
   c.lj = lj.p;
+  c.lj_entries = (int)lj.n;
   c.exc_start = exc_start.p;
   c.exc_partner = exc_partner.p;
   c.exc_param = exc_param.p;

@@ -100,6 +100,7 @@ struct LaunchCtx {
   float4 *wrap;
   // nonbonded
   const float2 *lj;
+  int lj_entries;  // float2 entries of `lj` (all systems' type tables)
   const int *exc_start, *exc_partner;
   const float4 *exc_param;
   unsigned long long *force;

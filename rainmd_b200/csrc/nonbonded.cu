@@ -45,7 +45,14 @@ __global__ void __launch_bounds__(128) k_nonbonded(
     const float2 *__restrict__ lj, const int *__restrict__ nbr, const int *__restrict__ nbr_count,
     const int *__restrict__ exc_start, const int *__restrict__ exc_partner,
     const float4 *__restrict__ exc_param, unsigned long long *__restrict__ force,
-    double *__restrict__ e_lj, double *__restrict__ e_coul, double *__restrict__ e_vir, int n_atoms) {
+    double *__restrict__ e_lj, double *__restrict__ e_coul, double *__restrict__ e_vir, int n_atoms,
+    int lj_entries) {
+  // the type tables in shared memory when they fit (the launch sizes the buffer), so the
+  // pair's LJ parameters are one shared-memory read after its partner's type
+  extern __shared__ float2 lj_shared[];
+  const bool lj_in_smem = lj_entries > 0;
+  for (int k = threadIdx.x; k < lj_entries; k += blockDim.x) lj_shared[k] = lj[k];
+  if (lj_in_smem) __syncthreads();
   const int gid = blockIdx.x * blockDim.x + threadIdx.x;
   // A warp may hold a group past the last atom (LANES < 32): it works on a clamped atom
   // with an empty row and stores nothing, so every lane reaches the shuffles.
@@ -58,7 +65,7 @@ __global__ void __launch_bounds__(128) k_nonbonded(
   const float4 pw = spos[si];
   const float qik = (float)ONE_4PI_EPS0 * pw.w;
   const int ti = sorted_type[si];
-  const float2 *ljrow = lj + s.lj_base + ti * s.type_count;
+  const float2 *ljrow = (lj_in_smem ? lj_shared : lj) + s.lj_base + ti * s.type_count;
   const float alpha = s.alpha;
   const float gauss_k = 2.0f * alpha * 0.5641895835477563f;  // 2a/sqrt(pi)
   const float cut2 = s.cutoff2;
@@ -71,6 +78,7 @@ __global__ void __launch_bounds__(128) k_nonbonded(
     const unsigned e = (unsigned)__ldg(row + k);
     const int g = (int)(e & NBR_SLOT_MASK);
     const float4 pj = __ldg(spos + g);
+    const int tj = __ldg(sorted_type + g);  // issued with the position, not after the cutoff test
     const float4 S = s.shift[e >> NBR_SLOT_BITS];  // the partner's image (code 0..26), fixed at the rebuild
     const float3 d = make_float3(pw.x - pj.x - S.x, pw.y - pj.y - S.y, pw.z - pj.z - S.z);
     const float r2 = fmaf(d.x, d.x, fmaf(d.y, d.y, d.z * d.z));
@@ -78,7 +86,7 @@ __global__ void __launch_bounds__(128) k_nonbonded(
       const float inv_r = rsqrt_refined(r2);
       const float inv_r2 = inv_r * inv_r;
       const float inv_r6 = inv_r2 * inv_r2 * inv_r2;
-      const float2 ab = __ldg(ljrow + __ldg(sorted_type + g));
+      const float2 ab = ljrow[tj];
       const float a12 = ab.x * inv_r6 * inv_r6, b6 = ab.y * inv_r6;
       float scalar = (12.0f * a12 - 6.0f * b6) * inv_r2;
       const float qq = qik * pj.w;
@@ -197,9 +205,11 @@ static void launch_nb(const LaunchCtx &c, cudaStream_t stream) {
   const int threads = 128;
   const long long total = (long long)c.n_atoms * LANES;
   const int blocks = (int)((total + threads - 1) / threads);
-  k_nonbonded<ENERGY, LANES, PAIR_FIXED><<<blocks, threads, 0, stream>>>(
+  constexpr int LJ_SMEM_MAX = 4096;  // float2 entries (32 KB)
+  const int lj_entries = c.lj_entries <= LJ_SMEM_MAX ? c.lj_entries : 0;
+  k_nonbonded<ENERGY, LANES, PAIR_FIXED><<<blocks, threads, sizeof(float2) * lj_entries, stream>>>(
       c.posq, c.spos, c.sorted_orig, c.sorted_type, c.sys_of_atom, c.sys, c.lj, c.nbr, c.nbr_count, c.exc_start,
-      c.exc_partner, c.exc_param, c.force, c.e_lj, c.e_coul, c.e_vir, c.n_atoms);
+      c.exc_partner, c.exc_param, c.force, c.e_lj, c.e_coul, c.e_vir, c.n_atoms, lj_entries);
 }
 
 template <bool PAIR_FIXED>
