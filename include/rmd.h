@@ -104,7 +104,7 @@ typedef struct {
                                    (order-independent, bitwise reproducible; default);
                                    1 = per-lane f32 partial sums, converted once per lane */
   /* kernel shapes; 0 = chosen by the engine's autotuner at initialise() */
-  int32_t neighbour_group_atoms; /* atoms per neighbour-search warp: 8, 16 or 32 */
+  int32_t neighbour_group_atoms; /* atoms per neighbour-search warp: 4, 8, 16 or 32 */
   int32_t nonbonded_lanes;       /* lanes per atom in the pair loop: 8, 16 or 32 */
   int32_t spread_atoms_per_block; /* atoms per PME charge-spreading block: 4, 8 or 16 */
   /* learned barostat (learned_barostat = 1) */
@@ -316,7 +316,7 @@ rmd_status rmd_surrogate_evaluate(const float *params, const float *inputs, cons
 /* Kernel launch shapes in use: shapes = {atoms per neighbour-search warp, lanes per atom in
  * the pair loop, atoms per PME spreading block}. When the options left a shape at 0,
  * initialise() chose it by timing every candidate (the engine's autotuner); tune_ms (may be
- * NULL) receives those times in ms per launch, in the order group 8/16/32, lanes 8/16/32,
+ * NULL) receives those times in ms per launch, in the order group 4/8/16, lanes 8/16/32,
  * spreading 4/8/16, with -1 for shapes that were not tuned. No reference counterpart: the
  * reference's WGSL kernels have fixed workgroup sizes. */
 rmd_status rmd_kernel_shapes(const rmd_sim *sim, int32_t shapes[3], double tune_ms[9]);

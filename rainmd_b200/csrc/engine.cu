@@ -441,7 +441,7 @@ void Engine::build(int count, const rmd_system *systems, const rmd_options *opti
   {
     const rmd_options &o = options[0];
     auto pick = [](int v, int a, int b, int c, int dflt) { return v == a || v == b || v == c ? v : dflt; };
-    group_atoms = pick(o.neighbour_group_atoms, 8, 16, 32, 8);
+    group_atoms = o.neighbour_group_atoms == 32 ? 32 : pick(o.neighbour_group_atoms, 4, 8, 16, 8);
     nb_lanes = pick(o.nonbonded_lanes, 8, 16, 32, 32);
     spread_atoms = pick(o.spread_atoms_per_block, 4, 8, 16, 8);
     tune_group = o.neighbour_group_atoms == 0;
@@ -804,7 +804,7 @@ void Engine::upload_all(const std::vector<const rmd_system *> &src) {
     for (int c = 0; c < cells; ++c) h_cell_sys.push_back(s);
     // search groups: at most ceil(n / 32) full ones plus one partial group per cell
     d.group_base = (int)h_group_sys.size();
-    const int groups = neighbour_group_slots(h.n, cells, 8);  // enough for every group size
+    const int groups = neighbour_group_slots(h.n, cells, 4);  // enough for every group size
     for (int q = 0; q < groups; ++q) h_group_sys.push_back(s);
     cell_base += cells;
     cell_start_base += cells + 1;
@@ -1351,7 +1351,7 @@ std::map<std::string, std::array<int, 3>> g_tuned;
 
 // The kernel-shape autotuner. Three launch shapes change speed but not results (neighbour
 // rows are the same for every group size; fixed-point pair forces and the fixed-point charge
-// grid are independent of summation order): atoms per neighbour-search warp (8, 16, 32),
+// grid are independent of summation order): atoms per neighbour-search warp (4, 8, 16),
 // lanes per atom in the pair loop (8, 16, 32) and atoms per spreading block (4, 8, 16).
 // Each candidate is timed with CUDA events on the engine's stream over a few launches on the
 // engine's own current state, the fastest is kept, and the choice is cached by workload
@@ -1386,7 +1386,7 @@ void Engine::autotune() {
     CUDA_OK(cudaEventElapsedTime(&ms, a, b));
     return (double)ms / reps;
   };
-  const int groups[3] = {8, 16, 32}, lanes[3] = {8, 16, 32}, spreads[3] = {4, 8, 16};
+  const int groups[3] = {4, 8, 16}, lanes[3] = {8, 16, 32}, spreads[3] = {4, 8, 16};
   if (tune_group) {
     double best = 1e30;
     int pick = group_atoms;
@@ -2429,7 +2429,8 @@ rmd_status rmd_set_kernel_shapes(rmd_sim *sim, int32_t group_atoms, int32_t nonb
                                  int32_t spread_atoms) {
   if (!sim) return RMD_ERR_INVALID;
   auto ok = [](int v, int a, int b, int c) { return v == 0 || v == a || v == b || v == c; };
-  if (!ok(group_atoms, 8, 16, 32) || !ok(nonbonded_lanes, 8, 16, 32) || !ok(spread_atoms, 4, 8, 16))
+  if (!(ok(group_atoms, 4, 8, 16) || group_atoms == 32) || !ok(nonbonded_lanes, 8, 16, 32) ||
+      !ok(spread_atoms, 4, 8, 16))
     return RMD_ERR_INVALID;
   auto &e = sim->engine;
   if (group_atoms) e.group_atoms = group_atoms;

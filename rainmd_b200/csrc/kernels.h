@@ -88,7 +88,7 @@ struct LaunchCtx {
   int *cell_gstart, *group_order;
   const int *group_sys;
   int n_groups_total;
-  int group_atoms;  // atoms per neighbour-search group: 8, 16 or 32
+  int group_atoms;  // atoms per neighbour-search group: 4, 8, 16 or 32
   const int *excl_start, *excl_partners;
   int *nbr, *nbr_count, *required;
   float4 *origin;

@@ -8,7 +8,7 @@
 //   - the histogram and the scatter use integer atomics, and a per-cell block rank-sort
 //     (shared memory) restores the deterministic index order;
 //   - the scan is one block per system;
-//   - the neighbour search is one WARP per group of 8, 16 or 32 spatially close atoms of a
+//   - the neighbour search is one WARP per group of 4, 8, 16 or 32 spatially close atoms of a
 //     cell: the group's bounding box culls stencil cells and candidates once for all its
 //     atoms, the survivors are staged in shared memory, and each atom's lanes append its
 //     hits in candidate order, so every row's order equals the sequential one.
@@ -438,7 +438,9 @@ void launch_rebuild(const LaunchCtx &ctx, cudaStream_t stream) {
   ctx.posq, ctx.group_sys, ctx.sys, ctx.cell_start, ctx.cell_gstart, ctx.group_order, ctx.excl_start,  \
       ctx.excl_partners, ctx.spos, ctx.sorted_orig, ctx.nbr, ctx.nbr_count, ctx.required, ctx.origin, \
       ctx.n_groups_total
-  if (G == 8)
+  if (G == 4)
+    k_neighbours<4><<<blocks, 32 * NBR_WARPS, 0, stream>>>(RMD_NBR_ARGS);
+  else if (G == 8)
     k_neighbours<8><<<blocks, 32 * NBR_WARPS, 0, stream>>>(RMD_NBR_ARGS);
   else if (G == 16)
     k_neighbours<16><<<blocks, 32 * NBR_WARPS, 0, stream>>>(RMD_NBR_ARGS);

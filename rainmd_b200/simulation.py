@@ -366,7 +366,7 @@ class BatchSimulation:
 
         return {"neighbourGroupAtoms": int(shapes[0]), "nonbondedLanes": int(shapes[1]),
                 "spreadAtomsPerBlock": int(shapes[2]),
-                "tuned": {"neighbourGroupAtoms": table(ms[0:3], (8, 16, 32)),
+                "tuned": {"neighbourGroupAtoms": table(ms[0:3], (4, 8, 16)),
                           "nonbondedLanes": table(ms[3:6], (8, 16, 32)),
                           "spreadAtomsPerBlock": table(ms[6:9], (4, 8, 16))}}
 

@@ -57,7 +57,7 @@ def symmetric_exclusions(system):
     return np.cumsum(start).astype(np.int32), b[order].astype(np.int32)
 
 
-@pytest.mark.parametrize("group", [8, 16, 32])
+@pytest.mark.parametrize("group", [4, 8, 16, 32])
 @pytest.mark.parametrize("cutoff", [1.0, 0.7, 0.5])
 def test_cell_and_neighbour_lists_bit_exact(cutoff, group):
     """check-nonbonded.mjs:12-19, 240-262 at three cell geometries and every search-group
