@@ -1230,20 +1230,21 @@ BaroArgs Engine::bargs() const {
 // ------------------------------------------------------------------------ operations
 void Engine::record_forces(bool rebuild, bool energy) {
   const LaunchCtx c = ctx();
-  if (rebuild) {
-    CUDA_OK(cudaMemsetAsync(required.p, 0, sizeof(int) * S, stream));
-    CUDA_OK(cudaMemsetAsync(disp.p, 0, sizeof(unsigned) * S, stream));  // slot 0: since rebuild
-    launch_rebuild(c, stream);
-    recorded += 5;
-  }
   // The reciprocal-space chain up to the convolved grid only reads positions, so it runs
-  // concurrently with the pair and bonded kernels; the gather, which adds into the force
-  // array the pair kernel stores, waits for both branches.
+  // concurrently with the list rebuild and the pair and bonded kernels; the gather, which
+  // adds into the force array the pair kernel stores (and reads the cell order the rebuild
+  // writes), waits for both branches.
   if (pme_on) {
     CUDA_OK(cudaEventRecord(ev_fork, stream));
     CUDA_OK(cudaStreamWaitEvent(side, ev_fork, 0));
     launch_pme_grid(c, energy, side);
     CUDA_OK(cudaEventRecord(ev_join, side));
+  }
+  if (rebuild) {
+    CUDA_OK(cudaMemsetAsync(required.p, 0, sizeof(int) * S, stream));
+    CUDA_OK(cudaMemsetAsync(disp.p, 0, sizeof(unsigned) * S, stream));  // slot 0: since rebuild
+    launch_rebuild(c, stream);
+    recorded += 5;
   }
   launch_nonbonded(c, energy, nb_lanes, stream);
   launch_bonded(c, energy, stream);
