@@ -301,6 +301,57 @@ class Oracle:
                                            float(tolerance), int(max_iterations), None)
         return pos, it
 
+    # -- steepest descent (webgpu/simulation.js:880-979, integrate.js:589-688) --
+    def minimise(self, positions, max_iterations=200, force_tolerance=500.0, max_step=0.002,
+                 max_displacement=0.05, constraint_tolerance=1e-7, **potential_args):
+        """The reference's line search in FP64: at the accepted structure, stop when the
+        largest per-atom force is within tolerance; otherwise try up to 14 steps that move the
+        largest force `max_step` nm (every displacement capped at `max_displacement`),
+        projected onto the constraints against the pre-move structure. A lower potential is
+        accepted and grows the step by 1.3; a rejection halves it, and 14 rejections or a step
+        below 1e-9 stall the search. As on the device, a rejected trial leaves the accepted
+        structure AND its forces in place."""
+        pos = np.asarray(positions, dtype=np.float64).reshape(-1, 3).copy()
+
+        def evaluate(p):
+            e, f = self.potential(p.reshape(-1), **potential_args)
+            return e["total"], f.reshape(-1, 3)
+
+        potential, forces = evaluate(pos)
+        iterations = rejected = 0
+        stalled = False
+        for iteration in range(max_iterations):
+            iterations = iteration + 1
+            worst = float(np.max(np.linalg.norm(forces, axis=1)))
+            if worst <= force_tolerance:
+                break
+            accepted = False
+            for _ in range(14):
+                d = forces * (max_step / max(worst, 1e-6))
+                norm = np.linalg.norm(d, axis=1)
+                over = norm > max_displacement
+                d[over] *= (max_displacement / norm[over])[:, None]
+                trial, _ = self.constrain_positions((pos + d).reshape(-1), pos.reshape(-1),
+                                                    constraint_tolerance)
+                trial = trial.reshape(-1, 3)
+                e, f = evaluate(trial)
+                if e < potential:
+                    potential, pos, forces = e, trial, f
+                    max_step *= 1.3
+                    accepted = True
+                    break
+                rejected += 1
+                max_step *= 0.5
+                if max_step < 1e-9:
+                    break
+            if not accepted:
+                stalled = True
+                break
+        worst = float(np.max(np.linalg.norm(forces, axis=1)))
+        return {"positions": pos.reshape(-1), "iterations": iterations, "rejected": rejected,
+                "stalled": stalled, "converged": worst <= force_tolerance, "potential": potential,
+                "max_force": worst, "max_step": max_step}
+
 
 def erfc(x: float) -> float:
     return lib().orc_erfc(float(x))

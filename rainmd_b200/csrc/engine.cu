@@ -1740,8 +1740,11 @@ std::vector<float> Engine::max_forces() {
   return out;
 }
 
-// minimise (simulation.js:880-979): steepest descent with a backtracking line search, one
-// host decision per trial. Every system of a batch keeps its own step and acceptance.
+// minimise (simulation.js:880-979): steepest descent with a backtracking line search. Every
+// system of a batch keeps its own step and acceptance, and every decision is taken on the
+// device (minimise.cu): one trial is one captured graph, launched in batches of 16 with the
+// states read back between batches. A trial whose neighbour list overflowed is undone on the
+// device; the host grows the list, re-captures and the trial runs again.
 // Departure: the positions AND forces of the last accepted structure are restored after a
 // rejected trial, so the next trial moves along the accepted gradient.
 void Engine::minimise(int max_iterations, double force_tolerance, double max_step, double cap,
@@ -1759,81 +1762,85 @@ void Engine::minimise(int max_iterations, double force_tolerance, double max_ste
     for (int s = 0; s < S; ++s) p[s] = e[(size_t)s * N_ENERGY + E_POTENTIAL];
     return p;
   };
-  std::vector<double> potential = potentials(), step(S, max_step);
-  std::vector<char> done(S, 0), stalled(S, 0);
-  std::vector<int> iterations(S, 0), rejected(S, 0);
-  DevArray<float> scale;
-  scale.alloc(S);
-  const size_t fbytes = sizeof(unsigned long long) * 3 * (size_t)N;
-  for (int it = 0; it < max_iterations; ++it) {
-    std::vector<float> worst = max_forces();
-    bool any = false;
-    for (int s = 0; s < S; ++s) {
-      if (done[s]) continue;
-      iterations[s] = it + 1;
-      if (worst[s] <= force_tolerance) done[s] = 1;
-      else any = true;
-    }
-    if (!any) break;
-    CUDA_OK(cudaMemcpyAsync(saved_posq.p, posq.p, sizeof(float4) * N, cudaMemcpyDeviceToDevice, stream));
-    CUDA_OK(cudaMemcpyAsync(saved_force.p, force.p, fbytes, cudaMemcpyDeviceToDevice, stream));
-    std::vector<char> accepted(S, 0), active(S, 0);
-    for (int s = 0; s < S; ++s) active[s] = !done[s];
-    for (int attempt = 0; attempt < 14; ++attempt) {
-      std::vector<float> sc(S, 0.f);
-      bool pending = false;
-      for (int s = 0; s < S; ++s)
-        if (active[s] && !accepted[s]) {
-          sc[s] = (float)(step[s] / std::max((double)worst[s], 1e-6));
-          pending = true;
-        }
-      if (!pending) break;
-      CUDA_OK(cudaMemcpyAsync(scale.p, sc.data(), sizeof(float) * S, cudaMemcpyHostToDevice, stream));
-      launch_displace(posq.p, force.p, sys_of_atom.p, N, scale.p, (float)cap, stream);
-      launch_integrate(iargs(0), INT_CONSTRAIN, stream);
-      std::vector<double> trial = potentials();
-      bool restore = false;
-      for (int s = 0; s < S; ++s) {
-        if (!active[s] || accepted[s]) continue;
-        if (trial[s] < potential[s]) {
-          potential[s] = trial[s];
-          step[s] *= 1.3;
-          accepted[s] = 1;
-        } else {
-          rejected[s]++;
-          step[s] *= 0.5;
-          restore = true;
-          if (step[s] < 1e-9) active[s] = 0;
-        }
-      }
-      if (restore) {
-        // put back every not-yet-accepted system (accepted ones keep their new state)
-        std::vector<float4> cur(N), old(N);
-        std::vector<unsigned long long> fc(3 * (size_t)N), fo(3 * (size_t)N);
-        CUDA_OK(cudaMemcpy(cur.data(), posq.p, sizeof(float4) * N, cudaMemcpyDeviceToHost));
-        CUDA_OK(cudaMemcpy(old.data(), saved_posq.p, sizeof(float4) * N, cudaMemcpyDeviceToHost));
-        CUDA_OK(cudaMemcpy(fc.data(), force.p, fbytes, cudaMemcpyDeviceToHost));
-        CUDA_OK(cudaMemcpy(fo.data(), saved_force.p, fbytes, cudaMemcpyDeviceToHost));
-        for (int s = 0; s < S; ++s) {
-          if (accepted[s]) continue;
-          for (int i = hs[s].atom_start; i < hs[s].atom_start + hs[s].n; ++i) {
-            cur[i] = old[i];
-            for (int c = 0; c < 3; ++c) fc[(size_t)c * N + i] = fo[(size_t)c * N + i];
-          }
-        }
-        CUDA_OK(cudaMemcpy(posq.p, cur.data(), sizeof(float4) * N, cudaMemcpyHostToDevice));
-        CUDA_OK(cudaMemcpy(force.p, fc.data(), fbytes, cudaMemcpyHostToDevice));
-      }
-    }
-    for (int s = 0; s < S; ++s)
-      if (!done[s] && !accepted[s]) {
-        stalled[s] = 1;
-        done[s] = 1;
-      }
+  const std::vector<double> start = potentials();
+  std::vector<MinState> state(S);
+  for (int s = 0; s < S; ++s) {
+    state[s] = MinState{};
+    state[s].potential = start[s];
+    state[s].step = max_step;
   }
+  DevArray<MinState> dstate;
+  DevArray<float> scale;
+  DevArray<unsigned> worst_bits;
+  dstate.alloc(S);
+  scale.alloc(S);
+  worst_bits.alloc(S);
+  CUDA_OK(cudaMemcpy(dstate.p, state.data(), sizeof(MinState) * S, cudaMemcpyHostToDevice));
+  cudaGraphExec_t trial = nullptr;
+  long long trial_kernels = 0;
+  auto capture = [&]() {
+    cudaGraph_t graph;
+    const long long before = recorded;
+    CUDA_OK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+    CUDA_OK(cudaMemsetAsync(worst_bits.p, 0, sizeof(unsigned) * S, stream));
+    launch_max_force(force.p, sys_of_atom.p, N, worst_bits.p, stream);
+    launch_min_begin(dstate.p, worst_bits.p, scale.p, S, max_iterations, (float)force_tolerance, stream);
+    launch_min_save(dstate.p, posq.p, force.p, saved_posq.p, saved_force.p, sys_of_atom.p, N, stream);
+    launch_displace(posq.p, force.p, sys_of_atom.p, N, scale.p, (float)cap, stream);
+    launch_integrate(iargs(0), INT_CONSTRAIN, stream);
+    record_forces(true, true);
+    launch_min_decide(dstate.p, energies.p, required.p, sys.p, S, stream);
+    launch_min_restore(dstate.p, posq.p, force.p, saved_posq.p, saved_force.p, sys_of_atom.p, N, stream);
+    recorded += 7;
+    CUDA_OK(cudaStreamEndCapture(stream, &graph));
+    trial_kernels = recorded - before;
+    CUDA_OK(cudaGraphInstantiate(&trial, graph, 0));
+    CUDA_OK(cudaGraphDestroy(graph));
+  };
+  capture();
+  // every iteration takes at most 14 trials and one more that finds it converged; each
+  // neighbour-list growth repeats one trial
+  const long long limit = (long long)(max_iterations + 1) * (MIN_ATTEMPTS + 1) + 64;
+  long long trials = 0;
+  while (trials < limit) {
+    const int batch = (int)std::min<long long>(16, limit - trials);
+    for (int k = 0; k < batch; ++k) CUDA_OK(cudaGraphLaunch(trial, stream));
+    trials += batch;
+    kernel_launches += trial_kernels * batch;
+    CUDA_OK(cudaMemcpyAsync(state.data(), dstate.p, sizeof(MinState) * S, cudaMemcpyDeviceToHost, stream));
+    sync();
+    bool all_done = true, grow = false;
+    for (int s = 0; s < S; ++s) {
+      if (!state[s].done) all_done = false;
+      if (state[s].overflow) {
+        HostSystem &h = hs[s];
+        h.worst_required = std::max(h.worst_required, state[s].need);
+        if (state[s].need > h.capacity) {  // grownPlan (cells.js:282-288)
+          h.capacity = (std::max(h.capacity + 32, (int)std::ceil(state[s].need * 1.25)) + 3) & ~3;
+          h.neighbour_growths++;
+        }
+        state[s].overflow = 0;
+        state[s].need = 0;
+        grow = true;
+      }
+    }
+    if (grow) {
+      // the pointers recorded in the trial graph change with the list's storage
+      CUDA_OK(cudaGraphExecDestroy(trial));
+      trial = nullptr;
+      allocate_neighbours();
+      CUDA_OK(cudaMemcpy(dstate.p, state.data(), sizeof(MinState) * S, cudaMemcpyHostToDevice));
+      capture();
+      continue;
+    }
+    if (all_done) break;
+  }
+  if (trial) CUDA_OK(cudaGraphExecDestroy(trial));
+  dstate.release();
+  worst_bits.release();
   scale.release();
   // forces at the final structure, and velocities zeroed (simulation.js:971-973)
-  potential = potentials();
+  const std::vector<double> potential = potentials();
   std::vector<float> worst = max_forces();
   std::vector<float4> v(N);
   CUDA_OK(cudaMemcpy(v.data(), vel.p, sizeof(float4) * N, cudaMemcpyDeviceToHost));
@@ -1842,13 +1849,13 @@ void Engine::minimise(int max_iterations, double force_tolerance, double max_ste
   launch_integrate(iargs(0), INT_CLOSE_KINETIC, stream);
   sync();
   if (out) {
-    out->iterations = iterations[0];
-    out->rejected = rejected[0];
-    out->stalled = stalled[0];
+    out->iterations = state[0].iterations;
+    out->rejected = state[0].rejected;
+    out->stalled = state[0].stalled;
     out->converged = worst[0] <= force_tolerance;
     out->potential = potential[0];
     out->max_force = worst[0];
-    out->max_step = step[0];
+    out->max_step = state[0].step;
   }
 }
 

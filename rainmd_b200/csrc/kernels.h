@@ -243,4 +243,31 @@ void launch_max_force(const unsigned long long *force, const int *sys_of_atom, i
 void launch_displace(float4 *posq, const unsigned long long *force, const int *sys_of_atom, int n_atoms,
                      const float *scale, float max_disp, cudaStream_t stream);
 
+// Line-search state of one system, owned by the device while the minimiser runs: every
+// accept/reject decision is taken by min_decide, so a trial needs no host round trip.
+struct MinState {
+  double potential;  // energy of the accepted structure
+  double step;       // line-search step (nm^2 mol/kJ scale of the largest force)
+  float worst;       // largest force of the accepted structure (kJ/mol/nm)
+  int iterations, rejected, attempt;
+  int open;       // an iteration is under way (its start structure is in saved_posq/saved_force)
+  int done, stalled;
+  int trial;      // this trial displaced the system
+  int save;       // this trial opened an iteration: copy the structure aside first
+  int reject_now; // this trial was rejected: put the accepted structure back
+  int overflow;   // a trial's neighbour list overflowed; paused until the host grows the list
+  int need;       // largest neighbour requirement seen in an overflowing trial
+};
+constexpr int MIN_ATTEMPTS = 14;  // trials per iteration (simulation.js:880-979)
+
+void launch_min_begin(MinState *st, const unsigned *worst_bits, float *scale, int n_systems, int max_iterations,
+                      float force_tolerance, cudaStream_t stream);
+void launch_min_save(const MinState *st, const float4 *posq, const unsigned long long *force, float4 *saved_posq,
+                     unsigned long long *saved_force, const int *sys_of_atom, int n_atoms, cudaStream_t stream);
+void launch_min_decide(MinState *st, const double *energies, const int *required, const DevSys *sys,
+                       int n_systems, cudaStream_t stream);
+void launch_min_restore(const MinState *st, float4 *posq, unsigned long long *force, const float4 *saved_posq,
+                        const unsigned long long *saved_force, const int *sys_of_atom, int n_atoms,
+                        cudaStream_t stream);
+
 }  // namespace rmd

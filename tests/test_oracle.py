@@ -182,6 +182,37 @@ def test_shake_restores_lengths():
     assert np.max(np.abs(lengths - c["distance"]) / c["distance"]) < 1e-7
 
 
+def test_line_search_descends_and_keeps_constraints():
+    """The FP64 line search (simulation.js:880-979) lowers the potential at every accepted
+    step, keeps the constraints, and reports the potential of the structure it returns."""
+    s, pos, _ = system_for("ala-wat")
+    o = oracle.Oracle(s)
+    args = dict(method="PME", alpha=2.6282608939112584, grid=[24, 24, 24], order=5)
+    start = o.potential(pos, **args)[0]["total"]
+    seen = []
+    evaluate = o.potential
+
+    def record(p, **k):
+        e, f = evaluate(p, **k)
+        seen.append(e["total"])
+        return e, f
+
+    o.potential = record
+    r = o.minimise(pos, max_iterations=12, **args)
+    assert r["iterations"] == 12 and r["rejected"] >= 1 and not r["stalled"]
+    accepted = [seen[0]]
+    for e in seen[1:]:
+        if e < accepted[-1]:
+            accepted.append(e)
+    assert len(accepted) == 1 + 12  # the start and one accepted trial per iteration
+    assert r["potential"] == accepted[-1] < start
+    c = s["constraints"]
+    p = r["positions"].reshape(-1, 3)
+    lengths = np.linalg.norm(p[c["atomA"]] - p[c["atomB"]], axis=1)
+    assert np.max(np.abs(lengths - c["distance"]) / c["distance"]) < 1e-6
+    assert r["potential"] == pytest.approx(evaluate(r["positions"], **args)[0]["total"], rel=1e-12)
+
+
 def test_force_gradients_central_difference():
     # tools/check-force-gradients.mjs: bar 1e-5 of rms, on bonded and nonbonded terms
     s, pos, _ = system_for("ala-wat")
