@@ -491,6 +491,7 @@ def main():
         torch.cuda.synchronize()
 
     launches0 = sim.kernelLaunches()
+    builds0 = sim.diagnostics()["list_builds"]
     barrier()
     with ClockSampler(local if world == 1 else 0) as clocks:
         device_ms = sim.benchRun(args.steps, block, flushL2=True)
@@ -505,8 +506,9 @@ def main():
     value, seconds_per_step = aggregate(device_ms, args.steps, world, reduce_max)
 
     # energies stay finite and the run was physical
-    e = sim.energy()
     diag = sim.diagnostics()
+    builds = diag["list_builds"] - builds0
+    e = sim.energy()
 
     # end to end through the public API: host arrays in, run, host arrays out
     state = sim.readState()
@@ -572,6 +574,8 @@ def main():
         "batched": batched,
         "clocks": clocks.summary(),
         "physics": {"temperature": e["temperature"], "potential": e["potential"],
+                    "list_builds_timed": builds, "steps_per_list_build": args.steps / max(builds, 1),
+                    "rebuild_on_demand": diag["rebuild_on_demand"],
                     "rebuild_interval": diag["rebuild_interval"], "skin_violations": diag["skin_violations"],
                     "neighbour_capacity": diag["neighbour_capacity"]},
         "cpu_baseline": base,

@@ -111,6 +111,13 @@ typedef struct {
   int32_t learned_warmup_moves;  /* exact moves that train the surrogate before it screens; <= 0: 2000 */
   int32_t learned_steps_per_move; /* Adam steps after each exact move; <= 0: 4 */
   double learned_rate;           /* Adam learning rate; <= 0: 1e-3 */
+  /* 1 (default): the device checks every step whether some atom has moved more than half the
+   * skin since the last build and rebuilds the lists exactly then (an IF node of the step
+   * graph), so no step uses a stale list and no rebuild is early; rebuild_interval and
+   * adaptive_rebuild are then unused. 0: the reference's host-side schedule (a rebuild every
+   * rebuild_interval steps, adapted between blocks when adaptive_rebuild is set,
+   * simulation.js:544-623). No reference counterpart. */
+  int32_t rebuild_on_demand;
 } rmd_options;
 
 #define RMD_NO_PRESSURE (-1.0e300)
@@ -174,6 +181,8 @@ typedef struct {
   int32_t pme_order;
   int32_t cluster_count, settle_count;
   int64_t device_bytes;
+  int64_t list_builds;       /* neighbour-list builds so far (every system of a handle builds together) */
+  int32_t rebuild_on_demand; /* the option in effect */
 } rmd_diagnostics_report;
 
 /* Fills `options` with the reference's defaults. */

@@ -54,7 +54,7 @@ class RmdOptions(C.Structure):
         ("force_accumulation", C.c_int32), ("neighbour_group_atoms", C.c_int32),
         ("nonbonded_lanes", C.c_int32), ("spread_atoms_per_block", C.c_int32),
         ("learned_warmup_moves", C.c_int32), ("learned_steps_per_move", C.c_int32),
-        ("learned_rate", C.c_double),
+        ("learned_rate", C.c_double), ("rebuild_on_demand", C.c_int32),
     ]
 
 
@@ -116,6 +116,7 @@ class RmdDiagnostics(C.Structure):
         ("tolerance_floor", C.c_double), ("cell_counts", C.c_int32 * 3),
         ("pme_grid", C.c_int32 * 3), ("pme_alpha", C.c_double), ("pme_order", C.c_int32),
         ("cluster_count", C.c_int32), ("settle_count", C.c_int32), ("device_bytes", C.c_int64),
+        ("list_builds", C.c_int64), ("rebuild_on_demand", C.c_int32),
     ]
 
 

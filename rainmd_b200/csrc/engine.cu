@@ -146,6 +146,7 @@ struct HostSystem {
   // adaptive rebuild (simulation.js:105-118, 544-623)
   int rebuild_interval = 20, requested_rebuild = 20;
   bool adaptive = true;
+  bool on_demand = true;  // the device decides each step (rmd_options.rebuild_on_demand)
   int calm_blocks = 0, rebuild_growths = 0, rebuild_shrinks = 0, skin_violations = 0;
   int64_t steps_with_stale = 0;
   int64_t steps_since_rebuild = 1LL << 40;
@@ -162,6 +163,9 @@ struct HostSystem {
 
 static const double LIGHT_ANCHOR_SKIN = 0.40;  // cells.js:67-91
 
+// How a force evaluation treats the neighbour lists.
+enum RebuildMode { REBUILD_NONE = 0, REBUILD_FORCED = 1, REBUILD_IF_STALE = 2 };
+
 struct Engine {
   std::vector<HostSystem> hs;
   int S = 0, N = 0;
@@ -170,6 +174,9 @@ struct Engine {
   // back to `stream` with events (inside a captured graph these become parallel branches)
   cudaStream_t side = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  // the stream a conditional rebuild body is captured on (record_forces)
+  cudaStream_t cond = nullptr;
+  bool on_demand = true;  // lists rebuilt when the device finds them stale (all systems agree)
   std::string last_error;
   int nb_lanes = 32;
   int group_atoms = 8;   // atoms per neighbour-search warp
@@ -191,7 +198,10 @@ struct Engine {
   int n_cells_total = 0;
   DevArray<int> cell_gstart, group_order, group_sys;
   int n_groups_total = 0;
-  DevArray<int> nbr, nbr_count, required;
+  DevArray<int> nbr, nbr_count, required, required_max, stale;
+  // list builds counted on the device: [0] those an IF node took, [1] all of them
+  DevArray<unsigned long long> list_builds;
+  unsigned long long conditional_builds_seen = 0;
   DevArray<float4> spos, wrap;
   DevArray<int> sorted_orig, sorted_type, rank;
   DevArray<int2> bond_atoms;
@@ -241,6 +251,7 @@ struct Engine {
     if (ev_fork) cudaEventDestroy(ev_fork);
     if (ev_join) cudaEventDestroy(ev_join);
     if (side) cudaStreamDestroy(side);
+    if (cond) cudaStreamDestroy(cond);
     if (stream) cudaStreamDestroy(stream);
   }
 
@@ -264,7 +275,9 @@ struct Engine {
   void surrogate_train();
 
   // ---------------------------------------------------------------- operations
-  void record_forces(bool rebuild, bool energy);
+  // rebuild: REBUILD_NONE, REBUILD_FORCED, or REBUILD_IF_STALE (captured graphs only)
+  void record_forces(int rebuild, bool energy);
+  void record_conditional_rebuild(const LaunchCtx &c);
   void record_barostat();
   void evaluate(bool rebuild, bool energy);
   void set_state(int s, const double *pos, const double *vel, int64_t step, int supplied);
@@ -395,6 +408,7 @@ void Engine::plan_system(HostSystem &h, const rmd_system &s) {
   }
   h.requested_rebuild = o.rebuild_interval > 0 ? o.rebuild_interval : 20;
   h.adaptive = o.adaptive_rebuild != 0;
+  h.on_demand = o.rebuild_on_demand != 0;
   h.rebuild_interval = h.adaptive ? std::min(h.requested_rebuild, 4) : h.requested_rebuild;
   h.has_pressure = o.pressure > -1e299;
   h.barostat_interval = o.barostat_interval > 0 ? o.barostat_interval : 25;
@@ -461,6 +475,9 @@ void Engine::build(int count, const rmd_system *systems, const rmd_options *opti
   int lowest = 0, highest = 0;
   CUDA_OK(cudaDeviceGetStreamPriorityRange(&lowest, &highest));
   CUDA_OK(cudaStreamCreateWithPriority(&side, cudaStreamDefault, highest));
+  CUDA_OK(cudaStreamCreateWithFlags(&cond, cudaStreamNonBlocking));
+  on_demand = true;
+  for (auto &h : hs) on_demand = on_demand && h.on_demand;
   CUDA_OK(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
   CUDA_OK(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
   upload_all(src);
@@ -845,6 +862,12 @@ void Engine::upload_all(const std::vector<const rmd_system *> &src) {
   rank.zero();
   required.alloc(S);
   required.zero();
+  required_max.alloc(S);
+  required_max.zero();
+  stale.alloc(S);
+  stale.zero();
+  list_builds.alloc(2);
+  list_builds.zero();
 
   // ---- PME grids, moduli, twiddles, FFT plans and task tables
   {
@@ -1228,7 +1251,7 @@ BaroArgs Engine::bargs() const {
 }
 
 // ------------------------------------------------------------------------ operations
-void Engine::record_forces(bool rebuild, bool energy) {
+void Engine::record_forces(int rebuild, bool energy) {
   const LaunchCtx c = ctx();
   // The reciprocal-space chain up to the convolved grid only reads positions, so it runs
   // concurrently with the list rebuild and the pair and bonded kernels; the gather, which
@@ -1240,11 +1263,12 @@ void Engine::record_forces(bool rebuild, bool energy) {
     launch_pme_grid(c, energy, side);
     CUDA_OK(cudaEventRecord(ev_join, side));
   }
-  if (rebuild) {
-    CUDA_OK(cudaMemsetAsync(required.p, 0, sizeof(int) * S, stream));
-    CUDA_OK(cudaMemsetAsync(disp.p, 0, sizeof(unsigned) * S, stream));  // slot 0: since rebuild
+  if (rebuild == REBUILD_FORCED) {
+    launch_rebuild_reset(required.p, required_max.p, disp.p, S, list_builds.p + 1, nullptr, stream);  // disp slot 0: since rebuild
     launch_rebuild(c, stream);
-    recorded += 5;
+    recorded += 6;
+  } else if (rebuild == REBUILD_IF_STALE) {
+    record_conditional_rebuild(c);
   }
   launch_nonbonded(c, energy, nb_lanes, stream);
   launch_bonded(c, energy, stream);
@@ -1258,6 +1282,41 @@ void Engine::record_forces(bool rebuild, bool energy) {
     launch_energy_reduce(segments.p, n_segments, seg_out.p, energies.p, sysd.p, S, stream);
     recorded += 3;
   }
+}
+
+// The rebuild as the body of an IF node of the graph being captured on `stream`: a one-block
+// kernel sets the condition from the displacement the integrator just reduced, and the body
+// (reset + cell and neighbour kernels) is captured into the node's child graph on `cond`.
+// The body's six kernels are counted when they run (list_builds), not here.
+void Engine::record_conditional_rebuild(const LaunchCtx &c) {
+  cudaStreamCaptureStatus status;
+  cudaGraph_t graph;
+  const cudaGraphNode_t *deps = nullptr;
+  size_t ndeps = 0;
+  CUDA_OK(cudaStreamGetCaptureInfo(stream, &status, nullptr, &graph, &deps, &ndeps));
+  if (status != cudaStreamCaptureStatusActive)
+    throw Error(RMD_ERR_CUDA, "a conditional rebuild can only be recorded into a captured graph");
+  cudaGraphConditionalHandle handle;
+  CUDA_OK(cudaGraphConditionalHandleCreate(&handle, graph, 0, 0));
+  launch_rebuild_decide(handle, disp.p, sys.p, S, stale.p, list_builds.p, stream);
+  recorded += 1;
+  CUDA_OK(cudaStreamGetCaptureInfo(stream, &status, nullptr, &graph, &deps, &ndeps));
+  cudaGraphNodeParams params = {};
+  params.type = cudaGraphNodeTypeConditional;
+  params.conditional.handle = handle;
+  params.conditional.type = cudaGraphCondTypeIf;
+  params.conditional.size = 1;
+  cudaGraphNode_t node;
+  CUDA_OK(cudaGraphAddNode(&node, graph, deps, ndeps, &params));
+  CUDA_OK(cudaStreamUpdateCaptureDependencies(stream, &node, 1, cudaStreamSetCaptureDependencies));
+  cudaGraph_t body = params.conditional.phGraph_out[0];
+  CUDA_OK(cudaStreamBeginCaptureToGraph(cond, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+  LaunchCtx only = c;  // the systems of the batch that have gone stale
+  only.rebuild_only = stale.p;
+  launch_rebuild_reset(required.p, required_max.p, disp.p, S, list_builds.p + 1, stale.p, cond);
+  launch_rebuild(only, cond);
+  cudaGraph_t captured;
+  CUDA_OK(cudaStreamEndCapture(cond, &captured));
 }
 
 void Engine::evaluate(bool rebuild, bool energy) {
@@ -1306,16 +1365,20 @@ void Engine::set_state(int s, const double *pos, const double *vel_in, int64_t s
 }
 
 int Engine::check_capacity() {
-  std::vector<int> req(S);
+  // the last build's requirement, and the largest of the builds before it since the last check
+  std::vector<int> req(S), earlier(S);
   CUDA_OK(cudaMemcpy(req.data(), required.p, sizeof(int) * S, cudaMemcpyDeviceToHost));
+  CUDA_OK(cudaMemcpy(earlier.data(), required_max.p, sizeof(int) * S, cudaMemcpyDeviceToHost));
+  CUDA_OK(cudaMemset(required_max.p, 0, sizeof(int) * S));
   bool grow = false;
   int worst = 0;
   for (int s = 0; s < S; ++s) {
+    const int most = std::max(req[s], earlier[s]);
     hs[s].last_required = req[s];
-    hs[s].worst_required = std::max(hs[s].worst_required, req[s]);
-    worst = std::max(worst, req[s]);
-    if (req[s] > hs[s].capacity) {  // grownPlan (cells.js:282-288)
-      hs[s].capacity = (std::max(hs[s].capacity + 32, (int)std::ceil(req[s] * 1.25)) + 3) & ~3;
+    hs[s].worst_required = std::max(hs[s].worst_required, most);
+    worst = std::max(worst, most);
+    if (most > hs[s].capacity) {  // grownPlan (cells.js:282-288)
+      hs[s].capacity = (std::max(hs[s].capacity + 32, (int)std::ceil(most * 1.25)) + 3) & ~3;
       hs[s].neighbour_growths++;
       grow = true;
     }
@@ -1324,6 +1387,7 @@ int Engine::check_capacity() {
     allocate_neighbours();
     evaluate(true, false);
     sync();
+    CUDA_OK(cudaMemset(required_max.p, 0, sizeof(int) * S));
     CUDA_OK(cudaMemcpy(req.data(), required.p, sizeof(int) * S, cudaMemcpyDeviceToHost));
     for (int s = 0; s < S; ++s) {
       if (req[s] > hs[s].capacity)
@@ -1460,14 +1524,22 @@ void Engine::run_block(int n, bool barostat, bool energy_last) {
   }
   if (barostat) since = 1LL << 40;
   std::string key = "n" + std::to_string(n) + (barostat ? "B" : "") + (energy_last ? "E" : "") + ":";
-  std::vector<char> rebuild(n, 0);
-  for (int k = 0; k < n; ++k) {
-    if (since >= interval) {
-      rebuild[k] = 1;
-      since = 0;
+  std::vector<char> rebuild(n, REBUILD_NONE);
+  if (on_demand) {
+    // a list from before a box change, a new state or a capacity change is not measured by
+    // the displacement check: build it; every other step asks the device
+    for (int k = 0; k < n; ++k) rebuild[k] = REBUILD_IF_STALE;
+    if (since >= (1LL << 39)) rebuild[0] = REBUILD_FORCED;
+    key += rebuild[0] == REBUILD_FORCED ? "F" : "C";
+  } else {
+    for (int k = 0; k < n; ++k) {
+      if (since >= interval) {
+        rebuild[k] = REBUILD_FORCED;
+        since = 0;
+      }
+      since++;
+      key.push_back(rebuild[k] ? 'r' : '.');
     }
-    since++;
-    key.push_back(rebuild[k] ? 'r' : '.');
   }
   auto it = graphs.find(key);
   if (it == graphs.end()) {
@@ -1480,7 +1552,7 @@ void Engine::run_block(int n, bool barostat, bool energy_last) {
       int mode = (k == 0 ? INT_OPEN : (INT_CLOSE | INT_OPEN));
       if (k == n - 1) mode |= INT_OPEN_KINETIC;
       launch_integrate(iargs(k), mode, stream);
-      record_forces(rebuild[k] != 0, energy_last && k == n - 1);
+      record_forces(rebuild[k], energy_last && k == n - 1);
     }
     launch_integrate(iargs(n - 1), INT_CLOSE | INT_CLOSE_KINETIC, stream);
     launch_advance_steps(step_base.p, S, n, stream);
@@ -1508,9 +1580,13 @@ void Engine::run_block(int n, bool barostat, bool energy_last) {
   // host bookkeeping mirrors the device
   for (auto &h : hs) {
     int64_t s2 = barostat ? (1LL << 40) : h.steps_since_rebuild;
-    for (int k = 0; k < n; ++k) {
-      if (s2 >= interval) s2 = 0;
-      s2++;
+    if (on_demand) {
+      s2 = 1;  // the device keeps the lists fresh from here on
+    } else {
+      for (int k = 0; k < n; ++k) {
+        if (s2 >= interval) s2 = 0;
+        s2++;
+      }
     }
     h.steps_since_rebuild = s2;
     h.step += n;
@@ -1523,6 +1599,12 @@ void Engine::run_block(int n, bool barostat, bool energy_last) {
 void Engine::check_block(int steps) {
   std::vector<unsigned> d(2 * S);
   CUDA_OK(cudaMemcpy(d.data(), disp.p, sizeof(unsigned) * 2 * S, cudaMemcpyDeviceToHost));
+  if (on_demand) {  // the rebuild bodies that ran inside the block's graph
+    unsigned long long taken = 0;
+    CUDA_OK(cudaMemcpy(&taken, list_builds.p, sizeof taken, cudaMemcpyDeviceToHost));
+    kernel_launches += 6LL * (long long)(taken - conditional_builds_seen);
+    conditional_builds_seen = taken;
+  }
   for (int s = 0; s < S; ++s) {
     HostSystem &h = hs[s];
     float f0, f1;
@@ -1539,6 +1621,12 @@ void Engine::check_block(int steps) {
     const double worst = std::sqrt(std::max(0.0, (double)sq));
     h.worst_displacement = std::max(h.worst_displacement, worst);
     const double usage = 2.0 * worst / h.skin;
+    if (on_demand) {
+      // the block's largest displacement was measured before the step's rebuild decision:
+      // every force evaluation used a list that the check had found valid
+      h.worst_skin_usage = std::max(h.worst_skin_usage, std::min(usage, 1.0));
+      continue;
+    }
     h.worst_skin_usage = std::max(h.worst_skin_usage, usage);
     if (usage <= 1.0) {
       h.calm_blocks++;
@@ -1905,6 +1993,7 @@ void rmd_default_options(rmd_options *o) {
   o->max_constraint_iterations = 150;
   o->rebuild_interval = 20;
   o->adaptive_rebuild = 1;
+  o->rebuild_on_demand = 1;
   o->pressure = RMD_NO_PRESSURE;
   o->barostat_interval = 25;
   o->dispersion_correction = 1;
@@ -2117,6 +2206,10 @@ rmd_status rmd_diagnostics_at(rmd_sim *sim, int32_t s, rmd_diagnostics_report *o
     bytes += e.posq.bytes() * 4 + e.force.bytes() * 2 + e.nbr.bytes() + e.fixed_grid.bytes() + e.half.bytes() +
              e.real_grid.bytes() + e.cell_atoms.bytes() * 2 + e.e_lj.bytes() * 4;
     out->device_bytes = (int64_t)bytes;
+    unsigned long long builds[2] = {0, 0};
+    CUDA_OK(cudaMemcpy(builds, e.list_builds.p, sizeof builds, cudaMemcpyDeviceToHost));
+    out->list_builds = (int64_t)builds[1];
+    out->rebuild_on_demand = e.on_demand ? 1 : 0;
   });
 }
 

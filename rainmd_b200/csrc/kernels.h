@@ -89,6 +89,7 @@ struct LaunchCtx {
   const int *group_sys;
   int n_groups_total;
   int group_atoms;  // atoms per neighbour-search group: 4, 8, 16 or 32
+  const int *rebuild_only;  // per-system flags: rebuild only the flagged systems (null: every system)
   const int *excl_start, *excl_partners;
   int *nbr, *nbr_count, *required;
   float4 *origin;
@@ -140,6 +141,13 @@ struct LaunchCtx {
 };
 
 void launch_rebuild(const LaunchCtx &c, cudaStream_t stream);
+// Rebuild on demand (lists.cu): flag the systems that have moved past half their skin since
+// their last build and set `handle` (an IF node's condition) when any has; and the reset every
+// rebuild starts with (of the flagged systems, or of all when `only` is null).
+void launch_rebuild_decide(cudaGraphConditionalHandle handle, const unsigned *disp, const DevSys *sys, int S,
+                           int *stale, unsigned long long *rebuilds, cudaStream_t stream);
+void launch_rebuild_reset(int *required, int *required_max, unsigned *disp, int S, unsigned long long *builds,
+                          const int *only, cudaStream_t stream);
 // group slots a system needs for a given group size (its search groups never exceed this)
 int neighbour_group_slots(int atoms, int cells, int group_atoms);
 void launch_nonbonded(const LaunchCtx &c, bool energy, int lanes, cudaStream_t stream);

@@ -30,9 +30,10 @@ struct LaunchCtxView {
 
 __global__ void k_cells_assign(const float4 *__restrict__ posq, const int *__restrict__ sys_of_atom,
                                const DevSys *__restrict__ sys, int *__restrict__ cell_of_atom,
-                               int *__restrict__ cell_count, int n_atoms) {
+                               int *__restrict__ cell_count, int n_atoms, const int *__restrict__ only) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n_atoms) return;
+  if (only && !only[sys_of_atom[i]]) return;
   const DevSys &s = sys[sys_of_atom[i]];
   float4 p = posq[i];
   int3 c = cell_coord(make_float3(p.x, p.y, p.z), s);
@@ -73,7 +74,9 @@ __device__ __forceinline__ int block_exclusive_scan(int v, int *warp_totals, int
 // of neighbour-search groups per cell (ceil(count / group_atoms)) into cell_gstart;
 // count -> 0.
 __global__ void k_cells_scan(const DevSys *__restrict__ sys, int *__restrict__ cell_count,
-                             int *__restrict__ cell_start, int *__restrict__ cell_gstart, int group_atoms) {
+                             int *__restrict__ cell_start, int *__restrict__ cell_gstart, int group_atoms,
+                             const int *__restrict__ only) {
+  if (only && !only[blockIdx.x]) return;
   const DevSys &s = sys[blockIdx.x];
   const int cells = s.cell_counts[0] * s.cell_counts[1] * s.cell_counts[2];
   __shared__ int warp_totals[2][32];
@@ -101,9 +104,10 @@ __global__ void k_cells_scan(const DevSys *__restrict__ sys, int *__restrict__ c
 __global__ void k_cells_scatter(const int *__restrict__ sys_of_atom, const DevSys *__restrict__ sys,
                                 const int *__restrict__ cell_of_atom, const int *__restrict__ cell_start,
                                 int *__restrict__ cell_cursor, int *__restrict__ cell_atoms,
-                                int n_atoms) {
+                                int n_atoms, const int *__restrict__ only) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n_atoms) return;
+  if (only && !only[sys_of_atom[i]]) return;
   const DevSys &s = sys[sys_of_atom[i]];
   int cell = cell_of_atom[i];
   int slot = cell_start[s.cell_start_base + cell] + atomicAdd(&cell_cursor[s.cell_base + cell], 1);
@@ -145,8 +149,9 @@ __device__ __forceinline__ int place_sorted(const LaunchCtxView &v, const DevSys
 // slot) into group_order, so that 32 consecutive entries there are spatially compact.
 __global__ void k_cells_sort(const int *__restrict__ cell_sys, const DevSys *__restrict__ sys,
                              const int *__restrict__ cell_start, int *__restrict__ cell_cursor,
-                             int *__restrict__ cell_atoms, LaunchCtxView v) {
+                             int *__restrict__ cell_atoms, LaunchCtxView v, const int *__restrict__ only) {
   const int g = blockIdx.x;
+  if (only && !only[cell_sys[g]]) return;
   const DevSys &s = sys[cell_sys[g]];
   const int c = g - s.cell_base;
   const int cells = s.cell_counts[0] * s.cell_counts[1] * s.cell_counts[2];
@@ -234,7 +239,7 @@ __global__ void __launch_bounds__(32 * NBR_WARPS)
                  const int *__restrict__ excl_start, const int *__restrict__ excl_partners,
                  const float4 *__restrict__ spos, const int *__restrict__ sorted_orig,
                  int *__restrict__ nbr, int *__restrict__ nbr_count, int *__restrict__ required,
-                 float4 *__restrict__ origin, int n_groups) {
+                 float4 *__restrict__ origin, int n_groups, const int *__restrict__ only) {
   constexpr int J = 32 / G;
   __shared__ float4 stage_pos[NBR_WARPS][32];
   __shared__ int stage_orig[NBR_WARPS][32];
@@ -244,6 +249,7 @@ __global__ void __launch_bounds__(32 * NBR_WARPS)
   const int a = lane / J, sub = lane % J;
   if (warp >= n_groups) return;
   const int sidx = group_sys[warp];
+  if (only && !only[sidx]) return;  // this system's lists are still valid
   const DevSys &s = sys[sidx];
   const int q = warp - s.group_base;
   const int counts[3] = {s.cell_counts[0], s.cell_counts[1], s.cell_counts[2]};
@@ -415,6 +421,57 @@ __global__ void __launch_bounds__(32 * NBR_WARPS)
   if (lane == 0) atomicMax(&required[sidx], most);
 }
 
+// ---------------------------------------------------------------- rebuild on demand
+// A list built with cutoff rc + skin holds every pair that is within rc while no atom has
+// moved more than skin / 2 from where it was at the build (two atoms close by at most the sum
+// of their displacements). The integrator leaves each system's largest squared displacement
+// since the build in disp[s]; this kernel sets the graph's IF condition so that the rebuild
+// runs exactly when some system of the batch has passed that bound (with a 0.1% margin on the
+// squared distance for the f32 skin), and counts the rebuilds. A non-finite displacement does
+// not trigger one: the host's block check reports it.
+__global__ void k_rebuild_decide(cudaGraphConditionalHandle handle, const unsigned *__restrict__ disp,
+                                 const DevSys *__restrict__ sys, int S, int *__restrict__ stale,
+                                 unsigned long long *__restrict__ rebuilds) {
+  int need = 0;
+  for (int s = threadIdx.x; s < S; s += blockDim.x) {
+    const float skin = sys[s].list_cutoff - sys[s].cutoff;
+    const float limit2 = 0.25f * skin * skin * 0.999f;
+    const int mine = __uint_as_float(disp[s]) > limit2;
+    stale[s] = mine;
+    need |= mine;
+  }
+  need = __syncthreads_or(need);
+  if (threadIdx.x == 0) {
+    cudaGraphSetConditional(handle, need ? 1u : 0u);
+    if (need) *rebuilds += 1;
+  }
+}
+
+// Start of every rebuild: fold the previous build's requirement into the running maximum the
+// host reads after each block (so an overflow at a rebuild inside a block is seen too), then
+// clear the requirement and the displacement since the build, and count the build.
+__global__ void k_rebuild_reset(int *__restrict__ required, int *__restrict__ required_max,
+                                unsigned *__restrict__ disp, int S, unsigned long long *__restrict__ builds,
+                                const int *__restrict__ only) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) *builds += 1;
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < S; s += gridDim.x * blockDim.x) {
+    if (only && !only[s]) continue;
+    required_max[s] = max(required_max[s], required[s]);
+    required[s] = 0;
+    disp[s] = 0u;
+  }
+}
+
+void launch_rebuild_decide(cudaGraphConditionalHandle handle, const unsigned *disp, const DevSys *sys, int S,
+                           int *stale, unsigned long long *rebuilds, cudaStream_t stream) {
+  k_rebuild_decide<<<1, 256, 0, stream>>>(handle, disp, sys, S, stale, rebuilds);
+}
+
+void launch_rebuild_reset(int *required, int *required_max, unsigned *disp, int S, unsigned long long *builds,
+                          const int *only, cudaStream_t stream) {
+  k_rebuild_reset<<<(S + 255) / 256, 256, 0, stream>>>(required, required_max, disp, S, builds, only);
+}
+
 int neighbour_group_slots(int atoms, int cells, int group_atoms) {
   return (atoms + group_atoms - 1) / group_atoms + cells;
 }
@@ -423,21 +480,23 @@ void launch_rebuild(const LaunchCtx &ctx, cudaStream_t stream) {
   const int n = ctx.n_atoms;
   const int tb = 128;
   const int G = ctx.group_atoms;
+  const int *only = ctx.rebuild_only;
   k_cells_assign<<<(n + tb - 1) / tb, tb, 0, stream>>>(ctx.posq, ctx.sys_of_atom, ctx.sys,
-                                                        ctx.cell_of_atom, ctx.cell_count, n);
-  k_cells_scan<<<ctx.n_systems, 1024, 0, stream>>>(ctx.sys, ctx.cell_count, ctx.cell_start, ctx.cell_gstart, G);
+                                                        ctx.cell_of_atom, ctx.cell_count, n, only);
+  k_cells_scan<<<ctx.n_systems, 1024, 0, stream>>>(ctx.sys, ctx.cell_count, ctx.cell_start, ctx.cell_gstart, G,
+                                                   only);
   k_cells_scatter<<<(n + tb - 1) / tb, tb, 0, stream>>>(ctx.sys_of_atom, ctx.sys, ctx.cell_of_atom,
                                                          ctx.cell_start, ctx.cell_count,
-                                                         ctx.cell_atoms, n);
+                                                         ctx.cell_atoms, n, only);
   LaunchCtxView v{ctx.posq, ctx.atom_type, ctx.spos, ctx.wrap, ctx.sorted_orig, ctx.sorted_type, ctx.rank,
                   ctx.group_order};
   k_cells_sort<<<ctx.n_cells_total, 128, 0, stream>>>(ctx.cell_sys, ctx.sys, ctx.cell_start,
-                                                      ctx.cell_count, ctx.cell_atoms, v);
+                                                      ctx.cell_count, ctx.cell_atoms, v, only);
   const int blocks = (ctx.n_groups_total + NBR_WARPS - 1) / NBR_WARPS;
 #define RMD_NBR_ARGS                                                                                      \
   ctx.posq, ctx.group_sys, ctx.sys, ctx.cell_start, ctx.cell_gstart, ctx.group_order, ctx.excl_start,  \
       ctx.excl_partners, ctx.spos, ctx.sorted_orig, ctx.nbr, ctx.nbr_count, ctx.required, ctx.origin, \
-      ctx.n_groups_total
+      ctx.n_groups_total, only
   if (G == 4)
     k_neighbours<4><<<blocks, 32 * NBR_WARPS, 0, stream>>>(RMD_NBR_ARGS);
   else if (G == 8)

@@ -74,12 +74,32 @@ __global__ void __launch_bounds__(128) k_nonbonded(
 
   float fx = 0.f, fy = 0.f, fz = 0.f, elj = 0.f, ecoul = 0.f, evir = 0.f;
   long long qx = 0, qy = 0, qz = 0, qlj = 0, qcoul = 0, qvir = 0;
-  for (int k = lane; k < count; k += LANES) {
-    const unsigned e = (unsigned)__ldg(row + k);
-    const int g = (int)(e & NBR_SLOT_MASK);
-    const float4 pj = __ldg(spos + g);
-    const int tj = __ldg(sorted_type + g);  // issued with the position, not after the cutoff test
-    const float4 S = s.shift[e >> NBR_SLOT_BITS];  // the partner's image (code 0..26), fixed at the rebuild
+  // Software pipeline over the lane's entries: the row word two entries ahead and the
+  // partner record (position, type, image shift) one entry ahead are in flight while this
+  // entry's pair is computed, so the gathers' latency overlaps the arithmetic.
+  int k = lane;
+  unsigned e1 = 0, e2 = 0;
+  float4 pj1 = make_float4(0.f, 0.f, 0.f, 0.f), S1 = pj1;
+  int tj1 = 0;
+  if (k < count) {
+    e1 = (unsigned)__ldg(row + k);
+    const int g = (int)(e1 & NBR_SLOT_MASK);
+    pj1 = __ldg(spos + g);
+    tj1 = __ldg(sorted_type + g);
+    S1 = s.shift[e1 >> NBR_SLOT_BITS];  // the partner's image (code 0..26), fixed at the rebuild
+  }
+  if (k + LANES < count) e2 = (unsigned)__ldg(row + k + LANES);
+  for (; k < count; k += LANES) {
+    const float4 pj = pj1, S = S1;
+    const int tj = tj1;
+    if (k + LANES < count) {
+      e1 = e2;
+      const int g = (int)(e1 & NBR_SLOT_MASK);
+      pj1 = __ldg(spos + g);
+      tj1 = __ldg(sorted_type + g);
+      S1 = s.shift[e1 >> NBR_SLOT_BITS];
+      if (k + 2 * LANES < count) e2 = (unsigned)__ldg(row + k + 2 * LANES);
+    }
     const float3 d = make_float3(pw.x - pj.x - S.x, pw.y - pj.y - S.y, pw.z - pj.z - S.z);
     const float r2 = fmaf(d.x, d.x, fmaf(d.y, d.y, d.z * d.z));
     if (r2 <= cut2) {

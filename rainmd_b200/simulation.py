@@ -57,7 +57,7 @@ _OPTION_NAMES = {
     "forceAccumulation": "force_accumulation", "neighbourGroupAtoms": "neighbour_group_atoms",
     "nonbondedLanes": "nonbonded_lanes", "spreadAtomsPerBlock": "spread_atoms_per_block",
     "learnedWarmupMoves": "learned_warmup_moves", "learnedStepsPerMove": "learned_steps_per_move",
-    "learnedRate": "learned_rate",
+    "learnedRate": "learned_rate", "rebuildOnDemand": "rebuild_on_demand",
 }
 
 
