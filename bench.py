@@ -208,6 +208,54 @@ def learned_barostat_study(ps: float, seed: int = 3, warmup_moves: int = 2000):
     return out
 
 
+def trajectory_study(frames: int = 50, seed: int = 2):
+    """Trajectory output from the device (shared/traj/*.js restated in csrc/traj.cu): per
+    DCD frame and per restart, the whole call through the public API (imaging and packing
+    on the device, one copy of the finished bytes to the host), next to the position read
+    alone that any host-side writer starts from, and the CPU restatement of the writer."""
+    import oracle.traj as ot
+    from rainmd_b200 import traj
+    from rainmd_b200.simulation import GpuSimulation
+
+    out = {"study": "trajectory"}
+    for name in ("water-23558", "water-99999"):
+        system, pos, grid = workload(name, seed)
+        n = system["topology"]["atomCount"]
+        sim = GpuSimulation(system, options_for(grid, seed))
+        sim.setState(pos)
+        sim.initialise()
+        sim.minimise(maxIterations=20, forceTolerance=1000.0)
+        sim.run(500, blockSize=100)
+        writer = traj.DcdWriter(n, TIMESTEP_PS, 1, periodic=True)
+        writer.appendFrame(sim)
+        t0 = time.perf_counter()
+        for _ in range(frames):
+            writer.appendFrame(sim)
+        dcd_ms = (time.perf_counter() - t0) * 1e3 / frames
+        traj.writeRestart(sim)
+        t0 = time.perf_counter()
+        for _ in range(10):
+            text = traj.writeRestart(sim)
+        rst7_ms = (time.perf_counter() - t0) * 1e3 / 10
+        t0 = time.perf_counter()
+        for _ in range(frames):
+            state = sim.readState()
+        read_ms = (time.perf_counter() - t0) * 1e3 / frames
+        t = system["topology"]
+        t0 = time.perf_counter()
+        ot.dcd_frame(state["positions"].astype(np.float64), state["boxVectors"], t["moleculeOfAtom"],
+                     t["moleculeCount"])
+        cpu_dcd_ms = (time.perf_counter() - t0) * 1e3
+        frame_bytes = len(writer.chunks[0])
+        out[name] = {"atoms": n, "dcd_frame_bytes": frame_bytes, "dcd_ms_per_frame": dcd_ms,
+                     "dcd_frame_gb_per_s": frame_bytes / (dcd_ms * 1e-3) / 1e9,
+                     "restart_bytes": len(text), "restart_ms": rst7_ms,
+                     "read_state_ms": read_ms,
+                     "cpu_oracle_dcd_ms_per_frame": cpu_dcd_ms}
+        sim.release()
+    return out
+
+
 def large_combined_study(steps: int, seed: int = 5):
     """250,000 atoms (a 4,000-atom chain in TIP3P water, PME order 4 on 128^3) advanced in one
     batch with 16 solvated systems of 5,000-20,000 atoms, all NPT at 1 bar with the learned
@@ -423,7 +471,8 @@ def config_block(args, atoms, grid, world):
     return {"workload": f"{args.workload}: TIP3P water NVT 300 K, 2 fs, rc 0.9 nm, PME order 4 "
                         f"{grid[0]}x{grid[1]}x{grid[2]}, SETTLE, Langevin 1/ps",
             "atoms": atoms, "replicas": world, "parallelism": f"replicas{world}",
-            "l2": "flushed (256 MB written) before every timed block"}
+            "l2": "flushed (256 MB written) before every timed block",
+            "lists": "reference host schedule" if args.rebuild_schedule else "rebuilt on demand"}
 
 
 def main():
@@ -439,10 +488,13 @@ def main():
     parser.add_argument("--minimise", type=int, default=200, help="minimiser iterations before dynamics")
     parser.add_argument("--equilibrate", type=int, default=3000, help="untimed steps before warm-up")
     parser.add_argument("--no-batched", action="store_true", help="skip the 64-system batch measurement")
-    parser.add_argument("--study", choices=["learned-barostat", "large-combined"], default=None,
+    parser.add_argument("--study", choices=["learned-barostat", "large-combined", "trajectory"], default=None,
                         help="run a study instead of the benchmark and print its JSON line")
     parser.add_argument("--ps", type=float, default=500.0, help="length of a study run")
     parser.add_argument("--batch-steps", type=int, default=500)
+    parser.add_argument("--rebuild-schedule", action="store_true",
+                        help="rebuild the lists on the reference's host schedule instead of on demand "
+                             "(the same kernels; ncu profiles no kernel of a graph with conditional nodes)")
     args = parser.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -459,6 +511,10 @@ def main():
         if rank == 0:
             print(json.dumps(large_combined_study(args.steps)), flush=True)
         return
+    if args.study == "trajectory":
+        if rank == 0:
+            print(json.dumps(trajectory_study()), flush=True)
+        return
     # one GPU per process: make this rank's GPU device 0 before any CUDA initialisation
     if world > 1:
         os.environ["CUDA_VISIBLE_DEVICES"] = str(local)
@@ -474,7 +530,10 @@ def main():
 
     system, pos, grid = workload(args.workload, seed=1 + rank)
     n = system["topology"]["atomCount"]
-    sim = GpuSimulation(system, options_for(grid, seed=7 + rank))
+    opts = options_for(grid, seed=7 + rank)
+    if args.rebuild_schedule:
+        opts["rebuildOnDemand"] = False
+    sim = GpuSimulation(system, opts)
     sim.setState(pos)
     sim.initialise()
     sim.minimise(maxIterations=args.minimise, forceTolerance=1000.0)

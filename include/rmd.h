@@ -337,6 +337,42 @@ rmd_status rmd_set_kernel_shapes(rmd_sim *sim, int32_t group_atoms, int32_t nonb
  * per-pair fixed-point (1) or per-lane f32 (0) force accumulation. */
 rmd_status rmd_debug_set_nonbonded(rmd_sim *sim, int32_t lanes, int32_t pair_fixed);
 
+/* ---- On-device trajectory output (shared/traj/imaging.js, dcd.js, rst7.js). The page feeds
+ * readPositions() into these writers on the host; here the device images and packs the frame
+ * from its own position buffer and the caller receives finished bytes. */
+
+/* imageMolecules (shared/traj/imaging.js:39-91) of the system's current positions: every
+ * molecule translated by whole lattice vectors (c, then b, then a) so that its centroid lies in
+ * the cell, as FP64 nm, 3 per atom. */
+rmd_status rmd_image_molecules_at(rmd_sim *sim, int32_t system_index, double *positions_out);
+
+/* Bytes of one DCD frame (shared/traj/dcd.js:130-160): the 56-byte cell record when
+ * `periodic`, then the x, y and z records of 4 * atom_count + 8 bytes each. */
+int64_t rmd_dcd_frame_bytes(int32_t atom_count, int32_t periodic);
+
+/* DcdWriter.appendFrame (shared/traj/dcd.js:96-161) from the device: the frame's bytes,
+ * imaged by molecule when `image` (the writer's `molecules` option) and carrying the live
+ * box's cell record when `periodic`. A non-finite coordinate refuses the frame with
+ * RMD_ERR_NON_FINITE (dcd.js:112-128) and writes nothing. */
+rmd_status rmd_dcd_frame_at(rmd_sim *sim, int32_t system_index, int32_t periodic, int32_t image,
+                            uint8_t *frame_out);
+
+/* The 276-byte header DcdWriter.finish writes (shared/traj/dcd.js:175-199): `created` is the
+ * second title line (the reference writes "Created <ISO time>"); NULL leaves it empty. Needs no
+ * simulation and no GPU. */
+rmd_status rmd_dcd_header(int32_t atom_count, int32_t frames, int32_t first_step, int32_t interval,
+                          double timestep, int32_t periodic, const char *title, const char *created,
+                          uint8_t header_out[276]);
+
+/* writeRestart (shared/traj/rst7.js:63-101) of the system's device state: the title line, the
+ * atom count and `time` (ps), positions in angstroms, velocities in angstroms per AMBER time
+ * unit when `velocities`, and the live box as lengths and angles when `box`, every value as
+ * ECMAScript's toFixed(7) in 12 columns, six to a line. `out` NULL: only `*bytes` is set. A
+ * non-finite value gives RMD_ERR_NON_FINITE and one wider than 12 columns RMD_ERR_INVALID,
+ * whichever comes first in the file, and nothing is written. */
+rmd_status rmd_restart_at(rmd_sim *sim, int32_t system_index, const char *title, double time,
+                          int32_t velocities, int32_t box, char *out, int64_t capacity, int64_t *bytes);
+
 /* Allocation-free PME charge spreading, for callers that cannot call cudaMalloc: code
  * recording into its own CUDA graph during stream capture, hosts whose device memory all
  * comes from their own arena, and latency-bound callers that cannot take cudaMalloc's

@@ -130,7 +130,8 @@ EXPORTS = [
     "rmd_debug_time_kernel", "rmd_debug_kernel_launches", "rmd_debug_set_nonbonded",
     "rmd_bench_run", "rmd_debug_force_term", "rmd_debug_read", "rmd_spread_charges_noalloc",
     "rmd_kernel_shapes", "rmd_set_kernel_shapes", "rmd_surrogate_report_at", "rmd_surrogate_weights",
-    "rmd_surrogate_evaluate",
+    "rmd_surrogate_evaluate", "rmd_image_molecules_at", "rmd_dcd_frame_bytes", "rmd_dcd_frame_at",
+    "rmd_dcd_header", "rmd_restart_at",
 ]
 
 _lib = None
@@ -197,6 +198,14 @@ def load():
     lib.rmd_debug_read.argtypes = [sim, C.c_int32, C.c_int32, _dp]
     lib.rmd_spread_charges_noalloc.argtypes = [C.c_void_p, C.c_int32, _dp, _i32p, C.c_int32, C.c_void_p,
                                                C.c_void_p]
+    lib.rmd_image_molecules_at.argtypes = [sim, C.c_int32, _dp]
+    lib.rmd_dcd_frame_bytes.argtypes = [C.c_int32, C.c_int32]
+    lib.rmd_dcd_frame_bytes.restype = C.c_int64
+    lib.rmd_dcd_frame_at.argtypes = [sim, C.c_int32, C.c_int32, C.c_int32, C.c_void_p]
+    lib.rmd_dcd_header.argtypes = [C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_double, C.c_int32,
+                                   C.c_char_p, C.c_char_p, C.c_void_p]
+    lib.rmd_restart_at.argtypes = [sim, C.c_int32, C.c_char_p, C.c_double, C.c_int32, C.c_int32, C.c_void_p,
+                                   C.c_int64, C.POINTER(C.c_int64)]
     for name in EXPORTS:
         fn = getattr(lib, name)
         if fn.restype is C.c_int and name not in ("rmd_system_count",):

@@ -19,6 +19,7 @@ import numpy as np
 # shared/units.js
 KCAL_TO_KJ = 4.184
 NM_PER_ANGSTROM = 0.1
+AMBER_VELOCITY_SCALE = 20.455  # angstroms per AMBER time unit -> per ps (units.js:44)
 AMBER_CHARGE_SCALE = 18.2223
 ENERGY_SCALE = KCAL_TO_KJ
 BOND_K_SCALE = 2 * KCAL_TO_KJ / (NM_PER_ANGSTROM * NM_PER_ANGSTROM)
@@ -268,9 +269,13 @@ def parse_prmtop(text: str) -> dict:
 
 
 def parse_inpcrd(text: str, expected_atom_count: int | None = None) -> dict:
-    """ASCII inpcrd/rst7 in 12-column fields, Å → nm (inpcrd.js:34-130)."""
+    """ASCII inpcrd/rst7 in 12-column fields, Å → nm, velocities Å per AMBER time unit → nm/ps
+    (inpcrd.js:34-130)."""
     lines = text.splitlines()
-    atom_count = int(lines[1].split()[0])
+    title = lines[0].strip()
+    header = lines[1].split()
+    atom_count = int(header[0])
+    time = float(header[1]) if len(header) > 1 else None
     if expected_atom_count is not None and expected_atom_count != atom_count:
         raise ValueError(f"coordinate file has {atom_count} atoms but the topology has "
                          f"{expected_atom_count}")
@@ -289,12 +294,13 @@ def parse_inpcrd(text: str, expected_atom_count: int | None = None) -> dict:
     if total not in (n3, n3 + 6, 2 * n3, 2 * n3 + 6):
         raise ValueError(f"inpcrd holds {total} numbers for {atom_count} atoms")
     positions = np.array(numbers[:n3]) * NM_PER_ANGSTROM
-    velocities = np.array(numbers[n3:2 * n3]) if has_vel else None
+    velocities = (np.array(numbers[n3:2 * n3]) * AMBER_VELOCITY_SCALE * NM_PER_ANGSTROM) if has_vel else None
     box = None
     if has_box:
         b = numbers[-6:]
         box = {"lengths": [b[0] * 0.1, b[1] * 0.1, b[2] * 0.1], "angles": [b[3], b[4], b[5]]}
-    return {"atomCount": atom_count, "positions": positions, "velocities": velocities, "box": box}
+    return {"title": title, "atomCount": atom_count, "time": time, "positions": positions,
+            "velocities": velocities, "box": box}
 
 
 def box_vectors_from_lengths_and_angles(box: dict) -> np.ndarray:

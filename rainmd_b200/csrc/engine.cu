@@ -7,6 +7,7 @@
 // per block of steps: one replay launches every kernel of every step of every system.
 #include <algorithm>
 #include <array>
+#include <climits>
 #include <cmath>
 #include <functional>
 #include <map>
@@ -234,7 +235,12 @@ struct Engine {
   DevArray<int3> settle_atoms;
   DevArray<DevSettle> settle_param;
   int n_free = 0, n_clusters = 0, n_settle = 0;
-  DevArray<int> mol_start, mol_atoms;
+  DevArray<int> mol_start, mol_atoms, mol_of_atom;
+  // trajectory output (traj.cu): per-molecule translations, a staging buffer, error slots
+  DevArray<double3> traj_shift;
+  DevArray<unsigned char> traj_out;
+  DevArray<int> traj_status;
+  TrajArgs traj_args(int s, bool image);  // sizes the scratch; computes the translations when imaging
   DevArray<double> mol_vir, e_term_vir;
   std::vector<int> mol_base;  // first molecule of each system (S + 1)
   int n_molecules_total = 0;
@@ -765,7 +771,7 @@ void Engine::upload_all(const std::vector<const rmd_system *> &src) {
 
   // ---- molecules (global CSR over all systems)
   {
-    std::vector<int> ms(1, 0), ma;
+    std::vector<int> ms(1, 0), ma, moa(N, 0);
     mol_base.assign(1, 0);
     for (int s = 0; s < S; ++s) {
       const rmd_system &r = *src[s];
@@ -776,6 +782,7 @@ void Engine::upload_all(const std::vector<const rmd_system *> &src) {
         const int m = r.molecule_of_atom[a];
         if (m < 0 || m >= r.molecule_count) throw Error(RMD_ERR_INVALID, "molecule index out of range");
         mol[m].push_back(base + a);
+        moa[base + a] = mol_base[s] + m;
       }
       for (auto &m : mol) {
         ma.insert(ma.end(), m.begin(), m.end());
@@ -788,6 +795,7 @@ void Engine::upload_all(const std::vector<const rmd_system *> &src) {
     if (ma.empty()) ma.push_back(0);
     mol_start.upload(ms);
     mol_atoms.upload(ma);
+    mol_of_atom.upload(moa);
   }
 
   // ---- cells
@@ -1947,6 +1955,31 @@ void Engine::minimise(int max_iterations, double force_tolerance, double max_ste
   }
 }
 
+TrajArgs Engine::traj_args(int s, bool image) {
+  const HostSystem &h = hs[s];
+  TrajArgs t{};
+  t.posq = posq.p;
+  t.vel = vel.p;
+  t.mol_start = mol_start.p;
+  t.mol_atoms = mol_atoms.p;
+  t.mol_of_atom = mol_of_atom.p;
+  t.sysd = sysd.p;
+  t.sys = s;
+  t.atom_start = h.atom_start;
+  t.atom_count = h.n;
+  t.mol_first = mol_base[s];
+  t.mol_count = mol_base[s + 1] - mol_base[s];
+  t.image = image && t.mol_count > 0 ? 1 : 0;
+  if (traj_shift.n < (size_t)std::max(1, t.mol_count)) traj_shift.alloc(std::max(1, t.mol_count));
+  if (traj_status.n < 2) traj_status.alloc(2);
+  t.shift = traj_shift.p;
+  t.status = traj_status.p;
+  const int none[2] = {INT_MAX, INT_MAX};
+  CUDA_OK(cudaMemcpyAsync(traj_status.p, none, sizeof none, cudaMemcpyHostToDevice, stream));
+  if (t.image) launch_traj_shifts(t, stream);
+  return t;
+}
+
 }  // namespace rmd
 
 // =========================================================================== C ABI
@@ -2584,3 +2617,173 @@ rmd_status rmd_debug_fft(rmd_sim *sim, int32_t s, const double *data, double *ha
 }
 
 }  // extern "C"
+
+
+// ----------------------------------------------------------------- trajectory output
+// ECMAScript x.toExponential(7) (rst7.js:69): eight significant digits of the exact binary
+// value, the larger on a tie, "e", the exponent's sign and its digits without padding.
+static std::string script_exponential7(double x) {
+  if (x == 0.0) return "0.0000000e+0";
+  std::string sign = x < 0 ? "-" : "";
+  const double a = std::fabs(x);
+  // 40 exact significant digits (glibc prints the exact decimal expansion, rounded only at
+  // the last digit shown), then the tie-up rounding at the eighth by hand
+  char buf[64];
+  snprintf(buf, sizeof buf, "%.39e", a);
+  std::string digits;
+  const char *p = buf;
+  for (; *p && *p != 'e'; ++p)
+    if (*p >= '0' && *p <= '9') digits.push_back(*p);
+  int exponent = atoi(p + 1);
+  std::string head = digits.substr(0, 8);
+  bool up = digits[8] >= '5';
+  if (up) {
+    int k = 7;
+    while (k >= 0 && head[k] == '9') head[k--] = '0';
+    if (k < 0) {
+      head = "1" + head.substr(0, 7);
+      exponent += 1;
+    } else {
+      head[k] = (char)(head[k] + 1);
+    }
+  }
+  return sign + head.substr(0, 1) + "." + head.substr(1) + "e" + (exponent < 0 ? "-" : "+") +
+         std::to_string(std::abs(exponent));
+}
+
+static std::string pad_start(const std::string &s, size_t width) {
+  return s.size() >= width ? s : std::string(width - s.size(), ' ') + s;
+}
+
+rmd_status rmd_image_molecules_at(rmd_sim *sim, int32_t s, double *out) {
+  if (rmd_status c = check_index(sim, s)) return c;
+  if (!out) return RMD_ERR_INVALID;
+  return guarded(sim, [&]() {
+    auto &e = sim->engine;
+    const rmd::TrajArgs t = e.traj_args(s, true);
+    rmd::DevArray<double> wrapped;
+    wrapped.alloc(3 * (size_t)t.atom_count);
+    rmd::launch_traj_image(t, wrapped.p, e.stream);
+    CUDA_OK(cudaGetLastError());
+    CUDA_OK(cudaMemcpyAsync(out, wrapped.p, sizeof(double) * wrapped.n, cudaMemcpyDeviceToHost, e.stream));
+    e.sync();
+    wrapped.release();
+  });
+}
+
+int64_t rmd_dcd_frame_bytes(int32_t atom_count, int32_t periodic) {
+  if (atom_count < 0) return -1;
+  return (periodic ? 56 : 0) + 3 * (4 * (int64_t)atom_count + 8);
+}
+
+rmd_status rmd_dcd_frame_at(rmd_sim *sim, int32_t s, int32_t periodic, int32_t image, uint8_t *out) {
+  if (rmd_status c = check_index(sim, s)) return c;
+  if (!out) return RMD_ERR_INVALID;
+  return guarded(sim, [&]() {
+    auto &e = sim->engine;
+    rmd::TrajArgs t = e.traj_args(s, image != 0);
+    const size_t bytes = (size_t)rmd_dcd_frame_bytes(t.atom_count, periodic);
+    if (e.traj_out.n < bytes) e.traj_out.alloc(bytes);
+    t.out = e.traj_out.p;
+    rmd::launch_dcd_pack(t, periodic ? 1 : 0, e.stream);
+    CUDA_OK(cudaGetLastError());
+    int status[2];
+    CUDA_OK(cudaMemcpyAsync(status, e.traj_status.p, sizeof status, cudaMemcpyDeviceToHost, e.stream));
+    e.sync();
+    if (status[0] != INT_MAX)  // dcd.js:112-128
+      throw rmd::Error(RMD_ERR_NON_FINITE,
+                       "the simulation is no longer a number: a coordinate handed to the DCD writer (atom " +
+                           std::to_string(status[0]) + ") is not finite. The frame was refused, so the file "
+                           "holds the frames written before it and is still readable.");
+    CUDA_OK(cudaMemcpy(out, e.traj_out.p, bytes, cudaMemcpyDeviceToHost));
+  });
+}
+
+rmd_status rmd_dcd_header(int32_t atom_count, int32_t frames, int32_t first_step, int32_t interval, double timestep,
+                          int32_t periodic, const char *title, const char *created, uint8_t out[276]) {
+  if (!out || atom_count < 0 || frames < 0) return RMD_ERR_INVALID;
+  memset(out, 0, 276);
+  auto put32 = [&](int offset, int32_t v) { memcpy(out + offset, &v, 4); };
+  put32(0, 84);
+  memcpy(out + 4, "CORD", 4);
+  put32(8, frames);
+  put32(12, first_step);
+  put32(16, interval);
+  put32(20, std::max(0, frames - 1) * interval);  // the last frame's step, as OpenMM fills it
+  const float delta = (float)(timestep / 0.04888821);  // AKMA time units (dcd.js:56)
+  memcpy(out + 44, &delta, 4);
+  put32(48, periodic ? 1 : 0);
+  put32(84, 24);
+  put32(88, 84);
+  put32(92, 164);
+  put32(96, 2);
+  auto text = [&](int offset, const char *s) {  // NUL-padded, non-ASCII as '?' (dcd.js:243-254)
+    for (int k = 0; s && k < 80 && s[k]; ++k) {
+      const unsigned char c = (unsigned char)s[k];
+      out[offset + k] = c < 128 ? c : 0x3f;
+    }
+  };
+  text(100, title ? title : "Created by RainMD");
+  text(180, created);
+  put32(260, 164);
+  put32(264, 4);
+  put32(268, atom_count);
+  put32(272, 4);
+  return RMD_OK;
+}
+
+rmd_status rmd_restart_at(rmd_sim *sim, int32_t s, const char *title, double time, int32_t velocities, int32_t box,
+                          char *out, int64_t capacity, int64_t *bytes) {
+  if (rmd_status c = check_index(sim, s)) return c;
+  return guarded(sim, [&]() {
+    auto &e = sim->engine;
+    const auto &h = e.hs[s];
+    const std::string head = std::string(title ? title : "RainMD restart") + "\n" +
+                             pad_start(std::to_string(h.n), 5) + pad_start(script_exponential7(time), 15) + "\n";
+    const long long n3 = 3ll * h.n;
+    const long long total = (long long)head.size() + rmd::rst7_block_size(n3) * (velocities ? 2 : 1) +
+                            (box ? rmd::rst7_block_size(6) : 0);
+    if (bytes) *bytes = total;
+    if (!out) return;
+    if (capacity < total) throw rmd::Error(RMD_ERR_INVALID, "the restart needs " + std::to_string(total) + " bytes");
+    rmd::Rst7Box b{};
+    b.velocity_unit = 20.455 * 0.1;  // units.js:24, 44; rst7.js:87-89
+    if (box) {  // boxFromVectors (web/app.js:326-343) of the live box
+      rmd::DevSysD d;
+      CUDA_OK(cudaMemcpy(&d, e.sysd.p + s, sizeof d, cudaMemcpyDeviceToHost));
+      const double *v = d.box;
+      const double la = rmd::script_hypot(v[0], v[1], v[2]), lb = rmd::script_hypot(v[3], v[4], v[5]),
+                   lc = rmd::script_hypot(v[6], v[7], v[8]);
+      auto dot = [](const double *u, const double *w) { return u[0] * w[0] + u[1] * w[1] + u[2] * w[2]; };
+      auto degrees = [](double c) { return (std::acos(std::max(-1.0, std::min(1.0, c))) * 180) / M_PI; };
+      b.values[0] = la / 0.1;
+      b.values[1] = lb / 0.1;
+      b.values[2] = lc / 0.1;
+      b.values[3] = degrees(dot(v + 3, v + 6) / (lb * lc));
+      b.values[4] = degrees(dot(v, v + 6) / (la * lc));
+      b.values[5] = degrees(dot(v, v + 3) / (la * lb));
+    }
+    rmd::TrajArgs t = e.traj_args(s, false);
+    if (e.traj_out.n < (size_t)total) e.traj_out.alloc((size_t)total);
+    t.out = e.traj_out.p;
+    CUDA_OK(cudaMemcpyAsync(e.traj_out.p, head.data(), head.size(), cudaMemcpyHostToDevice, e.stream));
+    rmd::launch_rst7_format(t, (long long)head.size(), velocities ? 1 : 0, box ? 1 : 0, b, e.stream);
+    CUDA_OK(cudaGetLastError());
+    int status[2];
+    CUDA_OK(cudaMemcpyAsync(status, e.traj_status.p, sizeof status, cudaMemcpyDeviceToHost, e.stream));
+    e.sync();
+    // the first failing value in file order decides, as the reference's loop does (rst7.js:27-55)
+    if (status[0] != INT_MAX && status[0] < status[1])
+      throw rmd::Error(RMD_ERR_NON_FINITE,
+                       "the simulation is no longer a number: a coordinate handed to the restart writer (value " +
+                           std::to_string(status[0]) + ") is not finite. No restart was written. A restart is the "
+                           "one output that is fed straight back into a simulation, so writing a non-finite one "
+                           "would carry the blow-up into whatever ran next.");
+    if (status[1] != INT_MAX)
+      throw rmd::Error(RMD_ERR_INVALID,
+                       "coordinate " + std::to_string(status[1]) + " does not fit the 12-column restart format. "
+                       "An atom has left the box, which means the simulation blew up rather than that the "
+                       "writer is wrong.");
+    CUDA_OK(cudaMemcpy(out, e.traj_out.p, (size_t)total, cudaMemcpyDeviceToHost));
+  });
+}

@@ -251,6 +251,33 @@ void launch_max_force(const unsigned long long *force, const int *sys_of_atom, i
 void launch_displace(float4 *posq, const unsigned long long *force, const int *sys_of_atom, int n_atoms,
                      const float *scale, float max_disp, cudaStream_t stream);
 
+// On-device trajectory output (traj.cu): one system's atoms and molecules, the per-molecule
+// translations, the output staging buffer and two error slots (first non-finite and first
+// too-wide value; INT_MAX when none).
+struct TrajArgs {
+  const float4 *posq, *vel;
+  const int *mol_start, *mol_atoms, *mol_of_atom;
+  const DevSysD *sysd;
+  int sys, atom_start, atom_count, mol_first, mol_count, image;
+  double3 *shift;
+  unsigned char *out;
+  int *status;
+};
+struct Rst7Box {
+  double values[6];      // lengths in angstroms, angles in degrees
+  double velocity_unit;  // nm/ps per angstrom per AMBER time unit
+};
+void launch_traj_shifts(const TrajArgs &t, cudaStream_t stream);
+void launch_traj_image(const TrajArgs &t, double *out, cudaStream_t stream);
+void launch_dcd_pack(const TrajArgs &t, int periodic, cudaStream_t stream);
+void launch_rst7_format(const TrajArgs &t, long long header, int velocities, int box, const Rst7Box &b,
+                        cudaStream_t stream);
+// host forms of the same arithmetic (the header line, the box line)
+int fixed7_text(double x, char field[12]);
+long long rst7_block_size(long long values);
+void dcd_cell_host(const double *box, double cell[6]);
+double script_hypot(double x, double y, double z);
+
 // Line-search state of one system, owned by the device while the minimiser runs: every
 // accept/reject decision is taken by min_decide, so a trial needs no host round trip.
 struct MinState {

@@ -270,8 +270,7 @@ __global__ void __launch_bounds__(32 * NBR_WARPS)
   const int si = valid ? group_order[k] : -1;
   const int i = valid ? sorted_orig[si] : 0;
   const float4 pw = valid ? spos[si] : make_float4(0.f, 0.f, 0.f, 0.f);
-  const float4 po = valid ? posq[i] : make_float4(0.f, 0.f, 0.f, 0.f);
-  if (valid && sub == 0) origin[i] = po;  // displacement origin for the skin check
+  if (valid && sub == 0) origin[i] = posq[i];  // displacement origin for the skin check
   // exclusions of this lane's atom: sorted partners; the range check skips the search
   const int e_lo = valid ? excl_start[i] : 0, e_hi = valid ? excl_start[i + 1] : 0;
   const int p_min = e_lo < e_hi ? excl_partners[e_lo] : INT_MAX;
@@ -363,6 +362,20 @@ __global__ void __launch_bounds__(32 * NBR_WARPS)
                 d2 = fmaf(e, e, d2);
               }
               keep = d2 <= cull2;
+            } else if (rectangular) {
+              // fewer than three cells on an axis: every cell is visited and the image is
+              // chosen per pair, so the cull measures from the nearest image on each axis
+              // (for a rectangular lattice that is the nearest image of the whole box)
+              const float c[3] = {pj.x, pj.y, pj.z};
+              float d2 = 0.f;
+#pragma unroll
+              for (int d = 0; d < 3; ++d) {
+                float x = c[d] - 0.5f * (blo[d] + bhi[d]);
+                x = fmaf(-rintf(x * s.inv_diag[d]), s.box[4 * d], x);
+                const float e = fmaxf(fabsf(x) - 0.5f * (bhi[d] - blo[d]), 0.f);
+                d2 = fmaf(e, e, d2);
+              }
+              keep = d2 <= cull2;
             }
           }
           const unsigned mask = __ballot_sync(0xffffffffu, keep);
@@ -394,8 +407,8 @@ __global__ void __launch_bounds__(32 * NBR_WARPS)
               }
               const float r2 = fmaf(d.x, d.x, fmaf(d.y, d.y, d.z * d.z));
               in = r2 <= band_hi && gj != si;
-              if (in && r2 >= band_lo) {
-                const float4 qj = posq[j];
+              if (in && r2 >= band_lo) {  // rare: reload both original positions
+                const float4 po = posq[i], qj = posq[j];
                 const float3 d0 = make_float3(__fsub_rn(po.x, qj.x), __fsub_rn(po.y, qj.y), __fsub_rn(po.z, qj.z));
                 in = !(dot_exact(min_image_exact(d0, s)) > lc2);
               }

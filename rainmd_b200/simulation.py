@@ -182,6 +182,7 @@ class BatchSimulation:
             raise _ERRORS.get(status, RainMDError)(self._lib.rmd_last_error(None).decode())
         self._h = handle
         self.step = 0
+        self.timestep = float(ostructs[0].timestep)  # ps, for the restart's time
 
     # -- plumbing --
     def _check(self, status):
