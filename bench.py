@@ -256,6 +256,37 @@ def trajectory_study(frames: int = 50, seed: int = 2):
     return out
 
 
+def render_study(frames: int = 20, seed: int = 2):
+    """The headless viewer (csrc/raster.cu): a 1920x1080 frame of every atom of the
+    23,558-atom box as sphere impostors, through the public API (styles and camera in, the
+    RGBA image out), next to the CPU restatement of the same frame."""
+    import oracle
+    from rainmd_b200.simulation import GpuSimulation
+    from rainmd_b200.viewer import StructureViewer
+
+    system, pos, grid = workload("water-23558", seed)
+    t = system["topology"]
+    t = dict(t)
+    t.setdefault("atomicNumbers", [8 if m > 10 else 1 for m in t["masses"]])
+    sim = GpuSimulation(system, options_for(grid, seed))
+    sim.setState(pos)
+    viewer = StructureViewer(1920, 1080)
+    viewer.setStructure(t, positions=pos)
+    viewer.draw(sim)
+    t0 = time.perf_counter()
+    for _ in range(frames):
+        image = viewer.draw(sim)
+    ms = (time.perf_counter() - t0) * 1e3 / frames
+    t0 = time.perf_counter()
+    expected = oracle.render(sim.readState()["positions"], viewer.camera(), viewer.styles, width=1920,
+                             height=1080)
+    cpu_ms = (time.perf_counter() - t0) * 1e3
+    return {"study": "render", "atoms": t["atomCount"], "width": 1920, "height": 1080,
+            "ms_per_frame": ms, "frames_per_s": 1e3 / ms, "cpu_oracle_ms_per_frame": cpu_ms,
+            "identical_to_oracle": bool(np.array_equal(image, expected)),
+            "covered_pixels": int((image[..., :3] != image[0, 0, :3]).any(-1).sum())}
+
+
 def large_combined_study(steps: int, seed: int = 5):
     """250,000 atoms (a 4,000-atom chain in TIP3P water, PME order 4 on 128^3) advanced in one
     batch with 16 solvated systems of 5,000-20,000 atoms, all NPT at 1 bar with the learned
@@ -488,7 +519,8 @@ def main():
     parser.add_argument("--minimise", type=int, default=200, help="minimiser iterations before dynamics")
     parser.add_argument("--equilibrate", type=int, default=3000, help="untimed steps before warm-up")
     parser.add_argument("--no-batched", action="store_true", help="skip the 64-system batch measurement")
-    parser.add_argument("--study", choices=["learned-barostat", "large-combined", "trajectory"], default=None,
+    parser.add_argument("--study", choices=["learned-barostat", "large-combined", "trajectory", "render"],
+                        default=None,
                         help="run a study instead of the benchmark and print its JSON line")
     parser.add_argument("--ps", type=float, default=500.0, help="length of a study run")
     parser.add_argument("--batch-steps", type=int, default=500)
@@ -514,6 +546,10 @@ def main():
     if args.study == "trajectory":
         if rank == 0:
             print(json.dumps(trajectory_study()), flush=True)
+        return
+    if args.study == "render":
+        if rank == 0:
+            print(json.dumps(render_study()), flush=True)
         return
     # one GPU per process: make this rank's GPU device 0 before any CUDA initialisation
     if world > 1:

@@ -373,6 +373,31 @@ rmd_status rmd_dcd_header(int32_t atom_count, int32_t frames, int32_t first_step
 rmd_status rmd_restart_at(rmd_sim *sim, int32_t system_index, const char *title, double time,
                           int32_t velocities, int32_t box, char *out, int64_t capacity, int64_t *bytes);
 
+/* ---- Headless structure rendering (web/viewer.js): the viewer's sphere-impostor pass
+ * (viewer.js:230-308) and cartoon-ribbon pass (viewer.js:83-228) drawn by CUDA into an RGBA8
+ * image, row 0 at the top, with no window, swapchain or graphics API. */
+
+/* The viewer's camera uniform (viewer.js:683-692): view-projection (column-major), the
+ * camera's right, up and forward vectors, and the centre the scene is drawn about. */
+typedef struct {
+  float view_projection[16];
+  float right[4], up[4], forward[4], centre[4];
+} rmd_camera;
+
+/* StructureViewer.draw() over the system's own device positions: `styles` holds four floats
+ * an atom (colour rgb, radius in nm; 0 hides the atom, viewer.js:440-462), `guides` twelve a
+ * guide and `segments` four guide indices a segment as buildRibbon returns them
+ * (shared/analysis/ribbon.js:110-231). `rgba` receives width * height * 4 bytes. */
+rmd_status rmd_render_at(rmd_sim *sim, int32_t system_index, const rmd_camera *camera, const float *styles,
+                         const float *guides, int32_t guide_count, const uint32_t *segments,
+                         int32_t segment_count, int32_t draw_spheres, int32_t draw_ribbon, int32_t width,
+                         int32_t height, uint8_t *rgba);
+/* The same from host coordinates (3 floats an atom, nm): StructureViewer.upload() + draw(). */
+rmd_status rmd_render_positions(const float *positions, int32_t atom_count, const rmd_camera *camera,
+                                const float *styles, const float *guides, int32_t guide_count,
+                                const uint32_t *segments, int32_t segment_count, int32_t draw_spheres,
+                                int32_t draw_ribbon, int32_t width, int32_t height, uint8_t *rgba);
+
 /* Allocation-free PME charge spreading, for callers that cannot call cudaMalloc: code
  * recording into its own CUDA graph during stream capture, hosts whose device memory all
  * comes from their own arena, and latency-bound callers that cannot take cudaMalloc's

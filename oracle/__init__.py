@@ -19,6 +19,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "liboracle.so")
 SOURCE = os.path.join(HERE, "rmd_oracle.c")
+SOURCES = [SOURCE, os.path.join(HERE, "raster.c")]
 
 _i = C.POINTER(C.c_int)
 _d = C.POINTER(C.c_double)
@@ -50,10 +51,11 @@ class OrcIntegrator(C.Structure):
 
 def build(force: bool = False) -> str:
     """Compile liboracle.so with gcc (OpenMP, no floating-point contraction)."""
-    if not force and os.path.exists(LIB_PATH) and os.path.getmtime(LIB_PATH) >= os.path.getmtime(SOURCE):
+    if not force and os.path.exists(LIB_PATH) and all(
+            os.path.getmtime(LIB_PATH) >= os.path.getmtime(s) for s in SOURCES):
         return LIB_PATH
     cmd = ["gcc", "-O2", "-fopenmp", "-ffp-contract=off", "-fno-fast-math", "-shared", "-fPIC",
-           "-o", LIB_PATH, SOURCE, "-lm"]
+           "-o", LIB_PATH, *SOURCES, "-lm"]
     subprocess.run(cmd, check=True)
     return LIB_PATH
 
@@ -68,7 +70,34 @@ def lib():
             build()
         _lib = C.CDLL(LIB_PATH)
         _bind(_lib)
+        _bind_render(_lib)
     return _lib
+
+
+def _bind_render(L):
+    f = C.POINTER(C.c_float)
+    L.orc_render.argtypes = [f, C.c_int, f, f, f, C.c_int, C.POINTER(C.c_uint), C.c_int, C.c_int, C.c_int,
+                             C.c_int, C.c_int, C.POINTER(C.c_ubyte)]
+    L.orc_render.restype = None
+
+
+def render(positions, camera, styles, guides=None, segments=None, spheres=True, ribbon=True,
+           width=64, height=48):
+    """The renderer's oracle (raster.c): an RGBA8 image [height, width, 4]."""
+    L = lib()
+    f = C.POINTER(C.c_float)
+    pos = np.ascontiguousarray(positions, dtype=np.float32).reshape(-1)
+    cam = np.ascontiguousarray(camera, dtype=np.float32).reshape(-1)
+    sty = np.ascontiguousarray(styles if styles is not None else np.zeros(4), dtype=np.float32).reshape(-1)
+    gui = np.ascontiguousarray(guides if guides is not None else np.zeros(12), dtype=np.float32).reshape(-1)
+    seg = np.ascontiguousarray(segments if segments is not None else np.zeros(4), dtype=np.uint32).reshape(-1)
+    nseg = 0 if segments is None else len(seg) // 4
+    out = np.zeros((height, width, 4), np.uint8)
+    L.orc_render(pos.ctypes.data_as(f), len(pos) // 3, cam.ctypes.data_as(f), sty.ctypes.data_as(f),
+                 gui.ctypes.data_as(f), len(gui) // 12, seg.ctypes.data_as(C.POINTER(C.c_uint)), nseg,
+                 1 if spheres else 0, 1 if ribbon else 0, width, height,
+                 out.ctypes.data_as(C.POINTER(C.c_ubyte)))
+    return out
 
 
 def _bind(L):

@@ -131,7 +131,7 @@ EXPORTS = [
     "rmd_bench_run", "rmd_debug_force_term", "rmd_debug_read", "rmd_spread_charges_noalloc",
     "rmd_kernel_shapes", "rmd_set_kernel_shapes", "rmd_surrogate_report_at", "rmd_surrogate_weights",
     "rmd_surrogate_evaluate", "rmd_image_molecules_at", "rmd_dcd_frame_bytes", "rmd_dcd_frame_at",
-    "rmd_dcd_header", "rmd_restart_at",
+    "rmd_dcd_header", "rmd_restart_at", "rmd_render_at", "rmd_render_positions",
 ]
 
 _lib = None
@@ -206,6 +206,10 @@ def load():
                                    C.c_char_p, C.c_char_p, C.c_void_p]
     lib.rmd_restart_at.argtypes = [sim, C.c_int32, C.c_char_p, C.c_double, C.c_int32, C.c_int32, C.c_void_p,
                                    C.c_int64, C.POINTER(C.c_int64)]
+    render_args = [C.c_void_p, _fp, _fp, C.c_int32, C.POINTER(C.c_uint32), C.c_int32, C.c_int32, C.c_int32,
+                   C.c_int32, C.c_int32, C.POINTER(C.c_uint8)]
+    lib.rmd_render_at.argtypes = [sim, C.c_int32, *render_args]
+    lib.rmd_render_positions.argtypes = [_fp, C.c_int32, *render_args]
     for name in EXPORTS:
         fn = getattr(lib, name)
         if fn.restype is C.c_int and name not in ("rmd_system_count",):

@@ -27,11 +27,33 @@ def stale() -> bool:
     return any(os.path.getmtime(p) > built for p in SOURCES + HEADERS)
 
 
+# Sources whose floating-point results must not depend on the compiler's choice of fused
+# multiply-adds (the renderer: its image is compared bit for bit with a CPU restatement).
+UNFUSED = {"raster.cu"}
+OBJ_DIR = os.path.join(os.path.dirname(HERE), "_build")
+
+
 def build(force: bool = False, verbose: bool = False) -> str:
     if not force and not stale():
         return LIB
     extra = ["-Xptxas", "-v"] if verbose else []
-    cmd = [NVCC, *FLAGS, *extra, "-o", LIB, *SOURCES]
+    fused = [s for s in SOURCES if os.path.basename(s) not in UNFUSED]
+    objects = []
+    os.makedirs(OBJ_DIR, exist_ok=True)
+    for src in SOURCES:
+        if os.path.basename(src) not in UNFUSED:
+            continue
+        obj = os.path.join(OBJ_DIR, os.path.basename(src) + ".o")
+        flags = [f for f in FLAGS if f != "-shared"]
+        cmd = [NVCC, *flags, *extra, "-fmad=false", "-c", "-o", obj, src]
+        result = subprocess.run(cmd, capture_output=True, text=True)
+        if result.returncode != 0:
+            sys.stderr.write(result.stdout + result.stderr)
+            raise RuntimeError(f"nvcc failed to compile {os.path.basename(src)}")
+        if verbose:
+            sys.stderr.write(result.stderr)
+        objects.append(obj)
+    cmd = [NVCC, *FLAGS, *extra, "-o", LIB, *fused, *objects]
     result = subprocess.run(cmd, capture_output=True, text=True)
     if result.returncode != 0:
         sys.stderr.write(result.stdout + result.stderr)

@@ -2787,3 +2787,106 @@ rmd_status rmd_restart_at(rmd_sim *sim, int32_t s, const char *title, double tim
     CUDA_OK(cudaMemcpy(out, e.traj_out.p, (size_t)total, cudaMemcpyDeviceToHost));
   });
 }
+
+// ----------------------------------------------------------------- headless rendering
+namespace {
+// Every check a frame's inputs get before anything reaches the device.
+void validate_render(bool have_positions, int32_t atom_count, const rmd_camera *camera, const float *styles,
+                     const float *guides, int32_t guide_count, const uint32_t *segments, int32_t segment_count,
+                     int32_t draw_spheres, int32_t draw_ribbon, int32_t width, int32_t height, const uint8_t *rgba) {
+  if (!camera || !rgba || width <= 0 || height <= 0 || width > 16384 || height > 16384 || atom_count < 0)
+    throw rmd::Error(RMD_ERR_INVALID, "a frame needs a camera, an output image and a size of 1-16384 pixels a side");
+  if (draw_spheres && atom_count > 0 && !styles)
+    throw rmd::Error(RMD_ERR_INVALID, "drawing spheres needs a style (colour, radius) per atom");
+  if (draw_ribbon && segment_count > 0) {
+    if (!guides || !segments || guide_count <= 0)
+      throw rmd::Error(RMD_ERR_INVALID, "drawing the ribbon needs its guides and segments");
+    for (long long k = 0; k < 4ll * segment_count; ++k)
+      if (segments[k] >= (uint32_t)guide_count)
+        throw rmd::Error(RMD_ERR_INVALID, "a ribbon segment names guide " + std::to_string(segments[k]) +
+                                              " of " + std::to_string(guide_count));
+  }
+  if (draw_spheres && atom_count > 0 && !have_positions)
+    throw rmd::Error(RMD_ERR_INVALID, "drawing spheres needs positions");
+}
+
+rmd_status render_frame(const float4 *positions, int32_t atom_count, const rmd_camera *camera,
+                        const float *styles, const float *guides, int32_t guide_count, const uint32_t *segments,
+                        int32_t segment_count, int32_t draw_spheres, int32_t draw_ribbon, int32_t width,
+                        int32_t height, uint8_t *rgba, cudaStream_t stream) {
+  rmd::RenderArgs a{};
+  static_assert(sizeof(rmd::RenderCamera) == sizeof(rmd_camera), "the camera uniform is 36 floats");
+  memcpy(&a.camera, camera, sizeof a.camera);
+  a.atom_count = draw_spheres ? atom_count : 0;
+  a.segment_count = draw_ribbon ? segment_count : 0;
+  a.draw_spheres = draw_spheres && atom_count > 0 ? 1 : 0;
+  a.draw_ribbon = draw_ribbon && segment_count > 0 ? 1 : 0;
+  a.width = width;
+  a.height = height;
+  a.positions = positions;
+  rmd::DevArray<float4> d_styles, corners;
+  rmd::DevArray<float> d_guides, verts;
+  rmd::DevArray<uint4> d_segments;
+  rmd::DevArray<unsigned long long> keys;
+  rmd::DevArray<uchar4> image;
+  if (a.draw_spheres) {
+    d_styles.alloc(atom_count);
+    CUDA_OK(cudaMemcpyAsync(d_styles.p, styles, sizeof(float4) * atom_count, cudaMemcpyHostToDevice, stream));
+    corners.alloc(4 * (size_t)atom_count);
+    a.styles = d_styles.p;
+    a.sphere_corners = corners.p;
+  }
+  if (a.draw_ribbon) {
+    d_guides.alloc(12 * (size_t)guide_count);
+    CUDA_OK(cudaMemcpyAsync(d_guides.p, guides, sizeof(float) * 12 * guide_count, cudaMemcpyHostToDevice, stream));
+    d_segments.alloc(segment_count);
+    CUDA_OK(cudaMemcpyAsync(d_segments.p, segments, sizeof(uint4) * segment_count, cudaMemcpyHostToDevice, stream));
+    verts.alloc(12 * 24 * 8 * (size_t)segment_count);
+    a.guides = d_guides.p;
+    a.segments = d_segments.p;
+    a.ribbon_vertices = verts.p;
+  }
+  keys.alloc((size_t)width * height);
+  image.alloc((size_t)width * height);
+  a.keys = keys.p;
+  a.image = image.p;
+  rmd::launch_render(a, stream);
+  CUDA_OK(cudaGetLastError());
+  CUDA_OK(cudaMemcpyAsync(rgba, image.p, sizeof(uchar4) * (size_t)width * height, cudaMemcpyDeviceToHost, stream));
+  CUDA_OK(cudaStreamSynchronize(stream));
+  return RMD_OK;
+}
+}  // namespace
+
+rmd_status rmd_render_at(rmd_sim *sim, int32_t s, const rmd_camera *camera, const float *styles,
+                         const float *guides, int32_t guide_count, const uint32_t *segments, int32_t segment_count,
+                         int32_t draw_spheres, int32_t draw_ribbon, int32_t width, int32_t height, uint8_t *rgba) {
+  if (rmd_status c = check_index(sim, s)) return c;
+  return guarded(sim, [&]() {
+    auto &e = sim->engine;
+    const auto &h = e.hs[s];
+    validate_render(true, h.n, camera, styles, guides, guide_count, segments, segment_count, draw_spheres,
+                    draw_ribbon, width, height, rgba);
+    render_frame(e.posq.p + h.atom_start, h.n, camera, styles, guides, guide_count, segments, segment_count,
+                 draw_spheres, draw_ribbon, width, height, rgba, e.stream);
+  });
+}
+
+rmd_status rmd_render_positions(const float *positions, int32_t atom_count, const rmd_camera *camera,
+                                const float *styles, const float *guides, int32_t guide_count,
+                                const uint32_t *segments, int32_t segment_count, int32_t draw_spheres,
+                                int32_t draw_ribbon, int32_t width, int32_t height, uint8_t *rgba) {
+  return guarded(nullptr, [&]() {
+    validate_render(positions != nullptr, atom_count, camera, styles, guides, guide_count, segments,
+                    segment_count, draw_spheres, draw_ribbon, width, height, rgba);
+    rmd::DevArray<float4> p;
+    if (atom_count > 0 && positions) {
+      std::vector<float4> host(atom_count);
+      for (int i = 0; i < atom_count; ++i)
+        host[i] = make_float4(positions[3 * i], positions[3 * i + 1], positions[3 * i + 2], 0.0f);
+      p.upload(host);
+    }
+    render_frame(p.p, atom_count, camera, styles, guides, guide_count, segments, segment_count,
+                 draw_spheres, draw_ribbon, width, height, rgba, cudaStreamLegacy);
+  });
+}

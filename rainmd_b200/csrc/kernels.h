@@ -278,6 +278,28 @@ long long rst7_block_size(long long values);
 void dcd_cell_host(const double *box, double cell[6]);
 double script_hypot(double x, double y, double z);
 
+// Headless structure rendering (raster.cu): the viewer's 36-float camera uniform, and one
+// frame's inputs, scratch and output.
+struct RenderCamera {
+  float vp[16];  // view-projection, column-major
+  float right[4], up[4], forward[4], centre[4];
+};
+struct RenderArgs {
+  RenderCamera camera;
+  const float4 *positions;  // xyz in nm (w unused)
+  const float4 *styles;     // colour rgb, radius (0 hides the atom)
+  int atom_count;
+  const float *guides;      // 12 floats a guide: position, half width, side, half thickness, colour, pad
+  const uint4 *segments;    // four control guides a segment
+  int segment_count;
+  int draw_spheres, draw_ribbon, width, height;
+  float4 *sphere_corners;   // 4 per atom
+  float *ribbon_vertices;   // 12 floats per vertex, 24 * 8 vertices per segment
+  unsigned long long *keys; // per pixel: depth bits << 32 | primitive order
+  uchar4 *image;            // RGBA8, row 0 at the top
+};
+void launch_render(const RenderArgs &a, cudaStream_t stream);
+
 // Line-search state of one system, owned by the device while the minimiser runs: every
 // accept/reject decision is taken by min_decide, so a trial needs no host round trip.
 struct MinState {
