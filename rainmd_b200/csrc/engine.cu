@@ -885,6 +885,23 @@ void Engine::upload_all(const std::vector<const rmd_system *> &src) {
     std::vector<FftPlan> h_plans(S);
     std::vector<FftTask> tz, ty, tx;
     task_x_start.assign(S + 1, 0);
+    // Lines per block. The z and y passes (no sums across lines) are sized from the whole
+    // batch's line count: as many lines as fit the shared buffers and about 2 elements per
+    // thread, but few enough that a pass has at least ~4 blocks per SM (592 on 148 SMs), so 64
+    // small grids fill blocks as one large grid does. The x pass also sums the reciprocal
+    // energy per block, so its size depends on the line length alone: a system's energy
+    // partials are grouped the same way in a batch as alone, and come out bit for bit equal.
+    long long all_pairs = 0, all_ylines = 0;
+    for (int s = 0; s < S; ++s) {
+      all_pairs += ((long long)hs[s].grid[0] * hs[s].grid[1] + 1) / 2;
+      all_ylines += (long long)hs[s].grid[0] * (hs[s].grid[2] / 2 + 1);
+    }
+    auto lines_per_block = [](long long total_lines, int n, int cap) {
+      int m = std::max(1, std::min(cap, FFT_SMEM_HOST / n));
+      m = (int)std::min<long long>(m, std::max(1LL, (long long)std::ceil(total_lines / 592.0)));
+      m = std::min(m, std::max(1, 512 / n));
+      return m;
+    };
     for (int s = 0; s < S; ++s) {
       HostSystem &h = hs[s];
       DevSys &d = h_sys[s];
@@ -903,23 +920,15 @@ void Engine::upload_all(const std::vector<const rmd_system *> &src) {
           h_tw.push_back(make_float2((float)std::cos(a), (float)std::sin(a)));
         }
       }
-      // Lines per block: as many as fit the shared buffers, but few enough that a pass has
-      // at least ~4 blocks per SM (592 on 148 SMs) and about 2 elements per thread.
-      auto lines_per_block = [](int total_lines, int n, int cap) {
-        int m = std::max(1, std::min(cap, FFT_SMEM_HOST / n));
-        m = std::min(m, std::max(1, (int)std::ceil(total_lines / 592.0)));
-        m = std::min(m, std::max(1, 512 / n));
-        return m;
-      };
       // z pass: pairs of real lines
       const int lines = nx * ny, pairs = (lines + 1) / 2;
-      const int mz = lines_per_block(pairs, nz, 64);
+      const int mz = lines_per_block(all_pairs, nz, 64);
       for (int p = 0; p < pairs; p += mz) tz.push_back(FftTask{s, 0, p, std::min(mz, pairs - p)});
-      const int my = lines_per_block(nx * nzh, ny + 1, nzh);  // y and x lines are padded to n + 1
+      const int my = lines_per_block(all_ylines, ny + 1, nzh);  // y and x lines are padded to n + 1
       for (int x = 0; x < nx; ++x)
         for (int k = 0; k < nzh; k += my) ty.push_back(FftTask{s, x, k, std::min(my, nzh - k)});
       task_x_start[s] = (int)tx.size();
-      const int mx = lines_per_block(ny * nzh, nx + 1, nzh);
+      const int mx = std::max(1, std::min(nzh, std::min(FFT_SMEM_HOST / (nx + 1), 512 / (nx + 1))));
       for (int y = 0; y < ny; ++y)
         for (int k = 0; k < nzh; k += mx) tx.push_back(FftTask{s, y, k, std::min(mx, nzh - k)});
     }
