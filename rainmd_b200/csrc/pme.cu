@@ -74,7 +74,7 @@ __device__ __forceinline__ void dft_small(float2 *v, bool inv) {
 
 template <int R>
 __device__ __forceinline__ void stockham_stage(const float2 *__restrict__ in, float2 *__restrict__ out,
-                                               int lines, int N, int ld, int Ns, const float2 *__restrict__ tw,
+                                               int lines, int N, int ld, int Ns, const float2 *tw,
                                                bool inv) {
   const int per_line = N / R;
   const int stride_tw = N / (Ns * R);
@@ -102,7 +102,16 @@ __device__ __forceinline__ void stockham_stage(const float2 *__restrict__ in, fl
 // lines filled by a transpose use ld = N + 1 so that the transposing accesses, which step
 // by ld, fall in different shared-memory banks); returns the buffer holding the result.
 __device__ float2 *fft_lines(float2 *a, float2 *b, int lines, int N, int ld, const FftAxis &ax,
-                             const float2 *__restrict__ tw, bool inv) {
+                             const float2 *tw, bool inv) {
+  // the axis's twiddles in shared memory, so the stages read them without a global round
+  // trip after each barrier (tables longer than the cache stay in global memory)
+  constexpr int TW_CACHE = 512;
+  __shared__ float2 tw_cache[TW_CACHE];
+  if (N <= TW_CACHE) {
+    __syncthreads();  // a previous transform in this block has finished with the cache
+    for (int k = threadIdx.x; k < N; k += blockDim.x) tw_cache[k] = tw[k];
+    tw = tw_cache;    // visible after the barrier that opens the first stage
+  }
   int Ns = 1;
   for (int st = 0; st < ax.nstages; ++st) {
     const int R = ax.radix[st];
@@ -184,15 +193,13 @@ __global__ void __launch_bounds__(256) k_fft_z_r2c(const FftTask *__restrict__ t
     const int p = idx / N, k = idx - p * N;
     const int l = 2 * (t.first + p);
     unsigned long long *ra = g + (long long)l * N + k;
-    float re = from_fixed(*ra);
-    *ra = 0ull;
-    float im = 0.f;
-    if (l + 1 < nlines) {
-      unsigned long long *rb = ra + N;
-      im = from_fixed(*rb);
-      *rb = 0ull;
-    }
-    bufa[idx] = make_float2(re, im);
+    const bool two = l + 1 < nlines;
+    // both values read before either is cleared for the next step's spreading
+    const unsigned long long va = ra[0];
+    const unsigned long long vb = two ? ra[N] : 0ull;
+    ra[0] = 0ull;
+    if (two) ra[N] = 0ull;
+    bufa[idx] = make_float2(from_fixed(va), two ? from_fixed(vb) : 0.f);
   }
   float2 *r = fft_lines(bufa, bufb, M, N, N, pl.axis[2], twiddles + pl.axis[2].tw_base, false);
   float2 *h = half + s.half_base;
