@@ -216,8 +216,10 @@ struct Engine {
   DevArray<float2> half, twiddles;
   DevArray<float> real_grid, moduli;
   DevArray<FftPlan> fft_plans;
-  DevArray<FftTask> tasks_z, tasks_y, tasks_x;
-  std::vector<int> task_x_start;  // per system range of x tasks
+  DevArray<FftTask> tasks_z, tasks_y, tasks_x, tasks_plane, tasks_y_all, tasks_x_all;
+  std::vector<int> task_x_start;  // per system range of x tasks (systems on the separate passes)
+  std::vector<int> plane_start;   // per system range of kz-plane tasks (systems on the fused pass)
+  int plane_stride = 0;
   DevArray<DevSys> sys;
   DevArray<DevSysD> sysd;
   std::vector<DevSys> h_sys;
@@ -883,8 +885,10 @@ void Engine::upload_all(const std::vector<const rmd_system *> &src) {
     std::vector<float> h_mod;
     std::vector<float2> h_tw;
     std::vector<FftPlan> h_plans(S);
-    std::vector<FftTask> tz, ty, tx;
+    std::vector<FftTask> tz, ty, tx, tp, ty_all, tx_all;
     task_x_start.assign(S + 1, 0);
+    plane_start.assign(S + 1, 0);
+    plane_stride = 0;
     // Lines per block. The z and y passes (no sums across lines) are sized from the whole
     // batch's line count: as many lines as fit the shared buffers and about 2 elements per
     // thread, but few enough that a pass has at least ~4 blocks per SM (592 on 148 SMs), so 64
@@ -924,15 +928,32 @@ void Engine::upload_all(const std::vector<const rmd_system *> &src) {
       const int lines = nx * ny, pairs = (lines + 1) / 2;
       const int mz = lines_per_block(all_pairs, nz, 64);
       for (int p = 0; p < pairs; p += mz) tz.push_back(FftTask{s, 0, p, std::min(mz, pairs - p)});
+      // A system whose kz plane fits shared memory runs the fused y-x-convolve-x-y pass, one
+      // block a plane; the others run the separate y and x passes. The debug transforms run
+      // the separate passes over every system.
+      const bool fused = fft_plane_smem_bytes(nx, ny) > 0;
       const int my = lines_per_block(all_ylines, ny + 1, nzh);  // y and x lines are padded to n + 1
-      for (int x = 0; x < nx; ++x)
-        for (int k = 0; k < nzh; k += my) ty.push_back(FftTask{s, x, k, std::min(my, nzh - k)});
-      task_x_start[s] = (int)tx.size();
       const int mx = std::max(1, std::min(nzh, std::min(FFT_SMEM_HOST / (nx + 1), 512 / (nx + 1))));
+      for (int x = 0; x < nx; ++x)
+        for (int k = 0; k < nzh; k += my) {
+          ty_all.push_back(FftTask{s, x, k, std::min(my, nzh - k)});
+          if (!fused) ty.push_back(ty_all.back());
+        }
+      task_x_start[s] = (int)tx.size();
+      plane_start[s] = (int)tp.size();
       for (int y = 0; y < ny; ++y)
-        for (int k = 0; k < nzh; k += mx) tx.push_back(FftTask{s, y, k, std::min(mx, nzh - k)});
+        for (int k = 0; k < nzh; k += mx) {
+          tx_all.push_back(FftTask{s, y, k, std::min(mx, nzh - k)});
+          if (!fused) tx.push_back(tx_all.back());
+        }
+      if (fused) {
+        for (int kz = 0; kz < nzh; ++kz) tp.push_back(FftTask{s, kz, 0, 0});
+        plane_stride = std::max(plane_stride, std::max(nx * (ny + 1), ny * (nx + 1)));
+      }
     }
     task_x_start[S] = (int)tx.size();
+    plane_start[S] = (int)tp.size();
+    if (!tp.empty()) CUDA_OK(fft_plane_prepare());
     fixed_grid.alloc(gbase);
     fixed_grid.zero();
     half.alloc(hbase);
@@ -944,9 +965,14 @@ void Engine::upload_all(const std::vector<const rmd_system *> &src) {
     tasks_z.upload(tz);
     tasks_y.upload(ty);
     tasks_x.upload(tx);
-    e_pme.alloc(tx.size());
+    tasks_plane.upload(tp);
+    tasks_y_all.upload(ty_all);
+    tasks_x_all.upload(tx_all);
+    // energy partials: the x tasks' first, then the planes'
+    const size_t partials = std::max<size_t>(1, tx.size() + tp.size());
+    e_pme.alloc(partials);
     e_pme.zero();
-    e_pme_vir.alloc(tx.size());
+    e_pme_vir.alloc(partials);
     e_pme_vir.zero();
   }
 
@@ -1035,6 +1061,15 @@ void Engine::upload_all(const std::vector<const rmd_system *> &src) {
   // ---- energy segments
   {
     std::vector<Segment> seg;
+    // a system's reciprocal partials: its x tasks' on the separate passes, else its planes'
+    // (stored after every x task's)
+    const long long n_tx = (long long)tasks_x.n;
+    auto recip_begin = [&](int s) {
+      return plane_start[s + 1] > plane_start[s] ? n_tx + plane_start[s] : (long long)task_x_start[s];
+    };
+    auto recip_end = [&](int s) {
+      return plane_start[s + 1] > plane_start[s] ? n_tx + plane_start[s + 1] : (long long)task_x_start[s + 1];
+    };
     for (int s = 0; s < S; ++s) {
       const HostSystem &h = hs[s];
       const long long a0 = h.atom_start, a1 = h.atom_start + h.n;
@@ -1046,7 +1081,7 @@ void Engine::upload_all(const std::vector<const rmd_system *> &src) {
                             n_bonds + n_angles + n_tors + rstart[s + 1], nullptr});
       seg.push_back(Segment{s, E_LJ, e_lj.p, a0, a1, nullptr});
       seg.push_back(Segment{s, E_COUL_DIRECT, e_coul.p, a0, a1, nullptr});
-      seg.push_back(Segment{s, E_RECIP, e_pme.p, task_x_start[s], task_x_start[s + 1], nullptr});
+      seg.push_back(Segment{s, E_RECIP, e_pme.p, recip_begin(s), recip_end(s), nullptr});
       seg.push_back(Segment{s, E_VIR_SR, e_vir.p, a0, a1, nullptr});
       seg.push_back(Segment{s, E_VIR_SR, e_term_vir.p, bstart[s], bstart[s + 1], nullptr});
       seg.push_back(Segment{s, E_VIR_SR, e_term_vir.p, n_bonds + astart[s], n_bonds + astart[s + 1], nullptr});
@@ -1055,7 +1090,7 @@ void Engine::upload_all(const std::vector<const rmd_system *> &src) {
       seg.push_back(Segment{s, E_VIR_SR, e_term_vir.p, n_bonds + n_angles + n_tors + rstart[s],
                             n_bonds + n_angles + n_tors + rstart[s + 1], nullptr});
       seg.push_back(Segment{s, E_VIR_MOL, mol_vir.p, mol_base[s], mol_base[s + 1], nullptr});
-      seg.push_back(Segment{s, E_VIR_REC, e_pme_vir.p, task_x_start[s], task_x_start[s + 1], nullptr});
+      seg.push_back(Segment{s, E_VIR_REC, e_pme_vir.p, recip_begin(s), recip_end(s), nullptr});
       seg.push_back(Segment{s, E_KINETIC, ke_post.p, a0, a1, nullptr});
       seg.push_back(Segment{s, E_KINETIC_EARLY, ke_early.p, a0, a1, nullptr});
     }
@@ -1161,6 +1196,13 @@ LaunchCtx Engine::ctx() const {
   c.tasks_z = tasks_z.p;
   c.tasks_y = tasks_y.p;
   c.tasks_x = tasks_x.p;
+  c.tasks_plane = tasks_plane.p;
+  c.tasks_y_all = tasks_y_all.p;
+  c.tasks_x_all = tasks_x_all.p;
+  c.n_tasks_plane = (int)tasks_plane.n;
+  c.n_tasks_y_all = (int)tasks_y_all.n;
+  c.n_tasks_x_all = (int)tasks_x_all.n;
+  c.plane_stride = plane_stride;
   c.n_tasks_z = (int)tasks_z.n;
   c.n_tasks_y = (int)tasks_y.n;
   c.n_tasks_x = (int)tasks_x.n;

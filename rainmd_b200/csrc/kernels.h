@@ -135,8 +135,12 @@ struct LaunchCtx {
   const float *moduli;
   const float2 *twiddles;
   const FftPlan *fft_plans;
-  const FftTask *tasks_z, *tasks_y, *tasks_x;
-  int n_tasks_z, n_tasks_y, n_tasks_x;
+  // z tasks cover every system; y and x tasks the systems whose kz planes do not fit the fused
+  // plane kernel, whose plane tasks (one per kz plane) come last; *_all cover every system (the
+  // debug transforms)
+  const FftTask *tasks_z, *tasks_y, *tasks_x, *tasks_plane, *tasks_y_all, *tasks_x_all;
+  int n_tasks_z, n_tasks_y, n_tasks_x, n_tasks_plane, n_tasks_y_all, n_tasks_x_all;
+  int plane_stride;  // complex values per plane buffer (the largest plane among the fused systems)
   double *e_pme, *e_pme_vir;
 };
 
@@ -158,6 +162,10 @@ void launch_pme(const LaunchCtx &c, bool energy, cudaStream_t stream);
 void launch_pme_grid(const LaunchCtx &c, bool energy, cudaStream_t stream);
 void launch_pme_gather(const LaunchCtx &c, cudaStream_t stream);
 int pme_launches(const LaunchCtx &c);  // kernels launch_pme issues
+// dynamic shared memory of the fused plane pass for an nx x ny plane, 0 when it does not fit
+constexpr long long FFT_PLANE_SMEM_MAX = 200 * 1024;
+long long fft_plane_smem_bytes(int nx, int ny);
+cudaError_t fft_plane_prepare();
 void launch_fft_forward(const LaunchCtx &c, cudaStream_t stream);
 void launch_spread_only(const LaunchCtx &c, cudaStream_t stream);
 void launch_fft_inverse(const LaunchCtx &c, cudaStream_t stream);

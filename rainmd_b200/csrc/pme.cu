@@ -19,6 +19,8 @@
 // The FFT is a mixed-radix (4, 2, 3, 5) Stockham autosort over lines held in shared
 // memory; a host-built task table gives each block a set of lines of one system, so
 // systems with different grid sizes run in the same launch.
+#include <algorithm>
+
 #include "common.cuh"
 #include "kernels.h"
 
@@ -499,33 +501,186 @@ static void launch_gather(const LaunchCtx &c, cudaStream_t stream) {
 }
 
 // Forward transform of the spread grid to the half spectrum (z and y; x is left to the caller).
-static void launch_forward_zy(const LaunchCtx &c, cudaStream_t stream) {
+static void launch_forward_zy(const LaunchCtx &c, cudaStream_t stream, bool all = false) {
   k_fft_z_r2c<<<c.n_tasks_z, 256, 0, stream>>>(c.tasks_z, c.sys, c.fft_plans, c.twiddles, c.fixed_grid, c.half);
-  k_fft_y<<<c.n_tasks_y, 256, 0, stream>>>(c.tasks_y, c.sys, c.fft_plans, c.twiddles, c.half, 0);
+  const FftTask *ty = all ? c.tasks_y_all : c.tasks_y;
+  const int n = all ? c.n_tasks_y_all : c.n_tasks_y;
+  if (n > 0) k_fft_y<<<n, 256, 0, stream>>>(ty, c.sys, c.fft_plans, c.twiddles, c.half, 0);
 }
 
-static void launch_inverse_yz(const LaunchCtx &c, cudaStream_t stream) {
-  k_fft_y<<<c.n_tasks_y, 256, 0, stream>>>(c.tasks_y, c.sys, c.fft_plans, c.twiddles, c.half, 1);
+static void launch_inverse_yz(const LaunchCtx &c, cudaStream_t stream, bool all = false) {
+  const FftTask *ty = all ? c.tasks_y_all : c.tasks_y;
+  const int n = all ? c.n_tasks_y_all : c.n_tasks_y;
+  if (n > 0) k_fft_y<<<n, 256, 0, stream>>>(ty, c.sys, c.fft_plans, c.twiddles, c.half, 1);
   k_fft_z_c2r<<<c.n_tasks_z, 256, 0, stream>>>(c.tasks_z, c.sys, c.fft_plans, c.twiddles, c.half, c.real_grid);
 }
 
-int pme_launches(const LaunchCtx &c) { return c.pme_on ? 7 : 0; }
+// ----------------- y and x passes of one kz plane fused: forward y, forward x, the Ewald
+// convolution (and energy), inverse x, inverse y, with the whole plane in shared memory. One
+// block per (system, kz) plane of the half spectrum, for systems with small planes (see
+// fft_plane_smem_bytes): three launches and two trips of the half spectrum through L2 become
+// one. The per-point arithmetic is k_fft_x_convolve's; the energy
+// partial is the plane's, so a system's partials are grouped the same way in a batch as alone.
+template <bool ENERGY>
+__global__ void __launch_bounds__(256) k_fft_plane(const FftTask *__restrict__ tasks,
+                                                   const DevSys *__restrict__ sys,
+                                                   const DevSysD *__restrict__ sysd,
+                                                   const FftPlan *__restrict__ plans,
+                                                   const float2 *__restrict__ twiddles,
+                                                   const float *__restrict__ moduli,
+                                                   float2 *__restrict__ half, int plane_stride,
+                                                   double *__restrict__ e_pme, double *__restrict__ e_pme_vir) {
+  extern __shared__ float2 plane_smem[];
+  __shared__ double red[2][256 / 32];
+  float2 *bufa = plane_smem, *bufb = plane_smem + plane_stride;
+  const FftTask t = tasks[blockIdx.x];
+  const DevSys &s = sys[t.sys];
+  const FftPlan &pl = plans[t.sys];
+  const int nx = s.grid[0], ny = s.grid[1], nz = s.grid[2], nzh = nz / 2 + 1;
+  const int kz = t.fixed;
+  const int ldy = ny + 1, ldx = nx + 1;  // padded lines (bank-conflict-free transposes)
+  float2 *h = half + s.half_base + kz;  // element (x, y) at h[(x * ny + y) * nzh]
+  for (int idx = threadIdx.x; idx < nx * ny; idx += blockDim.x) {
+    const int x = idx / ny, y = idx - x * ny;
+    bufa[x * ldy + y] = h[(long long)idx * nzh];
+  }
+  // forward y: nx lines of ny
+  float2 *r = fft_lines(bufa, bufb, nx, ny, ldy, pl.axis[1], twiddles + pl.axis[1].tw_base, false);
+  float2 *o = (r == bufa) ? bufb : bufa;
+  for (int idx = threadIdx.x; idx < nx * ny; idx += blockDim.x) {
+    const int x = idx / ny, y = idx - x * ny;
+    o[y * ldx + x] = r[x * ldy + y];
+  }
+  // forward x: ny lines of nx
+  r = fft_lines(o, r, ny, nx, ldx, pl.axis[0], twiddles + pl.axis[0].tw_base, false);
+  const double volume = sysd[t.sys].volume;
+  const double alpha = sysd[t.sys].alpha;
+  const float factor = (float)(M_PI * M_PI / (alpha * alpha));
+  const float two_pref = (float)(2.0 * ONE_4PI_EPS0 / (2.0 * M_PI * volume));
+  const float *modx = moduli + s.moduli_base, *mody = modx + nx, *modz = mody + ny;
+  double energy = 0.0, virial = 0.0;
+  for (int idx = threadIdx.x; idx < nx * ny; idx += blockDim.x) {
+    const int y = idx / nx, mx = idx - y * nx;
+    const int kx = mx <= nx / 2 ? mx : mx - nx;
+    const int ky = y <= ny / 2 ? y : y - ny;
+    const int at = y * ldx + mx;
+    float2 v = r[at];
+    if (kx == 0 && ky == 0 && kz == 0) {
+      r[at] = make_float2(0.f, 0.f);
+      continue;
+    }
+    const float fx = (float)kx, fy = (float)ky, fz = (float)kz;
+    const float cx = fx * s.recip[0] + fy * s.recip[1] + fz * s.recip[2];
+    const float cy = fx * s.recip[3] + fy * s.recip[4] + fz * s.recip[5];
+    const float cz = fx * s.recip[6] + fy * s.recip[7] + fz * s.recip[8];
+    const float m2 = cx * cx + cy * cy + cz * cz;
+    const float kernel = __expf(-factor * m2) / (m2 * modx[mx] * mody[y] * modz[kz]);
+    if (ENERGY) {
+      const double weight = (kz == 0 || 2 * kz == nz) ? 1.0 : 2.0;
+      const double ek = weight * 0.5 * (double)two_pref * (double)kernel * ((double)v.x * v.x + (double)v.y * v.y);
+      energy += ek;
+      virial += ek * (1.0 + (double)factor * (double)m2);
+    }
+    const float sc = kernel * two_pref;
+    r[at] = make_float2(v.x * sc, v.y * sc);
+  }
+  // inverse x
+  o = (r == bufa) ? bufb : bufa;
+  r = fft_lines(r, o, ny, nx, ldx, pl.axis[0], twiddles + pl.axis[0].tw_base, true);
+  o = (r == bufa) ? bufb : bufa;
+  for (int idx = threadIdx.x; idx < nx * ny; idx += blockDim.x) {
+    const int x = idx / ny, y = idx - x * ny;
+    o[x * ldy + y] = r[y * ldx + x];
+  }
+  // inverse y
+  r = fft_lines(o, r, nx, ny, ldy, pl.axis[1], twiddles + pl.axis[1].tw_base, true);
+  for (int idx = threadIdx.x; idx < nx * ny; idx += blockDim.x) {
+    const int x = idx / ny, y = idx - x * ny;
+    h[(long long)idx * nzh] = r[x * ldy + y];
+  }
+  if (ENERGY) {
+    energy = warp_sum(energy);
+    virial = warp_sum(virial);
+    if ((threadIdx.x & 31) == 0) {
+      red[0][threadIdx.x >> 5] = energy;
+      red[1][threadIdx.x >> 5] = virial;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double total = 0, total_vir = 0;
+      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+        total += red[0][w];
+        total_vir += red[1][w];
+      }
+      e_pme[blockIdx.x] = total;
+      e_pme_vir[blockIdx.x] = total_vir;
+    }
+  }
+}
+
+// Bytes of dynamic shared memory the fused plane kernel takes for a grid, or 0 when the
+// system keeps the separate y and x passes: a plane of more than 52 x 52 points. The fused
+// pass runs one block a plane, so a large grid has few blocks each carrying a long serial
+// chain; measured on one B200 (the seven reciprocal kernels) it is faster at 32^3 (0.037
+// against 0.041 ms) and for 64 grids of 22^3-50^3 together (0.30 against 0.34 ms), slower at
+// 64^3 (0.071 against 0.056 ms) and 100^3 (0.194 against 0.152 ms). The rule depends on the
+// system alone, so a system takes the same pass in a batch as alone.
+long long fft_plane_smem_bytes(int nx, int ny) {
+  if ((long long)nx * ny > 52 * 52) return 0;
+  const long long plane = std::max((long long)nx * (ny + 1), (long long)ny * (nx + 1));
+  const long long bytes = 2 * plane * (long long)sizeof(float2);
+  return bytes <= FFT_PLANE_SMEM_MAX ? bytes : 0;
+}
+
+// The largest dynamic shared memory the plane kernel may take, set once per device before any
+// launch (and never lowered, so engines with different grids cannot undercut each other).
+cudaError_t fft_plane_prepare() {
+  cudaError_t e = cudaFuncSetAttribute(k_fft_plane<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)FFT_PLANE_SMEM_MAX);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(k_fft_plane<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)FFT_PLANE_SMEM_MAX);
+}
+
+static void launch_planes(const LaunchCtx &c, bool energy, cudaStream_t stream) {
+  if (c.n_tasks_plane <= 0) return;
+  const size_t smem = 2 * (size_t)c.plane_stride * sizeof(float2);
+  double *e = c.e_pme + c.n_tasks_x, *ev = c.e_pme_vir + c.n_tasks_x;  // after the x tasks' partials
+  if (energy)
+    k_fft_plane<true><<<c.n_tasks_plane, 256, smem, stream>>>(c.tasks_plane, c.sys, c.sysd, c.fft_plans, c.twiddles,
+                                                             c.moduli, c.half, c.plane_stride, e, ev);
+  else
+    k_fft_plane<false><<<c.n_tasks_plane, 256, smem, stream>>>(c.tasks_plane, c.sys, c.sysd, c.fft_plans,
+                                                              c.twiddles, c.moduli, c.half, c.plane_stride, e, ev);
+}
+
+int pme_launches(const LaunchCtx &c) {
+  if (!c.pme_on) return 0;
+  return 4 + (c.n_tasks_plane > 0 ? 1 : 0) + (c.n_tasks_x > 0 ? 3 : 0);
+}
 
 // Everything up to the convolved real grid: spreading, forward transform, convolution (and
 // energy), inverse transform.
+static void launch_transform_convolve(const LaunchCtx &c, bool energy, cudaStream_t stream) {
+  launch_forward_zy(c, stream);
+  launch_planes(c, energy, stream);
+  if (c.n_tasks_x > 0) {
+    if (energy)
+      k_fft_x_convolve<true><<<c.n_tasks_x, 256, 0, stream>>>(c.tasks_x, c.sys, c.sysd, c.fft_plans,
+                                                              c.twiddles, c.moduli, c.half, c.e_pme,
+                                                              c.e_pme_vir);
+    else
+      k_fft_x_convolve<false><<<c.n_tasks_x, 256, 0, stream>>>(c.tasks_x, c.sys, c.sysd, c.fft_plans,
+                                                               c.twiddles, c.moduli, c.half, c.e_pme,
+                                                               c.e_pme_vir);
+  }
+  launch_inverse_yz(c, stream);
+}
+
 void launch_pme_grid(const LaunchCtx &c, bool energy, cudaStream_t stream) {
   if (!c.pme_on) return;
   launch_spread_only(c, stream);
-  launch_forward_zy(c, stream);
-  if (energy)
-    k_fft_x_convolve<true><<<c.n_tasks_x, 256, 0, stream>>>(c.tasks_x, c.sys, c.sysd, c.fft_plans,
-                                                            c.twiddles, c.moduli, c.half, c.e_pme,
-                                                            c.e_pme_vir);
-  else
-    k_fft_x_convolve<false><<<c.n_tasks_x, 256, 0, stream>>>(c.tasks_x, c.sys, c.sysd, c.fft_plans,
-                                                             c.twiddles, c.moduli, c.half, c.e_pme,
-                                                             c.e_pme_vir);
-  launch_inverse_yz(c, stream);
+  launch_transform_convolve(c, energy, stream);
 }
 
 void launch_pme_gather(const LaunchCtx &c, cudaStream_t stream) {
@@ -535,16 +690,7 @@ void launch_pme_gather(const LaunchCtx &c, cudaStream_t stream) {
 void launch_pme(const LaunchCtx &c, bool energy, cudaStream_t stream) {
   if (!c.pme_on) return;
   launch_spread_only(c, stream);
-  launch_forward_zy(c, stream);
-  if (energy)
-    k_fft_x_convolve<true><<<c.n_tasks_x, 256, 0, stream>>>(c.tasks_x, c.sys, c.sysd, c.fft_plans,
-                                                            c.twiddles, c.moduli, c.half, c.e_pme,
-                                                            c.e_pme_vir);
-  else
-    k_fft_x_convolve<false><<<c.n_tasks_x, 256, 0, stream>>>(c.tasks_x, c.sys, c.sysd, c.fft_plans,
-                                                             c.twiddles, c.moduli, c.half, c.e_pme,
-                                                             c.e_pme_vir);
-  launch_inverse_yz(c, stream);
+  launch_transform_convolve(c, energy, stream);
   launch_gather(c, stream);
 }
 
@@ -584,14 +730,15 @@ void launch_spread_only(const LaunchCtx &c, cudaStream_t stream) {
     k_spread<5><<<blocks, per_block * 25, 0, stream>>>(c.posq, c.sys_of_atom, c.sys, c.fixed_grid, n);
 }
 
+// (the debug transforms run the separate passes over every system)
 void launch_fft_forward(const LaunchCtx &c, cudaStream_t stream) {
-  launch_forward_zy(c, stream);
-  k_fft_x_plain<<<c.n_tasks_x, 256, 0, stream>>>(c.tasks_x, c.sys, c.fft_plans, c.twiddles, c.half, 0);
+  launch_forward_zy(c, stream, true);
+  k_fft_x_plain<<<c.n_tasks_x_all, 256, 0, stream>>>(c.tasks_x_all, c.sys, c.fft_plans, c.twiddles, c.half, 0);
 }
 
 void launch_fft_inverse(const LaunchCtx &c, cudaStream_t stream) {
-  k_fft_x_plain<<<c.n_tasks_x, 256, 0, stream>>>(c.tasks_x, c.sys, c.fft_plans, c.twiddles, c.half, 1);
-  launch_inverse_yz(c, stream);
+  k_fft_x_plain<<<c.n_tasks_x_all, 256, 0, stream>>>(c.tasks_x_all, c.sys, c.fft_plans, c.twiddles, c.half, 1);
+  launch_inverse_yz(c, stream, true);
 }
 
 }  // namespace rmd

@@ -331,3 +331,30 @@ def test_restraint_vs_openmm():
     e, _ = sim.debugEvaluate()
     assert relative(e["position_restraint"], float(raw["ala-wat-restraint-500:group.CustomExternalForce"])) < 1e-5
     assert relative(e["potential"], float(raw["ala-wat-restraint-500:energy.total"])) < 5e-5
+
+
+def test_fused_and_separate_reciprocal_passes_agree():
+    """A system with a small kz plane takes the fused y-x-convolve-x-y pass, one with a large
+    plane (120 x 120) the separate passes. In one batch each gives its solo
+    energies bit for bit, and both match the FP64 oracle's reciprocal energy and forces."""
+    s, pos, _ = system_for("ala-wat")
+    grids = ([24, 24, 24], [120, 120, 24])
+    solo = []
+    for grid in grids:
+        sim = engine_for(s, pos, grid=grid)
+        e, forces = sim.debugEvaluate()
+        eo, fo = oracle_terms(s, pos, ALPHA, grid, 5)
+        assert relative(e["coulomb_reciprocal"], eo["coulombReciprocal"]) < 2e-5, grid
+        rms = math.sqrt(np.mean(fo ** 2))
+        assert np.max(np.abs(forces - fo)) / rms < 3e-3, grid
+        solo.append(e)
+        sim.release()
+    batch = BatchSimulation([s, s], [{"alpha": ALPHA, "grid": g, "skin": 0.1, "dispersionCorrection": False}
+                                     for g in grids])
+    batch.setState(0, pos)
+    batch.setState(1, pos)
+    batch.initialise()
+    for k in range(2):
+        e, _ = batch.debugEvaluate(k)
+        for key in ("coulomb_reciprocal", "potential"):
+            assert e[key] == solo[k][key], (k, key)
