@@ -216,10 +216,9 @@ struct Engine {
   DevArray<float2> half, twiddles;
   DevArray<float> real_grid, moduli;
   DevArray<FftPlan> fft_plans;
-  DevArray<FftTask> tasks_z, tasks_y, tasks_x, tasks_plane, tasks_y_all, tasks_x_all;
-  std::vector<int> task_x_start;  // per system range of x tasks (systems on the separate passes)
-  std::vector<int> plane_start;   // per system range of kz-plane tasks (systems on the fused pass)
-  int plane_stride = 0;
+  DevArray<FftTask> tasks_z, tasks_y, tasks_x, tasks_plane, tasks_cluster, tasks_y_all, tasks_x_all;
+  std::vector<long long> recip_lo, recip_hi;  // per system range [lo, hi) of reciprocal energy partials
+  int plane_stride = 0, cluster_rows = 0, cluster_cols = 0;
   DevArray<DevSys> sys;
   DevArray<DevSysD> sysd;
   std::vector<DevSys> h_sys;
@@ -885,10 +884,9 @@ void Engine::upload_all(const std::vector<const rmd_system *> &src) {
     std::vector<float> h_mod;
     std::vector<float2> h_tw;
     std::vector<FftPlan> h_plans(S);
-    std::vector<FftTask> tz, ty, tx, tp, ty_all, tx_all;
-    task_x_start.assign(S + 1, 0);
-    plane_start.assign(S + 1, 0);
-    plane_stride = 0;
+    std::vector<FftTask> tz, ty, tx, tp, tq, ty_all, tx_all;
+    std::vector<int> split(S);
+    plane_stride = cluster_rows = cluster_cols = 0;
     // Lines per block. The z and y passes (no sums across lines) are sized from the whole
     // batch's line count: as many lines as fit the shared buffers and about 2 elements per
     // thread, but few enough that a pass has at least ~4 blocks per SM (592 on 148 SMs), so 64
@@ -929,9 +927,10 @@ void Engine::upload_all(const std::vector<const rmd_system *> &src) {
       const int mz = lines_per_block(all_pairs, nz, 64);
       for (int p = 0; p < pairs; p += mz) tz.push_back(FftTask{s, 0, p, std::min(mz, pairs - p)});
       // A system whose kz plane fits shared memory runs the fused y-x-convolve-x-y pass, one
-      // block a plane; the others run the separate y and x passes. The debug transforms run
-      // the separate passes over every system.
-      const bool fused = fft_plane_smem_bytes(nx, ny) > 0;
+      // block or one cluster of blocks a plane; the others run the separate y and x passes. The
+      // debug transforms run the separate passes over every system.
+      split[s] = fft_plane_split(nx, ny);
+      const bool fused = split[s] > 0;
       const int my = lines_per_block(all_ylines, ny + 1, nzh);  // y and x lines are padded to n + 1
       const int mx = std::max(1, std::min(nzh, std::min(FFT_SMEM_HOST / (nx + 1), 512 / (nx + 1))));
       for (int x = 0; x < nx; ++x)
@@ -939,21 +938,40 @@ void Engine::upload_all(const std::vector<const rmd_system *> &src) {
           ty_all.push_back(FftTask{s, x, k, std::min(my, nzh - k)});
           if (!fused) ty.push_back(ty_all.back());
         }
-      task_x_start[s] = (int)tx.size();
-      plane_start[s] = (int)tp.size();
       for (int y = 0; y < ny; ++y)
         for (int k = 0; k < nzh; k += mx) {
           tx_all.push_back(FftTask{s, y, k, std::min(mx, nzh - k)});
           if (!fused) tx.push_back(tx_all.back());
         }
-      if (fused) {
-        for (int kz = 0; kz < nzh; ++kz) tp.push_back(FftTask{s, kz, 0, 0});
-        plane_stride = std::max(plane_stride, std::max(nx * (ny + 1), ny * (nx + 1)));
+      int rows = 0, cols = 0;
+      if (fused) fft_plane_buffers(nx, ny, split[s], &rows, &cols);
+      std::vector<FftTask> &planes = split[s] == 1 ? tp : tq;
+      for (int kz = 0; fused && kz < nzh; ++kz) planes.push_back(FftTask{s, kz, 0, 0});
+      if (split[s] == 1) plane_stride = std::max(plane_stride, rows);
+      if (split[s] > 1) {
+        cluster_rows = std::max(cluster_rows, rows);
+        cluster_cols = std::max(cluster_cols, cols);
       }
     }
-    task_x_start[S] = (int)tx.size();
-    plane_start[S] = (int)tp.size();
-    if (!tp.empty()) CUDA_OK(fft_plane_prepare());
+    // energy partials: the x tasks' (one each), the planes' (one each), the clusters'
+    // (PLANE_CLUSTER each); a system's are contiguous within its pass's range
+    {
+      const long long base_p = (long long)tx.size(), base_q = base_p + (long long)tp.size();
+      recip_lo.assign(S, 0);
+      recip_hi.assign(S, 0);
+      for (int s = 0; s < S; ++s) recip_lo[s] = LLONG_MAX;
+      auto cover = [&](int s, long long k) {
+        recip_lo[s] = std::min(recip_lo[s], k);
+        recip_hi[s] = std::max(recip_hi[s], k + 1);
+      };
+      for (size_t k = 0; k < tx.size(); ++k) cover(tx[k].sys, (long long)k);
+      for (size_t k = 0; k < tp.size(); ++k) cover(tp[k].sys, base_p + (long long)k);
+      for (size_t k = 0; k < tq.size(); ++k)
+        for (int r = 0; r < PLANE_CLUSTER; ++r) cover(tq[k].sys, base_q + (long long)k * PLANE_CLUSTER + r);
+      for (int s = 0; s < S; ++s)
+        if (recip_lo[s] == LLONG_MAX) recip_lo[s] = recip_hi[s] = 0;  // no reciprocal tasks
+    }
+    if (!tp.empty() || !tq.empty()) CUDA_OK(fft_plane_prepare());
     fixed_grid.alloc(gbase);
     fixed_grid.zero();
     half.alloc(hbase);
@@ -966,10 +984,10 @@ void Engine::upload_all(const std::vector<const rmd_system *> &src) {
     tasks_y.upload(ty);
     tasks_x.upload(tx);
     tasks_plane.upload(tp);
+    tasks_cluster.upload(tq);
     tasks_y_all.upload(ty_all);
     tasks_x_all.upload(tx_all);
-    // energy partials: the x tasks' first, then the planes'
-    const size_t partials = std::max<size_t>(1, tx.size() + tp.size());
+    const size_t partials = std::max<size_t>(1, tx.size() + tp.size() + tq.size() * PLANE_CLUSTER);
     e_pme.alloc(partials);
     e_pme.zero();
     e_pme_vir.alloc(partials);
@@ -1061,15 +1079,8 @@ void Engine::upload_all(const std::vector<const rmd_system *> &src) {
   // ---- energy segments
   {
     std::vector<Segment> seg;
-    // a system's reciprocal partials: its x tasks' on the separate passes, else its planes'
-    // (stored after every x task's)
-    const long long n_tx = (long long)tasks_x.n;
-    auto recip_begin = [&](int s) {
-      return plane_start[s + 1] > plane_start[s] ? n_tx + plane_start[s] : (long long)task_x_start[s];
-    };
-    auto recip_end = [&](int s) {
-      return plane_start[s + 1] > plane_start[s] ? n_tx + plane_start[s + 1] : (long long)task_x_start[s + 1];
-    };
+    auto recip_begin = [&](int s) { return recip_lo[s]; };
+    auto recip_end = [&](int s) { return recip_hi[s]; };
     for (int s = 0; s < S; ++s) {
       const HostSystem &h = hs[s];
       const long long a0 = h.atom_start, a1 = h.atom_start + h.n;
@@ -1200,6 +1211,10 @@ LaunchCtx Engine::ctx() const {
   c.tasks_y_all = tasks_y_all.p;
   c.tasks_x_all = tasks_x_all.p;
   c.n_tasks_plane = (int)tasks_plane.n;
+  c.tasks_cluster = tasks_cluster.p;
+  c.n_tasks_cluster = (int)tasks_cluster.n;
+  c.cluster_rows = cluster_rows;
+  c.cluster_cols = cluster_cols;
   c.n_tasks_y_all = (int)tasks_y_all.n;
   c.n_tasks_x_all = (int)tasks_x_all.n;
   c.plane_stride = plane_stride;

@@ -135,12 +135,15 @@ struct LaunchCtx {
   const float *moduli;
   const float2 *twiddles;
   const FftPlan *fft_plans;
-  // z tasks cover every system; y and x tasks the systems whose kz planes do not fit the fused
-  // plane kernel, whose plane tasks (one per kz plane) come last; *_all cover every system (the
-  // debug transforms)
-  const FftTask *tasks_z, *tasks_y, *tasks_x, *tasks_plane, *tasks_y_all, *tasks_x_all;
-  int n_tasks_z, n_tasks_y, n_tasks_x, n_tasks_plane, n_tasks_y_all, n_tasks_x_all;
-  int plane_stride;  // complex values per plane buffer (the largest plane among the fused systems)
+  // z tasks cover every system; y and x tasks the systems on the separate passes; plane tasks
+  // (one per kz plane) the systems whose planes a block transforms alone, cluster tasks (one
+  // per kz plane) those whose planes a cluster of PLANE_CLUSTER blocks shares; *_all cover
+  // every system (the debug transforms)
+  const FftTask *tasks_z, *tasks_y, *tasks_x, *tasks_plane, *tasks_cluster, *tasks_y_all, *tasks_x_all;
+  int n_tasks_z, n_tasks_y, n_tasks_x, n_tasks_plane, n_tasks_cluster, n_tasks_y_all, n_tasks_x_all;
+  int plane_stride;  // complex values per plane buffer (the largest plane among the one-block systems)
+  int cluster_rows, cluster_cols;  // complex values per row / column buffer of a cluster block
+  // energy partials: one per x task, then one per plane task, then PLANE_CLUSTER per cluster task
   double *e_pme, *e_pme_vir;
 };
 
@@ -162,9 +165,16 @@ void launch_pme(const LaunchCtx &c, bool energy, cudaStream_t stream);
 void launch_pme_grid(const LaunchCtx &c, bool energy, cudaStream_t stream);
 void launch_pme_gather(const LaunchCtx &c, cudaStream_t stream);
 int pme_launches(const LaunchCtx &c);  // kernels launch_pme issues
-// dynamic shared memory of the fused plane pass for an nx x ny plane, 0 when it does not fit
+// The fused y-x-convolve-x-y pass over kz planes (pme.cu). fft_plane_split gives how a system's
+// nx x ny planes are transformed: 1 = one block a plane, PLANE_CLUSTER = a thread-block cluster
+// of that many blocks a plane (rows and columns split between them, exchanged through
+// distributed shared memory), 0 = the separate y and x passes.
 constexpr long long FFT_PLANE_SMEM_MAX = 200 * 1024;
-long long fft_plane_smem_bytes(int nx, int ny);
+constexpr int PLANE_CLUSTER = 4;
+int fft_plane_split(int nx, int ny);
+// complex values per shared buffer for a split: the whole padded plane for 1; for a cluster,
+// a block's rows (rows_per x (ny + 1)) and its columns (cols_per x (nx + 1))
+void fft_plane_buffers(int nx, int ny, int split, int *rows, int *cols);
 cudaError_t fft_plane_prepare();
 void launch_fft_forward(const LaunchCtx &c, cudaStream_t stream);
 void launch_spread_only(const LaunchCtx &c, cudaStream_t stream);

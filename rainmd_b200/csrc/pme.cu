@@ -15,16 +15,23 @@
 //   x pass   forward FFT along x, the Ewald convolution and the FP64 energy partial, and
 //            the inverse FFT along x, all while the lines are in shared memory;
 //   y pass   inverse; z pass C2R back to a real f32 grid; gather four threads per atom.
+//   planes   where a kz plane fits shared memory, the y pass, the x pass and the inverse y
+//            pass are one kernel over whole planes: one block a plane for small planes, a
+//            thread-block cluster a plane (distributed shared memory) for larger ones.
 // Lines filled by a transpose (y and x passes) are padded to n + 1 in shared memory.
 // The FFT is a mixed-radix (4, 2, 3, 5) Stockham autosort over lines held in shared
 // memory; a host-built task table gives each block a set of lines of one system, so
 // systems with different grid sizes run in the same launch.
 #include <algorithm>
 
+#include <cooperative_groups.h>
+
 #include "common.cuh"
 #include "kernels.h"
 
 namespace rmd {
+
+namespace cg = cooperative_groups;
 
 __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
   return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
@@ -102,18 +109,10 @@ __device__ __forceinline__ void stockham_stage(const float2 *__restrict__ in, fl
 
 // Transform `lines` lines of length N held in a, line l starting at a + l * ld (ld >= N;
 // lines filled by a transpose use ld = N + 1 so that the transposing accesses, which step
-// by ld, fall in different shared-memory banks); returns the buffer holding the result.
-__device__ float2 *fft_lines(float2 *a, float2 *b, int lines, int N, int ld, const FftAxis &ax,
-                             const float2 *tw, bool inv) {
-  // the axis's twiddles in shared memory, so the stages read them without a global round
-  // trip after each barrier (tables longer than the cache stay in global memory)
-  constexpr int TW_CACHE = 512;
-  __shared__ float2 tw_cache[TW_CACHE];
-  if (N <= TW_CACHE) {
-    __syncthreads();  // a previous transform in this block has finished with the cache
-    for (int k = threadIdx.x; k < N; k += blockDim.x) tw_cache[k] = tw[k];
-    tw = tw_cache;    // visible after the barrier that opens the first stage
-  }
+// by ld, fall in different shared-memory banks); returns the buffer holding the result. The
+// twiddles tw are read as given (global or shared memory).
+__device__ float2 *fft_stages(float2 *a, float2 *b, int lines, int N, int ld, const FftAxis &ax,
+                              const float2 *tw, bool inv) {
   int Ns = 1;
   for (int st = 0; st < ax.nstages; ++st) {
     const int R = ax.radix[st];
@@ -129,6 +128,22 @@ __device__ float2 *fft_lines(float2 *a, float2 *b, int lines, int N, int ld, con
   }
   __syncthreads();
   return a;
+}
+
+// Twiddle tables up to this length are read from shared memory.
+constexpr int TW_CACHE = 512;
+
+// fft_stages with the axis's twiddles first copied to shared memory, so the stages read them
+// without a global round trip after each barrier (longer tables stay in global memory).
+__device__ float2 *fft_lines(float2 *a, float2 *b, int lines, int N, int ld, const FftAxis &ax,
+                             const float2 *tw, bool inv) {
+  __shared__ float2 tw_cache[TW_CACHE];
+  if (N <= TW_CACHE) {
+    __syncthreads();  // a previous transform in this block has finished with the cache
+    for (int k = threadIdx.x; k < N; k += blockDim.x) tw_cache[k] = tw[k];
+    tw = tw_cache;    // visible after the barrier that opens the first stage
+  }
+  return fft_stages(a, b, lines, N, ld, ax, tw, inv);
 }
 
 constexpr int FFT_SMEM = 2048;  // complex values per buffer per block
@@ -515,12 +530,87 @@ static void launch_inverse_yz(const LaunchCtx &c, cudaStream_t stream, bool all 
   k_fft_z_c2r<<<c.n_tasks_z, 256, 0, stream>>>(c.tasks_z, c.sys, c.fft_plans, c.twiddles, c.half, c.real_grid);
 }
 
+// A plane pass's per-axis tables in shared memory: the y and x twiddles and B-spline moduli,
+// copied once when the plane is loaded (in the same round trip as the plane) instead of before
+// each of the four transforms. Planes on these passes have nx, ny <= TW_CACHE.
+struct PlaneTables {
+  float2 tw_y[TW_CACHE], tw_x[TW_CACHE];
+  float mod_x[TW_CACHE], mod_y[TW_CACHE];
+};
+
+// Fill the tables (visible after the barrier that opens the first transform stage); returns
+// the z moduli, read from global memory (one value a plane).
+__device__ __forceinline__ const float *stage_plane_tables(PlaneTables &tab, const FftPlan &pl,
+                                                           const float2 *__restrict__ twiddles,
+                                                           const float *__restrict__ mod, int nx, int ny) {
+  for (int k = threadIdx.x; k < ny; k += blockDim.x) {
+    tab.tw_y[k] = twiddles[pl.axis[1].tw_base + k];
+    tab.mod_y[k] = mod[nx + k];
+  }
+  for (int k = threadIdx.x; k < nx; k += blockDim.x) {
+    tab.tw_x[k] = twiddles[pl.axis[0].tw_base + k];
+    tab.mod_x[k] = mod[k];
+  }
+  return mod + nx + ny;
+}
+
+// The Ewald convolution of one half-spectrum point (x index mx, y index my, plane kz) in place,
+// with its energy and virial terms added when ENERGY: the per-point arithmetic of
+// k_fft_x_convolve, shared by the fused plane passes.
+template <bool ENERGY>
+__device__ __forceinline__ void convolve_point(float2 &v, int mx, int my, int kz, int nx, int ny, int nz,
+                                               const DevSys &s, const float *modx, const float *mody,
+                                               const float *modz, float factor, float two_pref,
+                                               double &energy, double &virial) {
+  const int kx = mx <= nx / 2 ? mx : mx - nx;
+  const int ky = my <= ny / 2 ? my : my - ny;
+  if (kx == 0 && ky == 0 && kz == 0) {
+    v = make_float2(0.f, 0.f);
+    return;
+  }
+  const float fx = (float)kx, fy = (float)ky, fz = (float)kz;
+  const float cx = fx * s.recip[0] + fy * s.recip[1] + fz * s.recip[2];
+  const float cy = fx * s.recip[3] + fy * s.recip[4] + fz * s.recip[5];
+  const float cz = fx * s.recip[6] + fy * s.recip[7] + fz * s.recip[8];
+  const float m2 = cx * cx + cy * cy + cz * cz;
+  const float kernel = __expf(-factor * m2) / (m2 * modx[mx] * mody[my] * modz[kz]);
+  if (ENERGY) {
+    const double weight = (kz == 0 || 2 * kz == nz) ? 1.0 : 2.0;
+    const double ek = weight * 0.5 * (double)two_pref * (double)kernel * ((double)v.x * v.x + (double)v.y * v.y);
+    energy += ek;
+    virial += ek * (1.0 + (double)factor * (double)m2);
+  }
+  const float sc = kernel * two_pref;
+  v = make_float2(v.x * sc, v.y * sc);
+}
+
+// Block sum of a thread's energy and virial terms, written by thread 0 to e[slot], ev[slot].
+__device__ __forceinline__ void block_energy(double energy, double virial, double *e, double *ev, int slot) {
+  __shared__ double red[2][256 / 32];
+  energy = warp_sum(energy);
+  virial = warp_sum(virial);
+  if ((threadIdx.x & 31) == 0) {
+    red[0][threadIdx.x >> 5] = energy;
+    red[1][threadIdx.x >> 5] = virial;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double total = 0, total_vir = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+      total += red[0][w];
+      total_vir += red[1][w];
+    }
+    e[slot] = total;
+    ev[slot] = total_vir;
+  }
+}
+
 // ----------------- y and x passes of one kz plane fused: forward y, forward x, the Ewald
 // convolution (and energy), inverse x, inverse y, with the whole plane in shared memory. One
 // block per (system, kz) plane of the half spectrum, for systems with small planes (see
-// fft_plane_smem_bytes): three launches and two trips of the half spectrum through L2 become
-// one. The per-point arithmetic is k_fft_x_convolve's; the energy
-// partial is the plane's, so a system's partials are grouped the same way in a batch as alone.
+// fft_plane_split): three launches and two trips of the half spectrum through L2 become
+// one. The energy partial is the plane's, so a system's partials are grouped the same way in a
+// batch as alone.
 template <bool ENERGY>
 __global__ void __launch_bounds__(256) k_fft_plane(const FftTask *__restrict__ tasks,
                                                    const DevSys *__restrict__ sys,
@@ -531,7 +621,7 @@ __global__ void __launch_bounds__(256) k_fft_plane(const FftTask *__restrict__ t
                                                    float2 *__restrict__ half, int plane_stride,
                                                    double *__restrict__ e_pme, double *__restrict__ e_pme_vir) {
   extern __shared__ float2 plane_smem[];
-  __shared__ double red[2][256 / 32];
+  __shared__ PlaneTables tab;
   float2 *bufa = plane_smem, *bufb = plane_smem + plane_stride;
   const FftTask t = tasks[blockIdx.x];
   const DevSys &s = sys[t.sys];
@@ -544,119 +634,196 @@ __global__ void __launch_bounds__(256) k_fft_plane(const FftTask *__restrict__ t
     const int x = idx / ny, y = idx - x * ny;
     bufa[x * ldy + y] = h[(long long)idx * nzh];
   }
+  const float *modz = stage_plane_tables(tab, pl, twiddles, moduli + s.moduli_base, nx, ny);
   // forward y: nx lines of ny
-  float2 *r = fft_lines(bufa, bufb, nx, ny, ldy, pl.axis[1], twiddles + pl.axis[1].tw_base, false);
+  float2 *r = fft_stages(bufa, bufb, nx, ny, ldy, pl.axis[1], tab.tw_y, false);
   float2 *o = (r == bufa) ? bufb : bufa;
   for (int idx = threadIdx.x; idx < nx * ny; idx += blockDim.x) {
     const int x = idx / ny, y = idx - x * ny;
     o[y * ldx + x] = r[x * ldy + y];
   }
   // forward x: ny lines of nx
-  r = fft_lines(o, r, ny, nx, ldx, pl.axis[0], twiddles + pl.axis[0].tw_base, false);
+  r = fft_stages(o, r, ny, nx, ldx, pl.axis[0], tab.tw_x, false);
   const double volume = sysd[t.sys].volume;
   const double alpha = sysd[t.sys].alpha;
   const float factor = (float)(M_PI * M_PI / (alpha * alpha));
   const float two_pref = (float)(2.0 * ONE_4PI_EPS0 / (2.0 * M_PI * volume));
-  const float *modx = moduli + s.moduli_base, *mody = modx + nx, *modz = mody + ny;
   double energy = 0.0, virial = 0.0;
   for (int idx = threadIdx.x; idx < nx * ny; idx += blockDim.x) {
     const int y = idx / nx, mx = idx - y * nx;
-    const int kx = mx <= nx / 2 ? mx : mx - nx;
-    const int ky = y <= ny / 2 ? y : y - ny;
-    const int at = y * ldx + mx;
-    float2 v = r[at];
-    if (kx == 0 && ky == 0 && kz == 0) {
-      r[at] = make_float2(0.f, 0.f);
-      continue;
-    }
-    const float fx = (float)kx, fy = (float)ky, fz = (float)kz;
-    const float cx = fx * s.recip[0] + fy * s.recip[1] + fz * s.recip[2];
-    const float cy = fx * s.recip[3] + fy * s.recip[4] + fz * s.recip[5];
-    const float cz = fx * s.recip[6] + fy * s.recip[7] + fz * s.recip[8];
-    const float m2 = cx * cx + cy * cy + cz * cz;
-    const float kernel = __expf(-factor * m2) / (m2 * modx[mx] * mody[y] * modz[kz]);
-    if (ENERGY) {
-      const double weight = (kz == 0 || 2 * kz == nz) ? 1.0 : 2.0;
-      const double ek = weight * 0.5 * (double)two_pref * (double)kernel * ((double)v.x * v.x + (double)v.y * v.y);
-      energy += ek;
-      virial += ek * (1.0 + (double)factor * (double)m2);
-    }
-    const float sc = kernel * two_pref;
-    r[at] = make_float2(v.x * sc, v.y * sc);
+    convolve_point<ENERGY>(r[y * ldx + mx], mx, y, kz, nx, ny, nz, s, tab.mod_x, tab.mod_y, modz, factor,
+                           two_pref, energy, virial);
   }
   // inverse x
   o = (r == bufa) ? bufb : bufa;
-  r = fft_lines(r, o, ny, nx, ldx, pl.axis[0], twiddles + pl.axis[0].tw_base, true);
+  r = fft_stages(r, o, ny, nx, ldx, pl.axis[0], tab.tw_x, true);
   o = (r == bufa) ? bufb : bufa;
   for (int idx = threadIdx.x; idx < nx * ny; idx += blockDim.x) {
     const int x = idx / ny, y = idx - x * ny;
     o[x * ldy + y] = r[y * ldx + x];
   }
   // inverse y
-  r = fft_lines(o, r, nx, ny, ldy, pl.axis[1], twiddles + pl.axis[1].tw_base, true);
+  r = fft_stages(o, r, nx, ny, ldy, pl.axis[1], tab.tw_y, true);
   for (int idx = threadIdx.x; idx < nx * ny; idx += blockDim.x) {
     const int x = idx / ny, y = idx - x * ny;
     h[(long long)idx * nzh] = r[x * ldy + y];
   }
-  if (ENERGY) {
-    energy = warp_sum(energy);
-    virial = warp_sum(virial);
-    if ((threadIdx.x & 31) == 0) {
-      red[0][threadIdx.x >> 5] = energy;
-      red[1][threadIdx.x >> 5] = virial;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      double total = 0, total_vir = 0;
-      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
-        total += red[0][w];
-        total_vir += red[1][w];
-      }
-      e_pme[blockIdx.x] = total;
-      e_pme_vir[blockIdx.x] = total_vir;
-    }
+  if (ENERGY) block_energy(energy, virial, e_pme, e_pme_vir, blockIdx.x);
+}
+
+// The same fused pass for larger planes, shared by a thread-block cluster of PLANE_CLUSTER
+// blocks so that a plane is not one block's serial chain. Block r of a cluster owns the x rows
+// [r * rows_per, ...) for the y transforms and the y columns [r * cols_per, ...) for the x
+// transforms and the convolution; between them each block gathers its lines from the other
+// blocks' shared memory (distributed shared memory), with three cluster barriers: after the
+// forward y pass (rows complete), after the inverse x pass (columns complete, and every block
+// done reading the rows), and after the gather back (every block done reading the columns, so
+// none exits while another still reads it). Every line goes through the same transform as in
+// k_fft_plane; the energy partials are one per block of the cluster.
+template <bool ENERGY>
+__global__ void __cluster_dims__(PLANE_CLUSTER, 1, 1) __launch_bounds__(256)
+    k_fft_plane_cluster(const FftTask *__restrict__ tasks, const DevSys *__restrict__ sys,
+                        const DevSysD *__restrict__ sysd, const FftPlan *__restrict__ plans,
+                        const float2 *__restrict__ twiddles, const float *__restrict__ moduli,
+                        float2 *__restrict__ half, int row_stride, int col_stride,
+                        double *__restrict__ e_pme, double *__restrict__ e_pme_vir) {
+  cg::cluster_group cluster = cg::this_cluster();
+  const int rank = (int)cluster.block_rank();
+  extern __shared__ float2 plane_smem[];
+  __shared__ PlaneTables tab;
+  float2 *ra = plane_smem, *rb = ra + row_stride, *ca = rb + row_stride, *cb = ca + col_stride;
+  const FftTask t = tasks[blockIdx.x / PLANE_CLUSTER];
+  const DevSys &s = sys[t.sys];
+  const FftPlan &pl = plans[t.sys];
+  const int nx = s.grid[0], ny = s.grid[1], nz = s.grid[2], nzh = nz / 2 + 1;
+  const int kz = t.fixed;
+  const int ldy = ny + 1, ldx = nx + 1;
+  const int rows_per = (nx + PLANE_CLUSTER - 1) / PLANE_CLUSTER, cols_per = (ny + PLANE_CLUSTER - 1) / PLANE_CLUSTER;
+  const int x0 = min(nx, rank * rows_per), nr = min(nx, x0 + rows_per) - x0;
+  const int y0 = min(ny, rank * cols_per), nc = min(ny, y0 + cols_per) - y0;
+  float2 *h = half + s.half_base + kz;  // element (x, y) at h[(x * ny + y) * nzh]
+  for (int idx = threadIdx.x; idx < nr * ny; idx += blockDim.x) {
+    const int xl = idx / ny, y = idx - xl * ny;
+    ra[xl * ldy + y] = h[((long long)(x0 + xl) * ny + y) * nzh];
   }
+  const float *modz = stage_plane_tables(tab, pl, twiddles, moduli + s.moduli_base, nx, ny);
+  // forward y over this block's rows; every block runs the same stages, so the result sits
+  // at the same offset in each block's shared memory
+  const float2 *rows = fft_stages(ra, rb, nr, ny, ldy, pl.axis[1], tab.tw_y, false);
+  cluster.sync();
+  for (int idx = threadIdx.x; idx < nc * nx; idx += blockDim.x) {
+    const int yl = idx / nx, x = idx - yl * nx;
+    const int owner = x / rows_per;
+    const float2 *src = cluster.map_shared_rank(rows, owner);
+    ca[yl * ldx + x] = src[(x - owner * rows_per) * ldy + y0 + yl];
+  }
+  // forward x over this block's columns, the convolution, inverse x
+  float2 *c = fft_stages(ca, cb, nc, nx, ldx, pl.axis[0], tab.tw_x, false);
+  const double volume = sysd[t.sys].volume;
+  const double alpha = sysd[t.sys].alpha;
+  const float factor = (float)(M_PI * M_PI / (alpha * alpha));
+  const float two_pref = (float)(2.0 * ONE_4PI_EPS0 / (2.0 * M_PI * volume));
+  double energy = 0.0, virial = 0.0;
+  for (int idx = threadIdx.x; idx < nc * nx; idx += blockDim.x) {
+    const int yl = idx / nx, mx = idx - yl * nx;
+    convolve_point<ENERGY>(c[yl * ldx + mx], mx, y0 + yl, kz, nx, ny, nz, s, tab.mod_x, tab.mod_y, modz, factor,
+                           two_pref, energy, virial);
+  }
+  const float2 *cols = fft_stages(c, c == ca ? cb : ca, nc, nx, ldx, pl.axis[0], tab.tw_x, true);
+  cluster.sync();
+  for (int idx = threadIdx.x; idx < nr * ny; idx += blockDim.x) {
+    const int xl = idx / ny, y = idx - xl * ny;
+    const int owner = y / cols_per;
+    const float2 *src = cluster.map_shared_rank(cols, owner);
+    ra[xl * ldy + y] = src[(y - owner * cols_per) * ldx + x0 + xl];
+  }
+  cluster.sync();
+  // inverse y over this block's rows
+  const float2 *r = fft_stages(ra, rb, nr, ny, ldy, pl.axis[1], tab.tw_y, true);
+  for (int idx = threadIdx.x; idx < nr * ny; idx += blockDim.x) {
+    const int xl = idx / ny, y = idx - xl * ny;
+    h[((long long)(x0 + xl) * ny + y) * nzh] = r[xl * ldy + y];
+  }
+  if (ENERGY) block_energy(energy, virial, e_pme, e_pme_vir, blockIdx.x);
 }
 
-// Bytes of dynamic shared memory the fused plane kernel takes for a grid, or 0 when the
-// system keeps the separate y and x passes: a plane of more than 52 x 52 points. The fused
-// pass runs one block a plane, so a large grid has few blocks each carrying a long serial
-// chain; measured on one B200 (the seven reciprocal kernels) it is faster at 32^3 (0.037
+// Planes of at most this many points go to one block each. A block's plane is one serial
+// chain, so larger grids run faster shared by a cluster: measured on one B200 (the seven
+// reciprocal kernels) one block a plane is faster than the separate passes at 32^3 (0.037
 // against 0.041 ms) and for 64 grids of 22^3-50^3 together (0.30 against 0.34 ms), slower at
-// 64^3 (0.071 against 0.056 ms) and 100^3 (0.194 against 0.152 ms). The rule depends on the
-// system alone, so a system takes the same pass in a batch as alone.
-long long fft_plane_smem_bytes(int nx, int ny) {
-  if ((long long)nx * ny > 52 * 52) return 0;
-  const long long plane = std::max((long long)nx * (ny + 1), (long long)ny * (nx + 1));
-  const long long bytes = 2 * plane * (long long)sizeof(float2);
-  return bytes <= FFT_PLANE_SMEM_MAX ? bytes : 0;
+// 64^3 (0.071 against 0.056 ms) and 100^3 (0.194 against 0.152 ms).
+#ifndef PLANE_SINGLE_MAX
+#define PLANE_SINGLE_MAX (52 * 52)
+#endif
+
+void fft_plane_buffers(int nx, int ny, int split, int *rows, int *cols) {
+  if (split == 1) {
+    *rows = *cols = std::max(nx * (ny + 1), ny * (nx + 1));
+    return;
+  }
+  *rows = (nx + split - 1) / split * (ny + 1);
+  *cols = (ny + split - 1) / split * (nx + 1);
 }
 
-// The largest dynamic shared memory the plane kernel may take, set once per device before any
+// The rule depends on the system alone, so a system takes the same pass in a batch as alone.
+// A cluster block's row and column buffers are each held to half the limit, so that the
+// largest rows and the largest columns of different systems in one launch still fit together.
+int fft_plane_split(int nx, int ny) {
+  int rows, cols;
+  fft_plane_buffers(nx, ny, 1, &rows, &cols);
+  if (nx > TW_CACHE || ny > TW_CACHE) return 0;
+  if ((long long)nx * ny <= PLANE_SINGLE_MAX && 2LL * rows * (long long)sizeof(float2) <= FFT_PLANE_SMEM_MAX) return 1;
+  if (nx < PLANE_CLUSTER || ny < PLANE_CLUSTER) return 0;
+  fft_plane_buffers(nx, ny, PLANE_CLUSTER, &rows, &cols);
+  const long long half_limit = FFT_PLANE_SMEM_MAX / 2;
+  if (2LL * rows * (long long)sizeof(float2) <= half_limit && 2LL * cols * (long long)sizeof(float2) <= half_limit)
+    return PLANE_CLUSTER;
+  return 0;
+}
+
+// The largest dynamic shared memory the plane kernels may take, set once per device before any
 // launch (and never lowered, so engines with different grids cannot undercut each other).
 cudaError_t fft_plane_prepare() {
-  cudaError_t e = cudaFuncSetAttribute(k_fft_plane<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)FFT_PLANE_SMEM_MAX);
-  if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(k_fft_plane<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)FFT_PLANE_SMEM_MAX);
+  const void *fns[4] = {(const void *)k_fft_plane<true>, (const void *)k_fft_plane<false>,
+                        (const void *)k_fft_plane_cluster<true>, (const void *)k_fft_plane_cluster<false>};
+  for (const void *f : fns) {
+    cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)FFT_PLANE_SMEM_MAX);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
 }
 
 static void launch_planes(const LaunchCtx &c, bool energy, cudaStream_t stream) {
-  if (c.n_tasks_plane <= 0) return;
-  const size_t smem = 2 * (size_t)c.plane_stride * sizeof(float2);
-  double *e = c.e_pme + c.n_tasks_x, *ev = c.e_pme_vir + c.n_tasks_x;  // after the x tasks' partials
-  if (energy)
-    k_fft_plane<true><<<c.n_tasks_plane, 256, smem, stream>>>(c.tasks_plane, c.sys, c.sysd, c.fft_plans, c.twiddles,
-                                                             c.moduli, c.half, c.plane_stride, e, ev);
-  else
-    k_fft_plane<false><<<c.n_tasks_plane, 256, smem, stream>>>(c.tasks_plane, c.sys, c.sysd, c.fft_plans,
-                                                              c.twiddles, c.moduli, c.half, c.plane_stride, e, ev);
+  // partials after the x tasks': the planes' one each, then the clusters' PLANE_CLUSTER each
+  double *e = c.e_pme + c.n_tasks_x, *ev = c.e_pme_vir + c.n_tasks_x;
+  if (c.n_tasks_plane > 0) {
+    const size_t smem = 2 * (size_t)c.plane_stride * sizeof(float2);
+    if (energy)
+      k_fft_plane<true><<<c.n_tasks_plane, 256, smem, stream>>>(c.tasks_plane, c.sys, c.sysd, c.fft_plans,
+                                                               c.twiddles, c.moduli, c.half, c.plane_stride, e, ev);
+    else
+      k_fft_plane<false><<<c.n_tasks_plane, 256, smem, stream>>>(c.tasks_plane, c.sys, c.sysd, c.fft_plans,
+                                                                c.twiddles, c.moduli, c.half, c.plane_stride, e, ev);
+  }
+  if (c.n_tasks_cluster > 0) {
+    e += c.n_tasks_plane;
+    ev += c.n_tasks_plane;
+    const size_t smem = 2 * ((size_t)c.cluster_rows + c.cluster_cols) * sizeof(float2);
+    const int blocks = c.n_tasks_cluster * PLANE_CLUSTER;
+    if (energy)
+      k_fft_plane_cluster<true><<<blocks, 256, smem, stream>>>(c.tasks_cluster, c.sys, c.sysd, c.fft_plans,
+                                                              c.twiddles, c.moduli, c.half, c.cluster_rows,
+                                                              c.cluster_cols, e, ev);
+    else
+      k_fft_plane_cluster<false><<<blocks, 256, smem, stream>>>(c.tasks_cluster, c.sys, c.sysd, c.fft_plans,
+                                                               c.twiddles, c.moduli, c.half, c.cluster_rows,
+                                                               c.cluster_cols, e, ev);
+  }
 }
 
 int pme_launches(const LaunchCtx &c) {
   if (!c.pme_on) return 0;
-  return 4 + (c.n_tasks_plane > 0 ? 1 : 0) + (c.n_tasks_x > 0 ? 3 : 0);
+  return 4 + (c.n_tasks_plane > 0 ? 1 : 0) + (c.n_tasks_cluster > 0 ? 1 : 0) + (c.n_tasks_x > 0 ? 3 : 0);
 }
 
 // Everything up to the convolved real grid: spreading, forward transform, convolution (and

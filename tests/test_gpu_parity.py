@@ -334,11 +334,13 @@ def test_restraint_vs_openmm():
 
 
 def test_fused_and_separate_reciprocal_passes_agree():
-    """A system with a small kz plane takes the fused y-x-convolve-x-y pass, one with a large
-    plane (120 x 120) the separate passes. In one batch each gives its solo
-    energies bit for bit, and both match the FP64 oracle's reciprocal energy and forces."""
+    """A system with a small kz plane (up to 52 x 52 points) takes the fused y-x-convolve-x-y
+    pass one block a plane; larger planes up to 128 x 128 take it one thread-block cluster a
+    plane, rows and columns split four ways (evenly, or raggedly as 54 = 14 + 14 + 14 + 12);
+    a 160 x 160 plane takes the separate passes. In one batch each gives its solo energies bit
+    for bit, and all match the FP64 oracle's reciprocal energy and forces."""
     s, pos, _ = system_for("ala-wat")
-    grids = ([24, 24, 24], [120, 120, 24])
+    grids = ([24, 24, 24], [54, 60, 20], [72, 54, 20], [120, 120, 24], [160, 160, 16])
     solo = []
     for grid in grids:
         sim = engine_for(s, pos, grid=grid)
@@ -349,12 +351,12 @@ def test_fused_and_separate_reciprocal_passes_agree():
         assert np.max(np.abs(forces - fo)) / rms < 3e-3, grid
         solo.append(e)
         sim.release()
-    batch = BatchSimulation([s, s], [{"alpha": ALPHA, "grid": g, "skin": 0.1, "dispersionCorrection": False}
-                                     for g in grids])
-    batch.setState(0, pos)
-    batch.setState(1, pos)
+    batch = BatchSimulation([s] * len(grids), [{"alpha": ALPHA, "grid": g, "skin": 0.1,
+                                                 "dispersionCorrection": False} for g in grids])
+    for k in range(len(grids)):
+        batch.setState(k, pos)
     batch.initialise()
-    for k in range(2):
+    for k in range(len(grids)):
         e, _ = batch.debugEvaluate(k)
         for key in ("coulomb_reciprocal", "potential"):
             assert e[key] == solo[k][key], (k, key)
