@@ -215,7 +215,14 @@ __device__ __forceinline__ bool is_excluded(const int *__restrict__ start, const
   return false;
 }
 
-constexpr int NBR_WARPS = 4;
+constexpr int NBR_WARPS = 4;        // groups per block when one warp searches for a group
+constexpr int NBR_SPLIT = 3;        // warps per group in the split search (one stencil x-slab each)
+constexpr int NBR_SPLIT_STAGE = 2048;  // hits a split warp stages in shared memory (G atoms together)
+// Launches with fewer groups than this take the split search (4-atom groups): half of what one
+// wave holds at 24 resident warps per SM on 148 SMs. Measured on one B200: a 2,854-atom box
+// (~800 groups) rebuilds in 0.117 ms split; a 23,558-atom box (~6,000 groups) took 0.315 ms
+// split against 0.221 ms with a warp a group.
+constexpr int NBR_SPLIT_GROUPS_MAX = 148 * 24 / 2;
 
 // One WARP per search group of G atoms of one cell, taken in sub-cell order so the group is
 // spatially compact; lane l works for the group's atom l / J on candidate sub-lane l % J
@@ -231,8 +238,16 @@ constexpr int NBR_WARPS = 4;
 // exact-rounding test of the reference's WGSL on the original coordinates, so rows are
 // bit-identical to the reference's. An entry is the partner's cell-ordered slot with the
 // code of the lattice shift to its nearest image.
-template <int G>
-__global__ void __launch_bounds__(32 * NBR_WARPS)
+//
+// SPLIT = 3 (4-atom groups in small launches): a block of three warps per group, warp w walking the
+// stencil's x-slab w (nine cells) and staging its hits per atom in shared memory; after a
+// block barrier each warp copies its hits to the rows behind those of the slabs before it,
+// so the rows are the same as one warp's. A group is then three short serial chains instead
+// of one long one, which fills the SMs when there are few groups. If a warp's hits overflow its
+// staging (512 per atom: a very dense neighbourhood) the first warp walks the whole stencil
+// again and writes the rows directly.
+template <int G, int SPLIT>
+__global__ void __launch_bounds__(SPLIT == 1 ? 32 * NBR_WARPS : 32 * SPLIT)
     k_neighbours(const float4 *__restrict__ posq, const int *__restrict__ group_sys,
                  const DevSys *__restrict__ sys, const int *__restrict__ cell_start,
                  const int *__restrict__ cell_gstart, const int *__restrict__ group_order,
@@ -241,12 +256,18 @@ __global__ void __launch_bounds__(32 * NBR_WARPS)
                  int *__restrict__ nbr, int *__restrict__ nbr_count, int *__restrict__ required,
                  float4 *__restrict__ origin, int n_groups, const int *__restrict__ only) {
   constexpr int J = 32 / G;
-  __shared__ float4 stage_pos[NBR_WARPS][32];
-  __shared__ int stage_orig[NBR_WARPS][32];
+  constexpr int WARPS = SPLIT == 1 ? NBR_WARPS : SPLIT;
+  constexpr int HITS = NBR_SPLIT_STAGE / G;  // staged hits per atom per split warp
+  __shared__ float4 stage_pos[WARPS][32];
+  __shared__ int stage_orig[WARPS][32];
+  __shared__ int split_hits[SPLIT == 1 ? 1 : SPLIT * NBR_SPLIT_STAGE];
+  __shared__ int split_found[SPLIT][G];
   const int wib = threadIdx.x >> 5;
-  const int warp = blockIdx.x * NBR_WARPS + wib;
+  const int warp = SPLIT == 1 ? blockIdx.x * NBR_WARPS + wib : blockIdx.x;  // the group
   const int lane = threadIdx.x & 31;
   const int a = lane / J, sub = lane % J;
+  // (every exit before the split search's barrier depends on the group alone, so the three
+  // warps of a split block leave together)
   if (warp >= n_groups) return;
   const int sidx = group_sys[warp];
   if (only && !only[sidx]) return;  // this system's lists are still valid
@@ -270,7 +291,7 @@ __global__ void __launch_bounds__(32 * NBR_WARPS)
   const int si = valid ? group_order[k] : -1;
   const int i = valid ? sorted_orig[si] : 0;
   const float4 pw = valid ? spos[si] : make_float4(0.f, 0.f, 0.f, 0.f);
-  if (valid && sub == 0) origin[i] = posq[i];  // displacement origin for the skin check
+  if (valid && sub == 0 && (SPLIT == 1 || wib == 0)) origin[i] = posq[i];  // skin check origin
   // exclusions of this lane's atom: sorted partners; the range check skips the search
   const int e_lo = valid ? excl_start[i] : 0, e_hi = valid ? excl_start[i + 1] : 0;
   const int p_min = e_lo < e_hi ? excl_partners[e_lo] : INT_MAX;
@@ -307,12 +328,15 @@ __global__ void __launch_bounds__(32 * NBR_WARPS)
   const float band_hi = lc2 * 1.00004f, band_lo = lc2 * 0.99996f, cull2 = band_hi * 1.0001f;
   const int cap = s.nbr_capacity;
   int *row = nbr + s.nbr_base + (long long)(valid ? si - s.atom_start : 0) * cap;
-  int found = 0;
   const unsigned seg_mask = J == 32 ? 0xffffffffu : ((1u << J) - 1u);
   const unsigned below = (1u << sub) - 1u;
   float4 *st_pos = stage_pos[wib];
   int *st_orig = stage_orig[wib];
-  for (int ox = 0; ox < count[0]; ++ox) {
+  // Walk the stencil's x-slabs [ox_begin, ox_end), appending this lane's atom's hits to
+  // dst[0 .. dst_cap); returns the atom's hit count (which may exceed dst_cap).
+  auto walk = [&](int ox_begin, int ox_end, int *dst, int dst_cap) -> int {
+  int found = 0;
+  for (int ox = ox_begin; ox < ox_end; ++ox) {
     const int rx = cc[0] + base[0] + ox;
     const int wx = rx < 0 ? -1 : (rx >= counts[0] ? 1 : 0);
     const int cx = rx - wx * counts[0];
@@ -418,7 +442,7 @@ __global__ void __launch_bounds__(32 * NBR_WARPS)
             const unsigned hits = (__ballot_sync(0xffffffffu, in) >> (a * J)) & seg_mask;
             if (in) {
               const int pos = found + __popc(hits & below);
-              if (pos < cap) row[pos] = entry;
+              if (pos < dst_cap) dst[pos] = entry;
             }
             found += __popc(hits);
           }
@@ -427,6 +451,52 @@ __global__ void __launch_bounds__(32 * NBR_WARPS)
       }
     }
   }
+  return found;
+  };
+  // One call site of the walk (a loop rather than two calls, so that it is inlined): the
+  // one-warp search walks every slab into the rows; a split warp walks its slab into shared
+  // memory and, only if some warp's staging overflowed, warp 0 walks again into the rows.
+  int *staged = split_hits + (SPLIT == 1 ? 0 : wib * NBR_SPLIT_STAGE);
+  int ox_begin = SPLIT == 1 ? 0 : min(wib, count[0]);
+  int ox_end = SPLIT == 1 ? count[0] : min(wib + 1, count[0]);
+  int *dst = SPLIT == 1 ? row : staged + a * HITS;
+  int dst_cap = SPLIT == 1 ? cap : HITS;
+  int found = 0;
+  for (int pass = 0;; ++pass) {
+    found = walk(ox_begin, ox_end, dst, dst_cap);
+    if (SPLIT == 1 || pass > 0) break;
+    if (sub == 0) split_found[wib][a] = valid ? found : 0;
+    __syncthreads();
+    bool spill = false;
+    found = 0;
+#pragma unroll
+    for (int w = 0; w < SPLIT; ++w) {
+      found += split_found[w][a];
+#pragma unroll
+      for (int b = 0; b < G; ++b) spill |= split_found[w][b] > HITS;
+    }
+    if (!spill) {
+      // this warp's staged hits of each atom, behind the earlier slabs' hits of that atom
+      for (int b = 0; b < G; ++b) {
+        const int n = split_found[wib][b];
+        const int sb = __shfl_sync(0xffffffffu, si, b * J);
+        if (n == 0) continue;  // (also every atom past the end of the cell)
+        int off = 0;
+        for (int w = 0; w < wib; ++w) off += split_found[w][b];
+        int *rb = nbr + s.nbr_base + (long long)(sb - s.atom_start) * cap;
+        const int *src = staged + b * HITS;
+        for (int k = lane; k < n; k += 32)
+          if (off + k < cap) rb[off + k] = src[k];
+      }
+      break;
+    }
+    if (wib != 0) break;
+    ox_begin = 0;
+    ox_end = count[0];
+    dst = row;
+    dst_cap = cap;
+  }
+  if (SPLIT > 1 && wib != 0) return;
   if (valid && sub == 0) nbr_count[si] = min(found, cap);
   int most = valid ? found : 0;
 #pragma unroll
@@ -510,14 +580,18 @@ void launch_rebuild(const LaunchCtx &ctx, cudaStream_t stream) {
   ctx.posq, ctx.group_sys, ctx.sys, ctx.cell_start, ctx.cell_gstart, ctx.group_order, ctx.excl_start,  \
       ctx.excl_partners, ctx.spos, ctx.sorted_orig, ctx.nbr, ctx.nbr_count, ctx.required, ctx.origin, \
       ctx.n_groups_total, only
-  if (G == 4)
-    k_neighbours<4><<<blocks, 32 * NBR_WARPS, 0, stream>>>(RMD_NBR_ARGS);
+  // 4-atom groups too few to fill the GPU with one warp each (a box of a few thousand atoms)
+  // search three warps a group; otherwise one warp a group keeps more groups resident
+  if (G == 4 && ctx.n_groups_total < NBR_SPLIT_GROUPS_MAX)
+    k_neighbours<4, NBR_SPLIT><<<ctx.n_groups_total, 32 * NBR_SPLIT, 0, stream>>>(RMD_NBR_ARGS);
+  else if (G == 4)
+    k_neighbours<4, 1><<<blocks, 32 * NBR_WARPS, 0, stream>>>(RMD_NBR_ARGS);
   else if (G == 8)
-    k_neighbours<8><<<blocks, 32 * NBR_WARPS, 0, stream>>>(RMD_NBR_ARGS);
+    k_neighbours<8, 1><<<blocks, 32 * NBR_WARPS, 0, stream>>>(RMD_NBR_ARGS);
   else if (G == 16)
-    k_neighbours<16><<<blocks, 32 * NBR_WARPS, 0, stream>>>(RMD_NBR_ARGS);
+    k_neighbours<16, 1><<<blocks, 32 * NBR_WARPS, 0, stream>>>(RMD_NBR_ARGS);
   else
-    k_neighbours<32><<<blocks, 32 * NBR_WARPS, 0, stream>>>(RMD_NBR_ARGS);
+    k_neighbours<32, 1><<<blocks, 32 * NBR_WARPS, 0, stream>>>(RMD_NBR_ARGS);
 #undef RMD_NBR_ARGS
 }
 
