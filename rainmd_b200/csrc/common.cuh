@@ -71,6 +71,34 @@ struct DevSysD {
   int pad0;
 };
 
+// ---------------------------------------------------- programmatic dependent launch
+// The kernels of the step's serial chains (integrator, spreading, FFT passes, gather) are
+// launched with programmatic stream serialisation (launch_chained): a kernel's blocks may be
+// scheduled while its predecessor in the stream is still running, which hides the launch
+// latency between short dependent kernels. Such a kernel must start with chain_begin(): it
+// waits until every predecessor grid has completed and its memory is visible, before any
+// memory access, then lets its own successor be scheduled. In a plain launch both are no-ops.
+__device__ __forceinline__ void chain_begin() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+template <typename... KernelArgs, typename... Args>
+inline void launch_chained(void (*kernel)(KernelArgs...), dim3 grid, dim3 block, size_t smem,
+                           cudaStream_t stream, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = stream;
+  cudaLaunchAttribute attr;
+  attr.id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr.val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = &attr;
+  cfg.numAttrs = 1;
+  (void)cudaLaunchKernelEx(&cfg, kernel, static_cast<KernelArgs>(args)...);  // errors surface in cudaGetLastError
+}
+
 // ---------------------------------------------------------------- fixed point
 __device__ __forceinline__ unsigned long long to_fixed(float v) {
   return (unsigned long long)__float2ll_rn(v * FORCE_SCALE_F);

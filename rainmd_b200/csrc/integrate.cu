@@ -443,6 +443,7 @@ __device__ __forceinline__ void process_unit(const IntegrateArgs &g, int index, 
 
 template <int MODE>
 __global__ void __launch_bounds__(64) k_integrate(IntegrateArgs g) {
+  chain_begin();
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int lane = threadIdx.x & 31;
   const bool active = t < g.n_units;
@@ -486,19 +487,18 @@ __global__ void __launch_bounds__(64) k_integrate(IntegrateArgs g) {
 void launch_integrate(const IntegrateArgs &a, int mode, cudaStream_t stream) {
   if (a.n_units == 0) return;
   const int tb = 64, blocks = (a.n_units + tb - 1) / tb;
+  void (*kernel)(IntegrateArgs);
   switch (mode) {
-    case INT_OPEN: k_integrate<INT_OPEN><<<blocks, tb, 0, stream>>>(a); break;
-    case INT_OPEN | INT_OPEN_KINETIC:
-      k_integrate<INT_OPEN | INT_OPEN_KINETIC><<<blocks, tb, 0, stream>>>(a); break;
-    case INT_CLOSE | INT_OPEN: k_integrate<INT_CLOSE | INT_OPEN><<<blocks, tb, 0, stream>>>(a); break;
-    case INT_CLOSE | INT_OPEN | INT_OPEN_KINETIC:
-      k_integrate<INT_CLOSE | INT_OPEN | INT_OPEN_KINETIC><<<blocks, tb, 0, stream>>>(a); break;
-    case INT_CLOSE: k_integrate<INT_CLOSE><<<blocks, tb, 0, stream>>>(a); break;
-    case INT_CLOSE | INT_CLOSE_KINETIC:
-      k_integrate<INT_CLOSE | INT_CLOSE_KINETIC><<<blocks, tb, 0, stream>>>(a); break;
-    case INT_CONSTRAIN: k_integrate<INT_CONSTRAIN><<<blocks, tb, 0, stream>>>(a); break;
-    default: k_integrate<INT_CLOSE_KINETIC><<<blocks, tb, 0, stream>>>(a); break;
+    case INT_OPEN: kernel = k_integrate<INT_OPEN>; break;
+    case INT_OPEN | INT_OPEN_KINETIC: kernel = k_integrate<INT_OPEN | INT_OPEN_KINETIC>; break;
+    case INT_CLOSE | INT_OPEN: kernel = k_integrate<INT_CLOSE | INT_OPEN>; break;
+    case INT_CLOSE | INT_OPEN | INT_OPEN_KINETIC: kernel = k_integrate<INT_CLOSE | INT_OPEN | INT_OPEN_KINETIC>; break;
+    case INT_CLOSE: kernel = k_integrate<INT_CLOSE>; break;
+    case INT_CLOSE | INT_CLOSE_KINETIC: kernel = k_integrate<INT_CLOSE | INT_CLOSE_KINETIC>; break;
+    case INT_CONSTRAIN: kernel = k_integrate<INT_CONSTRAIN>; break;
+    default: kernel = k_integrate<INT_CLOSE_KINETIC>; break;
   }
+  launch_chained(kernel, blocks, tb, 0, stream, a);
 }
 
 }  // namespace rmd

@@ -156,6 +156,7 @@ template <int ORDER>
 __global__ void k_spread(const float4 *__restrict__ posq, const int *__restrict__ sys_of_atom,
                          const DevSys *__restrict__ sys, unsigned long long *__restrict__ fixed_grid,
                          int n_atoms) {
+  chain_begin();
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const int i = (int)(t / (ORDER * ORDER));
   if (i >= n_atoms) return;
@@ -198,6 +199,7 @@ __global__ void __launch_bounds__(256) k_fft_z_r2c(const FftTask *__restrict__ t
                                                    const float2 *__restrict__ twiddles,
                                                    unsigned long long *__restrict__ fixed_grid,
                                                    float2 *__restrict__ half) {
+  chain_begin();
   __shared__ float2 bufa[FFT_SMEM], bufb[FFT_SMEM];
   const FftTask t = tasks[blockIdx.x];
   const DevSys &s = sys[t.sys];
@@ -240,6 +242,7 @@ __global__ void __launch_bounds__(256) k_fft_z_c2r(const FftTask *__restrict__ t
                                                    const float2 *__restrict__ twiddles,
                                                    const float2 *__restrict__ half,
                                                    float *__restrict__ real_grid) {
+  chain_begin();
   __shared__ float2 bufa[FFT_SMEM], bufb[FFT_SMEM];
   const FftTask t = tasks[blockIdx.x];
   const DevSys &s = sys[t.sys];
@@ -285,6 +288,7 @@ __global__ void __launch_bounds__(256) k_fft_y(const FftTask *__restrict__ tasks
                                                const FftPlan *__restrict__ plans,
                                                const float2 *__restrict__ twiddles,
                                                float2 *__restrict__ half, int inverse) {
+  chain_begin();
   __shared__ float2 bufa[FFT_SMEM], bufb[FFT_SMEM];
   const FftTask t = tasks[blockIdx.x];
   const DevSys &s = sys[t.sys];
@@ -315,6 +319,7 @@ __global__ void __launch_bounds__(256) k_fft_x_convolve(const FftTask *__restric
                                                         float2 *__restrict__ half,
                                                         double *__restrict__ e_pme,
                                                         double *__restrict__ e_pme_vir) {
+  chain_begin();
   __shared__ float2 bufa[FFT_SMEM], bufb[FFT_SMEM];
   __shared__ double red[2][256 / 32];
   const FftTask t = tasks[blockIdx.x];
@@ -444,6 +449,7 @@ __global__ void k_gather4(const float4 *__restrict__ posq, const int *__restrict
                           const int *__restrict__ sys_of_atom, const DevSys *__restrict__ sys,
                           const float *__restrict__ real_grid, unsigned long long *__restrict__ force,
                           int n_atoms) {
+  chain_begin();
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int slot = t >> 2, q = t & 3;
   const bool valid = slot < n_atoms;
@@ -510,24 +516,24 @@ static void launch_gather(const LaunchCtx &c, cudaStream_t stream) {
   const int n = c.n_atoms, tb = 128;
   const int blocks = (int)(((long long)n * 4 + tb - 1) / tb);
   if (c.pme_order == 4)
-    k_gather4<4><<<blocks, tb, 0, stream>>>(c.posq, c.sorted_orig, c.sys_of_atom, c.sys, c.real_grid, c.force, n);
+    launch_chained(k_gather4<4>, blocks, tb, 0, stream, c.posq, c.sorted_orig, c.sys_of_atom, c.sys, c.real_grid, c.force, n);
   else
-    k_gather4<5><<<blocks, tb, 0, stream>>>(c.posq, c.sorted_orig, c.sys_of_atom, c.sys, c.real_grid, c.force, n);
+    launch_chained(k_gather4<5>, blocks, tb, 0, stream, c.posq, c.sorted_orig, c.sys_of_atom, c.sys, c.real_grid, c.force, n);
 }
 
 // Forward transform of the spread grid to the half spectrum (z and y; x is left to the caller).
 static void launch_forward_zy(const LaunchCtx &c, cudaStream_t stream, bool all = false) {
-  k_fft_z_r2c<<<c.n_tasks_z, 256, 0, stream>>>(c.tasks_z, c.sys, c.fft_plans, c.twiddles, c.fixed_grid, c.half);
+  launch_chained(k_fft_z_r2c, c.n_tasks_z, 256, 0, stream, c.tasks_z, c.sys, c.fft_plans, c.twiddles, c.fixed_grid, c.half);
   const FftTask *ty = all ? c.tasks_y_all : c.tasks_y;
   const int n = all ? c.n_tasks_y_all : c.n_tasks_y;
-  if (n > 0) k_fft_y<<<n, 256, 0, stream>>>(ty, c.sys, c.fft_plans, c.twiddles, c.half, 0);
+  if (n > 0) launch_chained(k_fft_y, n, 256, 0, stream, ty, c.sys, c.fft_plans, c.twiddles, c.half, 0);
 }
 
 static void launch_inverse_yz(const LaunchCtx &c, cudaStream_t stream, bool all = false) {
   const FftTask *ty = all ? c.tasks_y_all : c.tasks_y;
   const int n = all ? c.n_tasks_y_all : c.n_tasks_y;
-  if (n > 0) k_fft_y<<<n, 256, 0, stream>>>(ty, c.sys, c.fft_plans, c.twiddles, c.half, 1);
-  k_fft_z_c2r<<<c.n_tasks_z, 256, 0, stream>>>(c.tasks_z, c.sys, c.fft_plans, c.twiddles, c.half, c.real_grid);
+  if (n > 0) launch_chained(k_fft_y, n, 256, 0, stream, ty, c.sys, c.fft_plans, c.twiddles, c.half, 1);
+  launch_chained(k_fft_z_c2r, c.n_tasks_z, 256, 0, stream, c.tasks_z, c.sys, c.fft_plans, c.twiddles, c.half, c.real_grid);
 }
 
 // A plane pass's per-axis tables in shared memory: the y and x twiddles and B-spline moduli,
@@ -620,6 +626,7 @@ __global__ void __launch_bounds__(256) k_fft_plane(const FftTask *__restrict__ t
                                                    const float *__restrict__ moduli,
                                                    float2 *__restrict__ half, int plane_stride,
                                                    double *__restrict__ e_pme, double *__restrict__ e_pme_vir) {
+  chain_begin();
   extern __shared__ float2 plane_smem[];
   __shared__ PlaneTables tab;
   float2 *bufa = plane_smem, *bufb = plane_smem + plane_stride;
@@ -687,6 +694,7 @@ __global__ void __cluster_dims__(PLANE_CLUSTER, 1, 1) __launch_bounds__(256)
                         const float2 *__restrict__ twiddles, const float *__restrict__ moduli,
                         float2 *__restrict__ half, int row_stride, int col_stride,
                         double *__restrict__ e_pme, double *__restrict__ e_pme_vir) {
+  chain_begin();
   cg::cluster_group cluster = cg::this_cluster();
   const int rank = (int)cluster.block_rank();
   extern __shared__ float2 plane_smem[];
@@ -798,26 +806,16 @@ static void launch_planes(const LaunchCtx &c, bool energy, cudaStream_t stream) 
   double *e = c.e_pme + c.n_tasks_x, *ev = c.e_pme_vir + c.n_tasks_x;
   if (c.n_tasks_plane > 0) {
     const size_t smem = 2 * (size_t)c.plane_stride * sizeof(float2);
-    if (energy)
-      k_fft_plane<true><<<c.n_tasks_plane, 256, smem, stream>>>(c.tasks_plane, c.sys, c.sysd, c.fft_plans,
-                                                               c.twiddles, c.moduli, c.half, c.plane_stride, e, ev);
-    else
-      k_fft_plane<false><<<c.n_tasks_plane, 256, smem, stream>>>(c.tasks_plane, c.sys, c.sysd, c.fft_plans,
-                                                                c.twiddles, c.moduli, c.half, c.plane_stride, e, ev);
+    launch_chained(energy ? k_fft_plane<true> : k_fft_plane<false>, c.n_tasks_plane, 256, smem, stream,
+                   c.tasks_plane, c.sys, c.sysd, c.fft_plans, c.twiddles, c.moduli, c.half, c.plane_stride, e, ev);
   }
   if (c.n_tasks_cluster > 0) {
     e += c.n_tasks_plane;
     ev += c.n_tasks_plane;
     const size_t smem = 2 * ((size_t)c.cluster_rows + c.cluster_cols) * sizeof(float2);
-    const int blocks = c.n_tasks_cluster * PLANE_CLUSTER;
-    if (energy)
-      k_fft_plane_cluster<true><<<blocks, 256, smem, stream>>>(c.tasks_cluster, c.sys, c.sysd, c.fft_plans,
-                                                              c.twiddles, c.moduli, c.half, c.cluster_rows,
-                                                              c.cluster_cols, e, ev);
-    else
-      k_fft_plane_cluster<false><<<blocks, 256, smem, stream>>>(c.tasks_cluster, c.sys, c.sysd, c.fft_plans,
-                                                               c.twiddles, c.moduli, c.half, c.cluster_rows,
-                                                               c.cluster_cols, e, ev);
+    launch_chained(energy ? k_fft_plane_cluster<true> : k_fft_plane_cluster<false>, c.n_tasks_cluster * PLANE_CLUSTER,
+                   256, smem, stream, c.tasks_cluster, c.sys, c.sysd, c.fft_plans, c.twiddles, c.moduli, c.half,
+                   c.cluster_rows, c.cluster_cols, e, ev);
   }
 }
 
@@ -831,16 +829,9 @@ int pme_launches(const LaunchCtx &c) {
 static void launch_transform_convolve(const LaunchCtx &c, bool energy, cudaStream_t stream) {
   launch_forward_zy(c, stream);
   launch_planes(c, energy, stream);
-  if (c.n_tasks_x > 0) {
-    if (energy)
-      k_fft_x_convolve<true><<<c.n_tasks_x, 256, 0, stream>>>(c.tasks_x, c.sys, c.sysd, c.fft_plans,
-                                                              c.twiddles, c.moduli, c.half, c.e_pme,
-                                                              c.e_pme_vir);
-    else
-      k_fft_x_convolve<false><<<c.n_tasks_x, 256, 0, stream>>>(c.tasks_x, c.sys, c.sysd, c.fft_plans,
-                                                               c.twiddles, c.moduli, c.half, c.e_pme,
-                                                               c.e_pme_vir);
-  }
+  if (c.n_tasks_x > 0)
+    launch_chained(energy ? k_fft_x_convolve<true> : k_fft_x_convolve<false>, c.n_tasks_x, 256, 0, stream,
+                   c.tasks_x, c.sys, c.sysd, c.fft_plans, c.twiddles, c.moduli, c.half, c.e_pme, c.e_pme_vir);
   launch_inverse_yz(c, stream);
 }
 
@@ -892,9 +883,9 @@ void launch_spread_only(const LaunchCtx &c, cudaStream_t stream) {
   const int per_block = c.spread_atoms > 0 ? c.spread_atoms : 8;
   const int blocks = (n + per_block - 1) / per_block;
   if (c.pme_order == 4)
-    k_spread<4><<<blocks, per_block * 16, 0, stream>>>(c.posq, c.sys_of_atom, c.sys, c.fixed_grid, n);
+    launch_chained(k_spread<4>, blocks, per_block * 16, 0, stream, c.posq, c.sys_of_atom, c.sys, c.fixed_grid, n);
   else
-    k_spread<5><<<blocks, per_block * 25, 0, stream>>>(c.posq, c.sys_of_atom, c.sys, c.fixed_grid, n);
+    launch_chained(k_spread<5>, blocks, per_block * 25, 0, stream, c.posq, c.sys_of_atom, c.sys, c.fixed_grid, n);
 }
 
 // (the debug transforms run the separate passes over every system)
