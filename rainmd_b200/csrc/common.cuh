@@ -84,8 +84,8 @@ __device__ __forceinline__ void chain_begin() {
 }
 
 template <typename... KernelArgs, typename... Args>
-inline void launch_chained(void (*kernel)(KernelArgs...), dim3 grid, dim3 block, size_t smem,
-                           cudaStream_t stream, Args... args) {
+inline void launch_kernel(bool chained, void (*kernel)(KernelArgs...), dim3 grid, dim3 block, size_t smem,
+                          cudaStream_t stream, Args... args) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = grid;
   cfg.blockDim = block;
@@ -95,8 +95,14 @@ inline void launch_chained(void (*kernel)(KernelArgs...), dim3 grid, dim3 block,
   attr.id = cudaLaunchAttributeProgrammaticStreamSerialization;
   attr.val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = &attr;
-  cfg.numAttrs = 1;
+  cfg.numAttrs = chained ? 1 : 0;
   (void)cudaLaunchKernelEx(&cfg, kernel, static_cast<KernelArgs>(args)...);  // errors surface in cudaGetLastError
+}
+
+template <typename... KernelArgs, typename... Args>
+inline void launch_chained(void (*kernel)(KernelArgs...), dim3 grid, dim3 block, size_t smem,
+                           cudaStream_t stream, Args... args) {
+  launch_kernel(true, kernel, grid, block, smem, stream, args...);
 }
 
 // ---------------------------------------------------------------- fixed point

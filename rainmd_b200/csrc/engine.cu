@@ -1137,6 +1137,7 @@ void Engine::allocate_neighbours() {
 
 LaunchCtx Engine::ctx() const {
   LaunchCtx c{};
+  c.chain_pme = on_demand ? 1 : 0;
   c.n_atoms = N;
   c.n_systems = S;
   c.posq = posq.p;

@@ -530,14 +530,15 @@ static void launch_forward_zy(const LaunchCtx &c, cudaStream_t stream, bool all 
   k_fft_z_r2c<<<c.n_tasks_z, 256, 0, stream>>>(c.tasks_z, c.sys, c.fft_plans, c.twiddles, c.fixed_grid, c.half);
   const FftTask *ty = all ? c.tasks_y_all : c.tasks_y;
   const int n = all ? c.n_tasks_y_all : c.n_tasks_y;
-  if (n > 0) launch_chained(k_fft_y, n, 256, 0, stream, ty, c.sys, c.fft_plans, c.twiddles, c.half, 0);
+  if (n > 0) launch_kernel(c.chain_pme, k_fft_y, n, 256, 0, stream, ty, c.sys, c.fft_plans, c.twiddles, c.half, 0);
 }
 
 static void launch_inverse_yz(const LaunchCtx &c, cudaStream_t stream, bool all = false) {
   const FftTask *ty = all ? c.tasks_y_all : c.tasks_y;
   const int n = all ? c.n_tasks_y_all : c.n_tasks_y;
-  if (n > 0) launch_chained(k_fft_y, n, 256, 0, stream, ty, c.sys, c.fft_plans, c.twiddles, c.half, 1);
-  launch_chained(k_fft_z_c2r, c.n_tasks_z, 256, 0, stream, c.tasks_z, c.sys, c.fft_plans, c.twiddles, c.half, c.real_grid);
+  if (n > 0) launch_kernel(c.chain_pme, k_fft_y, n, 256, 0, stream, ty, c.sys, c.fft_plans, c.twiddles, c.half, 1);
+  launch_kernel(c.chain_pme, k_fft_z_c2r, c.n_tasks_z, 256, 0, stream, c.tasks_z, c.sys, c.fft_plans, c.twiddles, c.half,
+                c.real_grid);
 }
 
 // A plane pass's per-axis tables in shared memory: the y and x twiddles and B-spline moduli,
@@ -810,14 +811,15 @@ static void launch_planes(const LaunchCtx &c, bool energy, cudaStream_t stream) 
   double *e = c.e_pme + c.n_tasks_x, *ev = c.e_pme_vir + c.n_tasks_x;
   if (c.n_tasks_plane > 0) {
     const size_t smem = 2 * (size_t)c.plane_stride * sizeof(float2);
-    launch_chained(energy ? k_fft_plane<true> : k_fft_plane<false>, c.n_tasks_plane, 256, smem, stream,
+    launch_kernel(c.chain_pme, energy ? k_fft_plane<true> : k_fft_plane<false>, c.n_tasks_plane, 256, smem, stream,
                    c.tasks_plane, c.sys, c.sysd, c.fft_plans, c.twiddles, c.moduli, c.half, c.plane_stride, e, ev);
   }
   if (c.n_tasks_cluster > 0) {
     e += c.n_tasks_plane;
     ev += c.n_tasks_plane;
     const size_t smem = 2 * ((size_t)c.cluster_rows + c.cluster_cols) * sizeof(float2);
-    launch_chained(energy ? k_fft_plane_cluster<true> : k_fft_plane_cluster<false>, c.n_tasks_cluster * PLANE_CLUSTER,
+    launch_kernel(c.chain_pme, energy ? k_fft_plane_cluster<true> : k_fft_plane_cluster<false>,
+                  c.n_tasks_cluster * PLANE_CLUSTER,
                    256, smem, stream, c.tasks_cluster, c.sys, c.sysd, c.fft_plans, c.twiddles, c.moduli, c.half,
                    c.cluster_rows, c.cluster_cols, e, ev);
   }
@@ -834,7 +836,7 @@ static void launch_transform_convolve(const LaunchCtx &c, bool energy, cudaStrea
   launch_forward_zy(c, stream);
   launch_planes(c, energy, stream);
   if (c.n_tasks_x > 0)
-    launch_chained(energy ? k_fft_x_convolve<true> : k_fft_x_convolve<false>, c.n_tasks_x, 256, 0, stream,
+    launch_kernel(c.chain_pme, energy ? k_fft_x_convolve<true> : k_fft_x_convolve<false>, c.n_tasks_x, 256, 0, stream,
                    c.tasks_x, c.sys, c.sysd, c.fft_plans, c.twiddles, c.moduli, c.half, c.e_pme, c.e_pme_vir);
   launch_inverse_yz(c, stream);
 }
@@ -887,9 +889,11 @@ void launch_spread_only(const LaunchCtx &c, cudaStream_t stream) {
   const int per_block = c.spread_atoms > 0 ? c.spread_atoms : 8;
   const int blocks = (n + per_block - 1) / per_block;
   if (c.pme_order == 4)
-    launch_chained(k_spread<4>, blocks, per_block * 16, 0, stream, c.posq, c.sys_of_atom, c.sys, c.fixed_grid, n);
+    launch_kernel(c.chain_pme, k_spread<4>, blocks, per_block * 16, 0, stream, c.posq, c.sys_of_atom, c.sys,
+                  c.fixed_grid, n);
   else
-    launch_chained(k_spread<5>, blocks, per_block * 25, 0, stream, c.posq, c.sys_of_atom, c.sys, c.fixed_grid, n);
+    launch_kernel(c.chain_pme, k_spread<5>, blocks, per_block * 25, 0, stream, c.posq, c.sys_of_atom, c.sys,
+                  c.fixed_grid, n);
 }
 
 // (the debug transforms run the separate passes over every system)
