@@ -764,10 +764,9 @@ __global__ void __cluster_dims__(PLANE_CLUSTER, 1, 1) __launch_bounds__(256)
 // chain, so larger grids run faster shared by a cluster: measured on one B200 (the seven
 // reciprocal kernels) one block a plane is faster than the separate passes at 32^3 (0.037
 // against 0.041 ms) and for 64 grids of 22^3-50^3 together (0.30 against 0.34 ms), slower at
-// 64^3 (0.071 against 0.056 ms) and 100^3 (0.194 against 0.152 ms).
-#ifndef PLANE_SINGLE_MAX
-#define PLANE_SINGLE_MAX (52 * 52)
-#endif
+// 64^3 (0.071 against 0.056 ms) and 100^3 (0.194 against 0.152 ms). A cluster a plane for
+// those 64 small grids too was slower again (0.375 ms): their 1,150 planes fill the GPU already.
+constexpr long long PLANE_SINGLE_MAX = 52 * 52;
 
 void fft_plane_buffers(int nx, int ny, int split, int *rows, int *cols) {
   if (split == 1) {
