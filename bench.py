@@ -661,8 +661,8 @@ def main():
                      "algorithmic_bytes": bytes_nb, "unique_pairs_within_cutoff": pairs,
                      "ms_per_launch": nb_ms},
         "kernels_ms": {"nonbonded": nb_ms, "nonbonded_per_lane_f32": nb_plain_ms,
-                       "pme_7_kernels": pme_ms, "integrate": integ_ms,
-                       "rebuild_5_kernels": rebuild_ms,
+                       "pme_kernels": pme_ms, "integrate": integ_ms,
+                       "rebuild_kernels": rebuild_ms,
                        "pme_roofline_frac": bytes_pme / (pme_ms * 1e-3) / 1e9 / peak},
         "kernel_shapes": {k: shapes[k] for k in ("neighbourGroupAtoms", "nonbondedLanes", "spreadAtomsPerBlock")},
         "autotune_ms": shapes["tuned"],
