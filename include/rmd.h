@@ -287,10 +287,15 @@ rmd_status rmd_debug_charge_grid(rmd_sim *sim, int32_t system_index, double *gri
 rmd_status rmd_debug_fft(rmd_sim *sim, int32_t system_index, const double *data,
                          double *half_spectrum, double *round_trip);
 
+/* How the reciprocal-space FFT transforms the y and x axes of an nx x ny grid plane: 1 = the
+ * fused y-x-convolve-x-y pass with one thread block a kz plane, 4 = the same pass with a
+ * 4-block thread-block cluster a plane, 0 = separate y and x passes. A host-side rule that
+ * depends on the grid alone (no device call); no reference counterpart. */
+int32_t rmd_debug_plane_pass(int32_t nx, int32_t ny);
 /* Average device time of one launch of a kernel group on the engine's own stream, by CUDA
- * events over `reps` back-to-back launches: 0 nonbonded (no energy), 1 the seven PME
- * kernels, 2 the fused integrator, 3 bonded, 4 the five list-rebuild kernels, 5 nonbonded
- * with energies. Positions and velocities are put back afterwards and the forces
+ * events over `reps` back-to-back launches: 0 nonbonded (no energy), 1 the PME kernels
+ * (five to seven, by grid), 2 the fused integrator, 3 bonded, 4 the list-rebuild kernels,
+ * 5 nonbonded with energies. Positions and velocities are put back afterwards and the forces
  * re-evaluated, so the simulation continues from where it was. For roofline measurement;
  * no reference counterpart. */
 rmd_status rmd_debug_time_kernel(rmd_sim *sim, int32_t which, int32_t reps, double *ms_per_launch);

@@ -127,7 +127,7 @@ EXPORTS = [
     "rmd_energy", "rmd_energy_at", "rmd_read_positions", "rmd_read_state", "rmd_read_state_at",
     "rmd_diagnostics", "rmd_diagnostics_at", "rmd_destroy", "rmd_last_error", "rmd_debug_cells",
     "rmd_debug_neighbours", "rmd_debug_evaluate", "rmd_debug_charge_grid", "rmd_debug_fft",
-    "rmd_debug_time_kernel", "rmd_debug_kernel_launches", "rmd_debug_set_nonbonded",
+    "rmd_debug_time_kernel", "rmd_debug_kernel_launches", "rmd_debug_set_nonbonded", "rmd_debug_plane_pass",
     "rmd_bench_run", "rmd_debug_force_term", "rmd_debug_read", "rmd_spread_charges_noalloc",
     "rmd_kernel_shapes", "rmd_set_kernel_shapes", "rmd_surrogate_report_at", "rmd_surrogate_weights",
     "rmd_surrogate_evaluate", "rmd_image_molecules_at", "rmd_dcd_frame_bytes", "rmd_dcd_frame_at",
@@ -187,6 +187,8 @@ def load():
     lib.rmd_debug_time_kernel.argtypes = [sim, C.c_int32, C.c_int32, _dp]
     lib.rmd_debug_kernel_launches.argtypes = [sim]
     lib.rmd_debug_kernel_launches.restype = C.c_int64
+    lib.rmd_debug_plane_pass.argtypes = [C.c_int32, C.c_int32]
+    lib.rmd_debug_plane_pass.restype = C.c_int32
     lib.rmd_debug_set_nonbonded.argtypes = [sim, C.c_int32, C.c_int32]
     lib.rmd_kernel_shapes.argtypes = [sim, _i32p, _dp]
     lib.rmd_set_kernel_shapes.argtypes = [sim, C.c_int32, C.c_int32, C.c_int32]

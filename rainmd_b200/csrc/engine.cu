@@ -2548,6 +2548,10 @@ rmd_status rmd_debug_time_kernel(rmd_sim *sim, int32_t which, int32_t reps, doub
 
 int64_t rmd_debug_kernel_launches(const rmd_sim *sim) { return sim ? sim->engine.kernel_launches : 0; }
 
+int32_t rmd_debug_plane_pass(int32_t nx, int32_t ny) {
+  return nx > 0 && ny > 0 ? rmd::fft_plane_split(nx, ny) : 0;
+}
+
 rmd_status rmd_surrogate_report_at(rmd_sim *sim, int32_t s, rmd_surrogate_report *out) {
   if (rmd_status c = check_index(sim, s)) return c;
   if (!out) return RMD_ERR_INVALID;

@@ -46,6 +46,21 @@ def test_default_options_are_the_references():
     assert o.pme_order == 5 and o.pressure < -1e299
 
 
+def test_plane_pass_rule():
+    """The reciprocal FFT's y and x axes: planes of up to 52 x 52 points take the fused pass one
+    block a plane; larger ones take it on a 4-block thread-block cluster while each block's
+    quarter of the rows and of the columns fits 100 KB of shared memory (up to 128 x 128);
+    larger planes, and axes longer than the 512-entry twiddle cache, take the separate passes.
+    The grids of the GPU test of the three passes are checked here against the rule."""
+    from rainmd_b200 import _lib
+
+    f = _lib.load().rmd_debug_plane_pass
+    assert [f(n, n) for n in (24, 32, 52)] == [1, 1, 1]
+    assert f(54, 50) == 1  # 2,700 points
+    assert [f(54, 60), f(72, 54), f(64, 64), f(100, 100), f(120, 120), f(128, 128)] == [4] * 6
+    assert [f(160, 160), f(600, 4), f(4, 600), f(0, 24)] == [0, 0, 0, 0]
+
+
 def test_struct_sizes_match_the_header():
     """The ctypes mirrors must have the C layout: check the size the compiler reports by
     asking the library for nothing but the default options round trip."""
