@@ -335,123 +335,123 @@ __global__ void __launch_bounds__(SPLIT == 1 ? 32 * NBR_WARPS : 32 * SPLIT)
   // Walk the stencil's x-slabs [ox_begin, ox_end), appending this lane's atom's hits to
   // dst[0 .. dst_cap); returns the atom's hit count (which may exceed dst_cap).
   auto walk = [&](int ox_begin, int ox_end, int *dst, int dst_cap) -> int {
-  int found = 0;
-  for (int ox = ox_begin; ox < ox_end; ++ox) {
-    const int rx = cc[0] + base[0] + ox;
-    const int wx = rx < 0 ? -1 : (rx >= counts[0] ? 1 : 0);
-    const int cx = rx - wx * counts[0];
-    for (int oy = 0; oy < count[1]; ++oy) {
-      const int ry = cc[1] + base[1] + oy;
-      const int wy = ry < 0 ? -1 : (ry >= counts[1] ? 1 : 0);
-      const int cy = ry - wy * counts[1];
-      for (int oz = 0; oz < count[2]; ++oz) {
-        const int rz = cc[2] + base[2] + oz;
-        const int wz = rz < 0 ? -1 : (rz >= counts[2] ? 1 : 0);
-        const int cz = rz - wz * counts[2];
-        const int cell = (cx * counts[1] + cy) * counts[2] + cz;
-        int code = 13;
-        float4 S = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (stencil_shift) {
-          code = shift_code(wx, wy, wz);
-          S = s.shift[code];
-          if (rectangular) {  // skip a cell whose box is beyond the list cutoff from the group's
-            const float r[3] = {(float)rx, (float)ry, (float)rz};
-            float d2 = 0.f;
-#pragma unroll
-            for (int d = 0; d < 3; ++d) {
-              const float clo = r[d] * wcell[d], chi = clo + wcell[d];
-              const float e = fmaxf(fmaxf(clo - bhi[d], blo[d] - chi), 0.f);
-              d2 = fmaf(e, e, d2);
-            }
-            if (d2 > cull2) continue;
-          }
-        }
-        // the bounding box seen from the unshifted copies of this cell's atoms
-        const float slo[3] = {blo[0] - S.x, blo[1] - S.y, blo[2] - S.z};
-        const float shi[3] = {bhi[0] - S.x, bhi[1] - S.y, bhi[2] - S.z};
-        const int begin = s.atom_start + cell_start[s.cell_start_base + cell];
-        const int end = s.atom_start + cell_start[s.cell_start_base + cell + 1];
-        for (int b = begin; b < end; b += 32) {
-          const int g = b + lane;
-          bool keep = g < end;
-          float4 pj = make_float4(0.f, 0.f, 0.f, 0.f);
-          if (keep) {
-            pj = spos[g];
-            if (stencil_shift) {  // drop candidates beyond the list cutoff from the bounding box
-              const float c[3] = {pj.x, pj.y, pj.z};
+    int found = 0;
+    for (int ox = ox_begin; ox < ox_end; ++ox) {
+      const int rx = cc[0] + base[0] + ox;
+      const int wx = rx < 0 ? -1 : (rx >= counts[0] ? 1 : 0);
+      const int cx = rx - wx * counts[0];
+      for (int oy = 0; oy < count[1]; ++oy) {
+        const int ry = cc[1] + base[1] + oy;
+        const int wy = ry < 0 ? -1 : (ry >= counts[1] ? 1 : 0);
+        const int cy = ry - wy * counts[1];
+        for (int oz = 0; oz < count[2]; ++oz) {
+          const int rz = cc[2] + base[2] + oz;
+          const int wz = rz < 0 ? -1 : (rz >= counts[2] ? 1 : 0);
+          const int cz = rz - wz * counts[2];
+          const int cell = (cx * counts[1] + cy) * counts[2] + cz;
+          int code = 13;
+          float4 S = make_float4(0.f, 0.f, 0.f, 0.f);
+          if (stencil_shift) {
+            code = shift_code(wx, wy, wz);
+            S = s.shift[code];
+            if (rectangular) {  // skip a cell whose box is beyond the list cutoff from the group's
+              const float r[3] = {(float)rx, (float)ry, (float)rz};
               float d2 = 0.f;
-#pragma unroll
+  #pragma unroll
               for (int d = 0; d < 3; ++d) {
-                const float e = fmaxf(fmaxf(slo[d] - c[d], c[d] - shi[d]), 0.f);
+                const float clo = r[d] * wcell[d], chi = clo + wcell[d];
+                const float e = fmaxf(fmaxf(clo - bhi[d], blo[d] - chi), 0.f);
                 d2 = fmaf(e, e, d2);
               }
-              keep = d2 <= cull2;
-            } else if (rectangular) {
-              // fewer than three cells on an axis: every cell is visited and the image is
-              // chosen per pair, so the cull measures from the nearest image on each axis
-              // (for a rectangular lattice that is the nearest image of the whole box)
-              const float c[3] = {pj.x, pj.y, pj.z};
-              float d2 = 0.f;
-#pragma unroll
-              for (int d = 0; d < 3; ++d) {
-                float x = c[d] - 0.5f * (blo[d] + bhi[d]);
-                x = fmaf(-rintf(x * s.inv_diag[d]), s.box[4 * d], x);
-                const float e = fmaxf(fabsf(x) - 0.5f * (bhi[d] - blo[d]), 0.f);
-                d2 = fmaf(e, e, d2);
-              }
-              keep = d2 <= cull2;
+              if (d2 > cull2) continue;
             }
           }
-          const unsigned mask = __ballot_sync(0xffffffffu, keep);
-          if (keep) {
-            const int at = __popc(mask & ((1u << lane) - 1u));
-            st_pos[at] = make_float4(pj.x + S.x, pj.y + S.y, pj.z + S.z, __int_as_float(g));
-            st_orig[at] = sorted_orig[g];
-          }
-          __syncwarp();
-          const int survivors = __popc(mask);
-          for (int t = 0; t < survivors; t += J) {
-            const int tt = t + sub;
-            bool in = valid && tt < survivors;
-            int entry = 0;
-            if (in) {
-              const float4 c = st_pos[tt];
-              const int j = st_orig[tt];
-              const int gj = __float_as_int(c.w);
-              float3 d = make_float3(pw.x - c.x, pw.y - c.y, pw.z - c.z);
-              int jcode = code;
-              if (!stencil_shift) {
-                const float kc = rintf(d.z * s.inv_diag[2]);
-                d.x = fmaf(-kc, s.box[6], d.x); d.y = fmaf(-kc, s.box[7], d.y); d.z = fmaf(-kc, s.box[8], d.z);
-                const float kb = rintf(d.y * s.inv_diag[1]);
-                d.x = fmaf(-kb, s.box[3], d.x); d.y = fmaf(-kb, s.box[4], d.y);
-                const float ka = rintf(d.x * s.inv_diag[0]);
-                d.x = fmaf(-ka, s.box[0], d.x);
-                jcode = shift_code(max(-1, min(1, (int)ka)), max(-1, min(1, (int)kb)), max(-1, min(1, (int)kc)));
+          // the bounding box seen from the unshifted copies of this cell's atoms
+          const float slo[3] = {blo[0] - S.x, blo[1] - S.y, blo[2] - S.z};
+          const float shi[3] = {bhi[0] - S.x, bhi[1] - S.y, bhi[2] - S.z};
+          const int begin = s.atom_start + cell_start[s.cell_start_base + cell];
+          const int end = s.atom_start + cell_start[s.cell_start_base + cell + 1];
+          for (int b = begin; b < end; b += 32) {
+            const int g = b + lane;
+            bool keep = g < end;
+            float4 pj = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (keep) {
+              pj = spos[g];
+              if (stencil_shift) {  // drop candidates beyond the list cutoff from the bounding box
+                const float c[3] = {pj.x, pj.y, pj.z};
+                float d2 = 0.f;
+  #pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                  const float e = fmaxf(fmaxf(slo[d] - c[d], c[d] - shi[d]), 0.f);
+                  d2 = fmaf(e, e, d2);
+                }
+                keep = d2 <= cull2;
+              } else if (rectangular) {
+                // fewer than three cells on an axis: every cell is visited and the image is
+                // chosen per pair, so the cull measures from the nearest image on each axis
+                // (for a rectangular lattice that is the nearest image of the whole box)
+                const float c[3] = {pj.x, pj.y, pj.z};
+                float d2 = 0.f;
+  #pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                  float x = c[d] - 0.5f * (blo[d] + bhi[d]);
+                  x = fmaf(-rintf(x * s.inv_diag[d]), s.box[4 * d], x);
+                  const float e = fmaxf(fabsf(x) - 0.5f * (bhi[d] - blo[d]), 0.f);
+                  d2 = fmaf(e, e, d2);
+                }
+                keep = d2 <= cull2;
               }
-              const float r2 = fmaf(d.x, d.x, fmaf(d.y, d.y, d.z * d.z));
-              in = r2 <= band_hi && gj != si;
-              if (in && r2 >= band_lo) {  // rare: reload both original positions
-                const float4 po = posq[i], qj = posq[j];
-                const float3 d0 = make_float3(__fsub_rn(po.x, qj.x), __fsub_rn(po.y, qj.y), __fsub_rn(po.z, qj.z));
-                in = !(dot_exact(min_image_exact(d0, s)) > lc2);
+            }
+            const unsigned mask = __ballot_sync(0xffffffffu, keep);
+            if (keep) {
+              const int at = __popc(mask & ((1u << lane) - 1u));
+              st_pos[at] = make_float4(pj.x + S.x, pj.y + S.y, pj.z + S.z, __int_as_float(g));
+              st_orig[at] = sorted_orig[g];
+            }
+            __syncwarp();
+            const int survivors = __popc(mask);
+            for (int t = 0; t < survivors; t += J) {
+              const int tt = t + sub;
+              bool in = valid && tt < survivors;
+              int entry = 0;
+              if (in) {
+                const float4 c = st_pos[tt];
+                const int j = st_orig[tt];
+                const int gj = __float_as_int(c.w);
+                float3 d = make_float3(pw.x - c.x, pw.y - c.y, pw.z - c.z);
+                int jcode = code;
+                if (!stencil_shift) {
+                  const float kc = rintf(d.z * s.inv_diag[2]);
+                  d.x = fmaf(-kc, s.box[6], d.x); d.y = fmaf(-kc, s.box[7], d.y); d.z = fmaf(-kc, s.box[8], d.z);
+                  const float kb = rintf(d.y * s.inv_diag[1]);
+                  d.x = fmaf(-kb, s.box[3], d.x); d.y = fmaf(-kb, s.box[4], d.y);
+                  const float ka = rintf(d.x * s.inv_diag[0]);
+                  d.x = fmaf(-ka, s.box[0], d.x);
+                  jcode = shift_code(max(-1, min(1, (int)ka)), max(-1, min(1, (int)kb)), max(-1, min(1, (int)kc)));
+                }
+                const float r2 = fmaf(d.x, d.x, fmaf(d.y, d.y, d.z * d.z));
+                in = r2 <= band_hi && gj != si;
+                if (in && r2 >= band_lo) {  // rare: reload both original positions
+                  const float4 po = posq[i], qj = posq[j];
+                  const float3 d0 = make_float3(__fsub_rn(po.x, qj.x), __fsub_rn(po.y, qj.y), __fsub_rn(po.z, qj.z));
+                  in = !(dot_exact(min_image_exact(d0, s)) > lc2);
+                }
+                if (in && j >= p_min && j <= p_max) in = !is_excluded(excl_start, excl_partners, i, j);
+                entry = (int)((unsigned)gj | ((unsigned)jcode << NBR_SLOT_BITS));
               }
-              if (in && j >= p_min && j <= p_max) in = !is_excluded(excl_start, excl_partners, i, j);
-              entry = (int)((unsigned)gj | ((unsigned)jcode << NBR_SLOT_BITS));
+              const unsigned hits = (__ballot_sync(0xffffffffu, in) >> (a * J)) & seg_mask;
+              if (in) {
+                const int pos = found + __popc(hits & below);
+                if (pos < dst_cap) dst[pos] = entry;
+              }
+              found += __popc(hits);
             }
-            const unsigned hits = (__ballot_sync(0xffffffffu, in) >> (a * J)) & seg_mask;
-            if (in) {
-              const int pos = found + __popc(hits & below);
-              if (pos < dst_cap) dst[pos] = entry;
-            }
-            found += __popc(hits);
+            __syncwarp();
           }
-          __syncwarp();
         }
       }
     }
-  }
-  return found;
+    return found;
   };
   // One call site of the walk (a loop rather than two calls, so that it is inlined): the
   // one-warp search walks every slab into the rows; a split warp walks its slab into shared
