@@ -435,6 +435,30 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
+# The pair kernel's arithmetic ceiling, reported beside its memory roofline. Every pair within
+# the cutoff is evaluated from both of its atoms (full neighbour rows), and one evaluation of the
+# force-only precision form issues, counted from the source of k_nonbonded: 49 FP32 operations,
+# 6 integer operations (three 64-bit fixed-point adds), 3 SFU operations (rsqrt, ex2, rcp) and
+# 3 float-to-int64 conversions. The ceiling is the larger of the issue time (one instruction per
+# lane per clock, 128 lanes per SM) and the SFU-and-conversion time (16 lanes per SM per clock)
+# on 148 SMs at the SM clock sampled during the run. List walking, loads, out-of-cutoff entries
+# and the exception loop are not counted, so the kernel cannot reach it.
+PAIR_LANE_OPS = 49 + 6 + 3 + 3
+PAIR_XU_OPS = 3 + 3
+B200_SMS = 148
+
+
+def pair_arithmetic_ceiling(pairs, kernel_ms, sm_mhz):
+    evaluations = 2 * int(pairs)
+    clock = float(sm_mhz) * 1e6
+    issue_s = evaluations * PAIR_LANE_OPS / (B200_SMS * 128 * clock)
+    xu_s = evaluations * PAIR_XU_OPS / (B200_SMS * 16 * clock)
+    ceiling_ms = max(issue_s, xu_s) * 1e3
+    return {"evaluations": evaluations, "lane_ops_per_evaluation": PAIR_LANE_OPS,
+            "sfu_and_conversion_ops_per_evaluation": PAIR_XU_OPS, "sm_mhz": float(sm_mhz),
+            "ceiling_ms": ceiling_ms, "frac": ceiling_ms / kernel_ms}
+
+
 def measured_peaks():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(path):
@@ -645,6 +669,8 @@ def main():
         return
     base = None if args.no_cpu_baseline else cpu_baseline(system, pos, grid, seed=1)
     traffic = measured_traffic("k_nonbonded", args.workload)
+    clock_summary = clocks.summary()
+    sm_clock = clock_summary.get("sm_mhz") or clock_summary.get("sm_max_mhz") or 1965.0
     line = {
         "metric": METRIC, "value": value, "unit": "ns/day", "n_gpus": world, "steps": args.steps,
         "warmup": max(3, args.warmup), "ms_per_step": seconds_per_step * 1e3, "higher_is_better": True,
@@ -659,7 +685,8 @@ def main():
                      "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                      "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
                      "algorithmic_bytes": bytes_nb, "unique_pairs_within_cutoff": pairs,
-                     "ms_per_launch": nb_ms},
+                     "ms_per_launch": nb_ms,
+                     "arithmetic_ceiling": pair_arithmetic_ceiling(pairs, nb_ms, sm_clock)},
         "kernels_ms": {"nonbonded": nb_ms, "nonbonded_per_lane_f32": nb_plain_ms,
                        "pme_kernels": pme_ms, "integrate": integ_ms,
                        "rebuild_kernels": rebuild_ms,
@@ -667,7 +694,7 @@ def main():
         "kernel_shapes": {k: shapes[k] for k in ("neighbourGroupAtoms", "nonbondedLanes", "spreadAtomsPerBlock")},
         "autotune_ms": shapes["tuned"],
         "batched": batched,
-        "clocks": clocks.summary(),
+        "clocks": clock_summary,
         "physics": {"temperature": e["temperature"], "potential": e["potential"],
                     "list_builds_timed": builds, "steps_per_list_build": args.steps / max(builds, 1),
                     "rebuild_on_demand": diag["rebuild_on_demand"],

@@ -61,6 +61,18 @@ def test_plane_pass_rule():
     assert [f(160, 160), f(600, 4), f(4, 600), f(0, 24)] == [0, 0, 0, 0]
 
 
+def test_pair_arithmetic_ceiling():
+    """bench.py's arithmetic ceiling of the pair kernel: 2 x 3,583,609 evaluations at 61 lane
+    operations on 148 x 128 lanes at 1,965 MHz (11.7 us) against 6 SFU/conversion operations on
+    148 x 16 lanes (9.2 us); the issue time is the ceiling."""
+    import bench
+
+    c = bench.pair_arithmetic_ceiling(3583609, 0.055, 1965.0)
+    assert c["evaluations"] == 7167218
+    assert abs(c["ceiling_ms"] - 7167218 * 61 / (148 * 128 * 1965e6) * 1e3) < 1e-12
+    assert 0.0116 < c["ceiling_ms"] < 0.0118 and 0.21 < c["frac"] < 0.215
+
+
 def test_struct_sizes_match_the_header():
     """The ctypes mirrors must have the C layout: check the size the compiler reports by
     asking the library for nothing but the default options round trip."""
