@@ -468,12 +468,15 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def cpu_baseline(system, positions, grid, seed, budget_s=20.0):
-    """The oracle's runDynamics (cpu/simulation.js:114-156 restated, FP64, O(N^2) direct
-    space, naive-DFT PME) on the host cores, for a bounded number of steps."""
+def cpu_baseline(system, positions, grid, seed, budget_s=20.0, threads=None, npt=False):
+    """The reference's CPU path on the host cores for a bounded sample of the workload: the
+    oracle's runDynamics (cpu/simulation.js:114-156 restated, FP64, O(N^2) direct space,
+    naive-DFT PME) for a few steps and, for an NPT workload, one volume move of the oracle's
+    attemptVolumeChange restatement (webgpu/simulation.js:995-1070; the reference's CPU path
+    has no barostat of its own), amortised at one move every 25 steps."""
     import oracle
 
-    threads = os.cpu_count() or 1
+    threads = threads or (os.cpu_count() or 1)
     oracle.set_threads(threads)
     o = oracle.Oracle(system)
     alpha = oracle.alpha_from_tolerance(0.9, 5e-4)
@@ -484,13 +487,26 @@ def cpu_baseline(system, positions, grid, seed, budget_s=20.0):
     per_eval = time.perf_counter() - t0
     steps = max(1, min(10, int(budget_s / max(per_eval, 1e-3))))
     t0 = time.perf_counter()
-    o.run_dynamics(positions, vel, steps, 0, integ, alpha, grid, 4)
+    pos1, vel1, _, _ = o.run_dynamics(positions, vel, steps, 0, integ, alpha, grid, 4)
     elapsed = time.perf_counter() - t0
     # run_dynamics evaluates the potential once before its loop
     per_step = max(1e-9, (elapsed - per_eval) / steps)
+    sample = (f"{steps} BAOAB steps of the FP64 oracle (O(N^2) direct space, naive-DFT PME) on this "
+              f"workload, {threads} thread{'s' if threads > 1 else ''}")
+    if npt:
+        box = system["boxVectors"]
+        t0 = time.perf_counter()
+        oracle.volume_move(system, pos1, vel1, 1, 0.01 * abs(box[0] * box[4] * box[8]), seed=seed,
+                           temperature=300.0, pressure=1.0, alpha=alpha, grid=grid, order=4)
+        move_s = time.perf_counter() - t0
+        per_step += move_s / BAROSTAT_INTERVAL
+        sample += f" and one volume move ({move_s:.2f} s) amortised over {BAROSTAT_INTERVAL} steps"
+    oracle.set_threads(os.cpu_count() or 1)
     return {"value": ns_per_day(per_step), "unit": "ns/day", "cores": threads, "kind": "port",
-            "sample": f"{steps} BAOAB steps of the FP64 oracle (O(N^2) direct space, naive-DFT PME) "
-                      f"on this workload, {threads} OpenMP threads, {per_step:.2f} s/step"}
+            "sample": sample + f": {per_step * 1e3:.1f} ms/step", "ms_per_step": per_step * 1e3}
+
+
+BAROSTAT_INTERVAL = 25
 
 
 def run_reference(args, rank, world):
@@ -498,7 +514,8 @@ def run_reference(args, rank, world):
         return
     system, pos, grid = workload(args.workload, seed=1)
     n = system["topology"]["atomCount"]
-    base = cpu_baseline(system, pos, grid, seed=1, budget_s=args.reference_budget)
+    npt = args.ensemble == "npt"
+    base = cpu_baseline(system, pos, grid, seed=1, budget_s=args.reference_budget, npt=npt)
     line = {
         "impl": "reference", "metric": METRIC, "value": base["value"], "unit": "ns/day", "n_gpus": 0,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ns_to_ms(base["value"]),
@@ -522,12 +539,109 @@ def ns_to_ms(value_ns_day):
     return TIMESTEP_PS * 1e-3 * 86400.0 / value_ns_day * 1e3
 
 
+def describe(name, grid, npt):
+    what = {"water-23558": "TIP3P water", "water-2854": "TIP3P water", "water-99999": "TIP3P water",
+            "chain-1190": "22-atom chain, Na+ and 389 TIP3P waters"}.get(name, name)
+    ensemble = (f"NPT 1 bar (MC barostat, a move every {BAROSTAT_INTERVAL} steps)" if npt else "NVT")
+    return (f"{name}: {what} {ensemble} 300 K, 2 fs, rc 0.9 nm, PME order 4 {grid[0]}x{grid[1]}x{grid[2]}, "
+            f"SETTLE, Langevin 1/ps")
+
+
 def config_block(args, atoms, grid, world):
-    return {"workload": f"{args.workload}: TIP3P water NVT 300 K, 2 fs, rc 0.9 nm, PME order 4 "
-                        f"{grid[0]}x{grid[1]}x{grid[2]}, SETTLE, Langevin 1/ps",
+    return {"workload": describe(args.workload, grid, args.ensemble == "npt"),
             "atoms": atoms, "replicas": world, "parallelism": f"replicas{world}",
             "l2": "flushed (256 MB written) before every timed block",
             "lists": "reference host schedule" if args.rebuild_schedule else "rebuilt on demand"}
+
+
+def prepare(system, pos, grid, seed, npt, args):
+    """A simulation of `system` minimised and equilibrated (untimed), with its block length:
+    NPT runs in blocks of the barostat interval (a move at the start of each block, as the
+    reference's run() attempts one at block boundaries), NVT in blocks of 100 steps."""
+    from rainmd_b200.simulation import GpuSimulation
+
+    opts = options_for(grid, seed=seed)
+    if npt:
+        opts.update({"pressure": 1.0, "barostatInterval": BAROSTAT_INTERVAL})
+    if args.rebuild_schedule:
+        opts["rebuildOnDemand"] = False
+    sim = GpuSimulation(system, opts)
+    sim.setState(pos)
+    sim.initialise()
+    sim.minimise(maxIterations=args.minimise, forceTolerance=1000.0)
+    block = BAROSTAT_INTERVAL if npt else args.block
+    sim.run(args.equilibrate, blockSize=block)
+    return sim, block
+
+
+def timed(sim, steps, warmup, block, barrier, min_warm_s=0.0):
+    """W warm-up blocks of `block` steps (and more until `min_warm_s` of wall time has passed, so
+    a clock sampler started before them sees the GPU under load), then exactly `steps` steps
+    timed with CUDA events on the engine's stream in blocks of at most `block`, L2 flushed
+    before every block. With the barostat, a block is the move interval: a move is due when the
+    timed region starts, and it holds one move per started interval (at 20 steps, one move).
+    Returns device ms and the kernels launched, lists built and volume moves attempted inside
+    the timed region."""
+    t0 = time.perf_counter()
+    done = 0
+    while done < max(3, warmup) or time.perf_counter() - t0 < min_warm_s:
+        sim.benchRun(block, block, flushL2=True)
+        done += 1
+    launches0 = sim.kernelLaunches()
+    builds0 = sim.diagnostics()["list_builds"]
+    moves0 = sim.diagnostics()["barostat_attempts"]
+    barrier()
+    device_ms = sim.benchRun(steps, min(block, steps), flushL2=True)
+    barrier()
+    d = sim.diagnostics()
+    return device_ms, sim.kernelLaunches() - launches0, d["list_builds"] - builds0, d["barostat_attempts"] - moves0
+
+
+def end_to_end(sim, n, steps, block, barrier, npt):
+    """The same steps through the public API with host arrays: setState (host f64 positions and
+    velocities), initialise, run, readState (host f32). With the barostat, an untimed block of
+    one move interval first, so that a move is due when the timed call starts, as in the
+    device-timed region. Returns (seconds, h2d bytes, d2h bytes, final state)."""
+    if npt:
+        sim.run(BAROSTAT_INTERVAL, blockSize=BAROSTAT_INTERVAL)
+    state = sim.readState()
+    host_pos = state["positions"].astype(np.float64)
+    host_vel = state["velocities"].astype(np.float64)
+    barrier()
+    t0 = time.perf_counter()
+    sim.setState(host_pos, host_vel, step=sim.step)
+    sim.initialise()
+    sim.run(steps, blockSize=min(block, steps))
+    out = sim.readState()
+    seconds = time.perf_counter() - t0
+    assert np.all(np.isfinite(out["positions"]))
+    return seconds, 2 * 16 * n, (16 + 16 + 24) * n + 8 * 9, out
+
+
+def config0_line(args, barrier):
+    """The reference's published configuration: 1,190 atoms (a 22-atom chain, Na+ and 389 TIP3P
+    waters in a 2.265 nm box), NPT at 1 bar with a move every 25 steps, PME order 4 on 24^3 —
+    device-timed, end to end through the API, and the CPU path single-threaded and on all
+    cores. The reference reports 133 ns/day for this system on Apple M-series WebGPU."""
+    system, pos, grid = workload("chain-1190", seed=1)
+    n = system["topology"]["atomCount"]
+    sim, block = prepare(system, pos, grid, seed=7, npt=True, args=args)
+    steps = max(args.steps, 100)
+    device_ms, launches, builds, moves = timed(sim, steps, args.warmup, block, barrier)
+    seconds, h2d, d2h, _ = end_to_end(sim, n, steps, block, barrier, True)
+    out = {"workload": describe("chain-1190", grid, True), "atoms": n, "steps": steps,
+           "ms_per_step": device_ms / steps, "value": ns_per_day(device_ms * 1e-3 / steps), "unit": "ns/day",
+           "volume_moves_timed": moves, "list_builds_timed": builds, "gpu_launches": launches,
+           "e2e": {"value": ns_per_day(seconds / steps), "unit": "ns/day", "h2d_bytes_per_step": h2d / steps,
+                   "d2h_bytes_per_step": d2h / steps},
+           "reference_published": {"value": 133, "unit": "ns/day",
+                                   "where": "Apple M-series WebGPU (the reference's docs/STATUS.md:184)"}}
+    sim.release()
+    if not args.no_cpu_baseline:
+        out["cpu_baseline_single_thread"] = cpu_baseline(system, pos, grid, seed=1, budget_s=5.0, threads=1,
+                                                         npt=True)
+        out["cpu_baseline_all_cores"] = cpu_baseline(system, pos, grid, seed=1, budget_s=5.0, npt=True)
+    return out
 
 
 def main():
@@ -537,12 +651,16 @@ def main():
     parser.add_argument("--warmup", type=int, default=3)
     parser.add_argument("--impl", default="ours", choices=["ours", "reference"])
     parser.add_argument("--workload", default="water-23558")
-    parser.add_argument("--block", type=int, default=100)
+    parser.add_argument("--ensemble", default="npt", choices=["npt", "nvt"],
+                        help="NPT (the default): 1 bar, a Monte Carlo volume move every 25 steps")
+    parser.add_argument("--block", type=int, default=100, help="steps per graph block in NVT")
     parser.add_argument("--reference-budget", type=float, default=20.0)
     parser.add_argument("--no-cpu-baseline", action="store_true")
     parser.add_argument("--minimise", type=int, default=200, help="minimiser iterations before dynamics")
     parser.add_argument("--equilibrate", type=int, default=3000, help="untimed steps before warm-up")
     parser.add_argument("--no-batched", action="store_true", help="skip the 64-system batch measurement")
+    parser.add_argument("--no-extra", action="store_true",
+                        help="skip the NVT comparison and the 1,190-atom configuration")
     parser.add_argument("--study", choices=["learned-barostat", "large-combined", "trajectory", "render"],
                         default=None,
                         help="run a study instead of the benchmark and print its JSON line")
@@ -586,69 +704,37 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
         torch.cuda.set_device(0)
 
-    from rainmd_b200.simulation import GpuSimulation
-
-    system, pos, grid = workload(args.workload, seed=1 + rank)
-    n = system["topology"]["atomCount"]
-    opts = options_for(grid, seed=7 + rank)
-    if args.rebuild_schedule:
-        opts["rebuildOnDemand"] = False
-    sim = GpuSimulation(system, opts)
-    sim.setState(pos)
-    sim.initialise()
-    sim.minimise(maxIterations=args.minimise, forceTolerance=1000.0)
-    # equilibrate and settle the adaptive rebuild interval (untimed), then W warm-up blocks
-    sim.run(args.equilibrate, blockSize=args.block)
-    block = min(args.block, args.steps)
-    for _ in range(max(3, args.warmup)):
-        sim.benchRun(block, block, flushL2=True)
-
     def barrier():
         torch.cuda.synchronize()
         if world > 1:
             dist.barrier()
         torch.cuda.synchronize()
 
-    launches0 = sim.kernelLaunches()
-    builds0 = sim.diagnostics()["list_builds"]
-    barrier()
-    with ClockSampler(local if world == 1 else 0) as clocks:
-        device_ms = sim.benchRun(args.steps, block, flushL2=True)
-    barrier()
-    launches = sim.kernelLaunches() - launches0
     def reduce_max(x):
         t = torch.tensor([x], dtype=torch.float64, device="cuda")
         if world > 1:
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
+    npt = args.ensemble == "npt"
+    system, pos, grid = workload(args.workload, seed=1 + rank)
+    n = system["topology"]["atomCount"]
+    sim, block = prepare(system, pos, grid, seed=7 + rank, npt=npt, args=args)
+    with ClockSampler(local if world == 1 else 0) as clocks:
+        device_ms, launches, builds, moves = timed(sim, args.steps, args.warmup, block, barrier, min_warm_s=1.5)
     value, seconds_per_step = aggregate(device_ms, args.steps, world, reduce_max)
 
     # energies stay finite and the run was physical
     diag = sim.diagnostics()
-    builds = diag["list_builds"] - builds0
     e = sim.energy()
 
     # end to end through the public API: host arrays in, run, host arrays out
-    state = sim.readState()
-    host_pos = state["positions"].astype(np.float64)
-    host_vel = state["velocities"].astype(np.float64)
-    barrier()
-    t0 = time.perf_counter()
-    sim.setState(host_pos, host_vel, step=sim.step)
-    sim.initialise()
-    sim.run(args.steps, blockSize=block)
-    out = sim.readState()
-    t1 = time.perf_counter()
-    e2e_seconds = t1 - t0
-    e2e_value = world * ns_per_day(e2e_seconds / args.steps)
-    h2d = 2 * 16 * n
-    d2h = (16 + 16 + 24) * n + 8 * 9
-    assert np.all(np.isfinite(out["positions"]))
+    e2e_seconds, h2d, d2h, out = end_to_end(sim, n, args.steps, block, barrier, npt)
+    e2e_value = world * ns_per_day(reduce_max(e2e_seconds) / args.steps)
 
     # roofline of the dominant kernel (nonbonded): algorithmic bytes per launch over the
     # CUDA-event launch time on the engine's stream
-    pairs = unique_pairs_within(out["positions"].astype(np.float64), system["boxVectors"][0], 0.9)
+    pairs = unique_pairs_within(out["positions"].astype(np.float64), out["boxVectors"][0], 0.9)
     nb_ms = sim.timeKernel("nonbonded", reps=50)
     shapes = sim.kernelShapes()
     sim.setNonbonded(shapes["nonbondedLanes"], pairFixed=False)
@@ -663,19 +749,38 @@ def main():
     bytes_pme = 32 * n + 24 * n + 16 * k3 + 32 * h
     peak, peak_kind = measured_peaks()
     achieved = bytes_nb / (nb_ms * 1e-3) / 1e9
+    sim.release()
 
+    extra = {}
+    if not args.no_extra:
+        # the same box without the barostat (the precision study's NVT form)
+        other = "nvt" if npt else "npt"
+        sim2, block2 = prepare(system, pos, grid, seed=7 + rank, npt=not npt, args=args)
+        ms2, launches2, builds2, moves2 = timed(sim2, args.steps, args.warmup, block2, barrier)
+        sim2.release()
+        v2, sps2 = aggregate(ms2, args.steps, world, reduce_max)
+        extra[other] = {"value": v2, "unit": "ns/day", "ms_per_step": sps2 * 1e3, "gpu_launches": launches2,
+                        "list_builds_timed": builds2, "volume_moves_timed": moves2,
+                        "workload": describe(args.workload, grid, not npt)}
+        extra["config0"] = config0_line(args, barrier)
     batched = None if args.no_batched else batched_block(args.batch_steps, seed=rank)
     if rank != 0:
+        if world > 1:
+            dist.destroy_process_group()
         return
-    base = None if args.no_cpu_baseline else cpu_baseline(system, pos, grid, seed=1)
+    base = None
+    if not args.no_cpu_baseline:
+        base = cpu_baseline(system, pos, grid, seed=1, npt=npt)
+        base["single_thread"] = cpu_baseline(system, pos, grid, seed=1, budget_s=12.0, threads=1, npt=npt)
     traffic = measured_traffic("k_nonbonded", args.workload)
     clock_summary = clocks.summary()
+    clock_summary["window"] = "warm-up blocks (at least 1.5 s) and the timed region"
     sm_clock = clock_summary.get("sm_mhz") or clock_summary.get("sm_max_mhz") or 1965.0
     line = {
         "metric": METRIC, "value": value, "unit": "ns/day", "n_gpus": world, "steps": args.steps,
         "warmup": max(3, args.warmup), "ms_per_step": seconds_per_step * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic (seeded TIP3P lattice, minimised and equilibrated 3000 steps)",
+        "data": f"synthetic (seeded TIP3P lattice, minimised and equilibrated {args.equilibrate} steps)",
         "config": config_block(args, n, grid, world),
         "e2e": {"value": e2e_value, "unit": "ns/day", "h2d_bytes_per_step": h2d / args.steps,
                 "d2h_bytes_per_step": d2h / args.steps,
@@ -693,10 +798,13 @@ def main():
                        "pme_roofline_frac": bytes_pme / (pme_ms * 1e-3) / 1e9 / peak},
         "kernel_shapes": {k: shapes[k] for k in ("neighbourGroupAtoms", "nonbondedLanes", "spreadAtomsPerBlock")},
         "autotune_ms": shapes["tuned"],
+        **extra,
         "batched": batched,
         "clocks": clock_summary,
-        "physics": {"temperature": e["temperature"], "potential": e["potential"],
+        "physics": {"temperature": e["temperature"], "potential": e["potential"], "volume": e["volume"],
                     "list_builds_timed": builds, "steps_per_list_build": args.steps / max(builds, 1),
+                    "volume_moves_timed": moves, "barostat_attempts": diag["barostat_attempts"],
+                    "barostat_accepted": diag["barostat_accepted"],
                     "rebuild_on_demand": diag["rebuild_on_demand"],
                     "rebuild_interval": diag["rebuild_interval"], "skin_violations": diag["skin_violations"],
                     "neighbour_capacity": diag["neighbour_capacity"]},

@@ -3,8 +3,7 @@
  *
  * Every entry point replaces one member of RainMD's `class GpuSimulation`
  * (webgpu/simulation.js:82-1341); the comment on each names the member and its line.
- * A Node N-API addon binds these 1:1; Python binds them with ctypes
- * (rainmd_b200/_lib.py).
+ * A Node N-API addon binds these 1:1; Python binds them with ctypes (rainmd_b200/_lib.py).
  *
  * Conventions
  *   - Units are RainMD's (shared/units.js): nm, ps, kJ/mol, amu, elementary charge, K, bar.
@@ -188,6 +187,33 @@ typedef struct {
 /* Fills `options` with the reference's defaults. */
 void rmd_default_options(rmd_options *options);
 
+/* The cell plan, skin and PME parameters of one system, computed on the host with no device
+ * work (callable without a GPU), exactly as rmd_create plans each system: skinFor
+ * (shared/topology/cells.js:67-91) unless options->skin is given, planCellList
+ * (cells.js:101-171) and pmeParameters (shared/pme/parameters.js:227-252). These are the
+ * numbers GpuSimulation exposes as plan.counts, pme.grid and pme.alpha
+ * (web/app.js:1140-1142). */
+typedef struct {
+  double skin, cutoff, list_cutoff;   /* nm */
+  int32_t counts[3];                  /* cells per axis */
+  int32_t cell_count;
+  int32_t stencil_cells;              /* cells of the deduplicated stencil (axisOffsets) */
+  double estimated_neighbours;        /* density x (4/3) pi list_cutoff^3 */
+  int32_t max_neighbours;             /* planCellList's maxNeighbours */
+  int32_t capacity;                   /* entries a neighbour row holds: maxNeighbours rounded up to a
+                                         multiple of 4, so rows start on 16-byte boundaries */
+  double mean_occupancy;              /* atoms per cell */
+  double alpha;                       /* Ewald splitting, 1/nm */
+  int32_t grid[3];
+  int32_t order;
+} rmd_plan;
+rmd_status rmd_plan_system(const rmd_system *system, const rmd_options *options, rmd_plan *out);
+
+/* grownPlan(plan, required) — cells.js:282-288: the row capacity after a build that needed
+ * `required` entries a row: max(capacity + 32, ceil(1.25 required)), rounded up to a
+ * multiple of 4. The engine grows its lists by this rule. */
+int32_t rmd_grown_capacity(int32_t capacity, int32_t required);
+
 /* new GpuSimulation(device, system, options) — simulation.js:83-190 */
 rmd_status rmd_create(const rmd_system *system, const rmd_options *options, rmd_sim **out);
 
@@ -276,8 +302,10 @@ rmd_status rmd_debug_evaluate(rmd_sim *sim, int32_t system_index, rmd_energy_rep
 /* Forces of one term alone at the current positions and list: 0 direct space with the
  * exceptions, 1 bonded and restraints, 2 PME reciprocal space. */
 rmd_status rmd_debug_force_term(rmd_sim *sim, int32_t system_index, int32_t term, double *forces);
-/* Copy a PME work buffer of the last evaluation: 0 the real grid after the inverse
- * transform (K^3 doubles), 1 the half spectrum (2*Kx*Ky*(Kz/2+1) doubles). */
+/* Copy a work buffer: 0 the real grid of the last evaluation after the inverse transform
+ * (K^3 doubles), 1 its half spectrum (2*Kx*Ky*(Kz/2+1) doubles), 2 the positions the current
+ * neighbour list was built from (3N doubles, the f32 values exactly; the displacement
+ * check's origin, simulation.js:380-386). */
 rmd_status rmd_debug_read(rmd_sim *sim, int32_t system_index, int32_t which, double *out);
 /* The real spread charge grid (K^3, z fastest) of the last evaluation. */
 rmd_status rmd_debug_charge_grid(rmd_sim *sim, int32_t system_index, double *grid);
@@ -292,6 +320,13 @@ rmd_status rmd_debug_fft(rmd_sim *sim, int32_t system_index, const double *data,
  * 4-block thread-block cluster a plane, 0 = separate y and x passes. A host-side rule that
  * depends on the grid alone (no device call); no reference counterpart. */
 int32_t rmd_debug_plane_pass(int32_t nx, int32_t ny);
+
+/* The thermostat's counter-based draws on the device for atoms [atom0, atom0 + count) at
+ * `step`, through the device functions the integrator calls: uniformAt(seed, atom, step, c)
+ * for c = 0..3 (shared/random.js:59) into uniforms[4 count], and gaussianTriple
+ * (random.js:66-87) into normals[3 count]. Host buffers; for parity tests. */
+rmd_status rmd_debug_draws(uint32_t seed, uint32_t atom0, int32_t count, uint32_t step, float *uniforms,
+                           float *normals);
 /* Average device time of one launch of a kernel group on the engine's own stream, by CUDA
  * events over `reps` back-to-back launches: 0 nonbonded (no energy), 1 the PME kernels
  * (five to seven, by grid), 2 the fused integrator, 3 bonded, 4 the list-rebuild kernels,
@@ -414,8 +449,10 @@ rmd_status rmd_render_positions(const float *positions, int32_t atom_count, cons
  * at most 64^3 points (2 MiB); larger grids return RMD_ERR_INVALID. Work is queued on
  * `stream` (NULL: the legacy default stream) and is complete when the stream is. The
  * array is shared by all calls: calls that overlap on the GPU race. The first call on a
- * device resolves the array's device address (cudaGetSymbolAddress) and must come before
- * any stream capture; later calls allocate nothing and can be captured. */
+ * device resolves the array's device address (cudaGetSymbolAddress) and loads the kernels
+ * it launches; it must come before any stream capture. The resolved address is not valid
+ * after cudaDeviceReset on that device. Sizes are checked before anything is launched; an
+ * error already pending from earlier work returns RMD_ERR_CUDA before anything is launched. */
 rmd_status rmd_spread_charges_noalloc(const void *posq, int32_t atom_count, const double box_vectors[9],
                                       const int32_t grid[3], int32_t order, double *grid_out, void *stream);
 

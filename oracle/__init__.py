@@ -11,6 +11,7 @@ neighbour search for bit-exact checks) by `build()`.
 from __future__ import annotations
 
 import ctypes as C
+import math
 import os
 import subprocess
 
@@ -491,3 +492,101 @@ def neighbour_list_f32(positions32, params, counts, cell_start, cell_atoms, excl
                                        _p(ep, C.c_int), int(capacity), _p(nb, C.c_int),
                                        _p(nc, C.c_int))
     return nb.reshape(n, capacity), nc, req
+
+
+# ---------------------------------------------------------------------------- cell plan
+# shared/topology/cells.js restated in Python floats (the JavaScript Number): the stencil's
+# per-axis offsets, skinFor, planCellList and grownPlan. Test infrastructure only.
+
+def axis_offsets(cell_count: int):
+    """cells.js:25-29: three cells or more visit {-1, 0, 1}; two visit {0, 1}; one {0}."""
+    if cell_count >= 3:
+        return [-1, 0, 1]
+    if cell_count == 2:
+        return [0, 1]
+    return [0]
+
+
+def skin_for(masses, box, cutoff, timestep=0.002, temperature=298.0):
+    """cells.js:67-91 (lightestMovingMass :35-41, halfSmallestWidth :93-97): the 0.40 nm anchor
+    scaled linearly by the timestep and by sqrt(T/298 * 1.008/m) of the lightest moving atom,
+    capped at 0.9 of the room between the cutoff and half the smallest box width."""
+    lightest = math.inf
+    for m in masses:
+        if m > 0 and m < lightest:
+            lightest = float(m)
+    if not math.isfinite(lightest):
+        lightest = 1.008
+    speed_ratio = math.sqrt((temperature / 298) * (1.008 / lightest))
+    scaled = 0.40 * (timestep / 0.002) * speed_ratio
+    widest = None if box is None else min(abs(box[0]), abs(box[4]), abs(box[8])) / 2
+    room = math.inf if widest is None else widest - cutoff
+    return max(0.1, min(scaled, room * 0.9 if room > 0 else 0.1))
+
+
+def plan_cell_list(atom_count, box, cutoff, skin=0.1, neighbour_slack=2.0, max_neighbours=None):
+    """cells.js:101-171: cells per axis floor(|w| / (cutoff + skin)) (at least one), the
+    deduplicated stencil, and the capacity max(32, ceil(density * 4/3 pi (rc+skin)^3 * slack))."""
+    list_cutoff = cutoff + skin
+    widths = [box[0], box[4], box[8]]
+    counts = [max(1, math.floor(abs(w) / list_cutoff)) for w in widths]
+    offsets = [axis_offsets(c) for c in counts]
+    stencil = [(dx, dy, dz) for dx in offsets[0] for dy in offsets[1] for dz in offsets[2]]
+    volume = abs(box[0] * box[4] * box[8])
+    density = atom_count / volume
+    estimated = density * ((4 / 3) * math.pi * list_cutoff ** 3)
+    capacity = max_neighbours if max_neighbours is not None else max(32, math.ceil(estimated * neighbour_slack))
+    return {"skin": skin, "cutoff": cutoff, "listCutoff": list_cutoff, "counts": counts,
+            "cellCount": counts[0] * counts[1] * counts[2], "stencil": stencil,
+            "maxNeighbours": capacity, "estimatedNeighbours": estimated,
+            "meanOccupancy": atom_count / (counts[0] * counts[1] * counts[2])}
+
+
+def grown_plan(max_neighbours, required):
+    """cells.js:282-288: max(maxNeighbours + 32, ceil(required * 1.25))."""
+    return max(max_neighbours + 32, math.ceil(required * 1.25))
+
+
+# ------------------------------------------------------------------------ volume move
+BAR_TO_KJ_PER_MOL_NM3 = 0.06022140857   # shared/units.js:53
+BOLTZMANN = 0.008314462618              # shared/units.js:50
+
+
+def volume_move(system, positions, velocities, attempt, volume_scale, *, seed, temperature, pressure,
+                alpha, grid, order, dispersion=True):
+    """One Monte Carlo volume move, attemptVolumeChange (webgpu/simulation.js:995-1070) restated in
+    FP64 on the oracle: the potential at the current state, a volume change drawn from
+    uniformAt(seed ^ 0x5a17, attempt, 0, 0), molecule centroids scaled with the box, the
+    potential of the scaled state, metropolisWeight (barostat.js:158-162) and the second draw;
+    a rejected move restores the state and evaluates it again, as the reference does. The PME
+    grid stays fixed. Returns (accepted, positions, box, weight, delta_volume)."""
+    box = np.asarray(system["boxVectors"], dtype=np.float64)
+    volume = abs(box[0] * box[4] * box[8])
+    kT = BOLTZMANN * temperature
+    p = pressure * BAR_TO_KJ_PER_MOL_NM3
+
+    def total(sys_, pos, vol):
+        e, _ = Oracle(sys_).potential(pos, method="PME", alpha=alpha, grid=grid, order=order)
+        if dispersion:
+            e["total"] += Oracle(sys_).dispersion(vol, sys_["options"]["cutoff"])
+        return e["total"]
+
+    old = total(system, positions, volume)
+    draw = uniform_at((seed ^ 0x5A17) & 0xFFFFFFFF, attempt, 0, 0)
+    delta = volume_scale * 2 * (draw - 0.5)
+    new_volume = volume + delta
+    if not new_volume > 0:
+        return False, positions, box, 0.0, delta
+    scale = float(np.cbrt(new_volume / volume))
+    if system["options"]["cutoff"] > 0.5 * scale * min(abs(box[0]), abs(box[4]), abs(box[8])):
+        return False, positions, box, 0.0, delta
+    scaled_system = dict(system)
+    scaled_system["boxVectors"] = box * scale
+    scaled = Oracle(system).scale_molecules(positions, scale)
+    new = total(scaled_system, scaled, new_volume)
+    weight = metropolis_weight(new - old, delta, new_volume / volume, p, kT, system["molecules"]["count"])
+    accept = weight <= 0 or uniform_at((seed ^ 0x5A17) & 0xFFFFFFFF, attempt, 1, 0) < math.exp(-weight / kT)
+    if accept:
+        return True, scaled, box * scale, weight, delta
+    total(system, positions, volume)
+    return False, positions, box, weight, delta

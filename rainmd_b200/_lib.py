@@ -120,6 +120,15 @@ class RmdDiagnostics(C.Structure):
     ]
 
 
+class RmdPlan(C.Structure):
+    _fields_ = [
+        ("skin", C.c_double), ("cutoff", C.c_double), ("list_cutoff", C.c_double),
+        ("counts", C.c_int32 * 3), ("cell_count", C.c_int32), ("stencil_cells", C.c_int32),
+        ("estimated_neighbours", C.c_double), ("max_neighbours", C.c_int32), ("capacity", C.c_int32),
+        ("mean_occupancy", C.c_double), ("alpha", C.c_double), ("grid", C.c_int32 * 3), ("order", C.c_int32),
+    ]
+
+
 EXPORTS = [
     "rmd_default_options", "rmd_create", "rmd_create_batch", "rmd_system_count", "rmd_set_state",
     "rmd_set_state_at", "rmd_set_noise", "rmd_set_noise_at", "rmd_initialise", "rmd_run",
@@ -131,7 +140,8 @@ EXPORTS = [
     "rmd_bench_run", "rmd_debug_force_term", "rmd_debug_read", "rmd_spread_charges_noalloc",
     "rmd_kernel_shapes", "rmd_set_kernel_shapes", "rmd_surrogate_report_at", "rmd_surrogate_weights",
     "rmd_surrogate_evaluate", "rmd_image_molecules_at", "rmd_dcd_frame_bytes", "rmd_dcd_frame_at",
-    "rmd_dcd_header", "rmd_restart_at", "rmd_render_at", "rmd_render_positions",
+    "rmd_dcd_header", "rmd_restart_at", "rmd_render_at", "rmd_render_positions", "rmd_plan_system",
+    "rmd_grown_capacity", "rmd_debug_draws",
 ]
 
 _lib = None
@@ -212,6 +222,10 @@ def load():
                    C.c_int32, C.c_int32, C.POINTER(C.c_uint8)]
     lib.rmd_render_at.argtypes = [sim, C.c_int32, *render_args]
     lib.rmd_render_positions.argtypes = [_fp, C.c_int32, *render_args]
+    lib.rmd_plan_system.argtypes = [C.POINTER(RmdSystem), C.POINTER(RmdOptions), C.POINTER(RmdPlan)]
+    lib.rmd_grown_capacity.argtypes = [C.c_int32, C.c_int32]
+    lib.rmd_grown_capacity.restype = C.c_int32
+    lib.rmd_debug_draws.argtypes = [C.c_uint32, C.c_uint32, C.c_int32, C.c_uint32, _fp, _fp]
     for name in EXPORTS:
         fn = getattr(lib, name)
         if fn.restype is C.c_int and name not in ("rmd_system_count",):

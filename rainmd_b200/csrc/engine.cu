@@ -164,6 +164,16 @@ struct HostSystem {
 
 static const double LIGHT_ANCHOR_SKIN = 0.40;  // cells.js:67-91
 
+// Neighbour rows hold a multiple of 4 entries so that every row starts on a 16-byte boundary
+// (a departure from planCellList's maxNeighbours, which it rounds up, never down).
+static int row_capacity(int max_neighbours) { return (max_neighbours + 3) & ~3; }
+
+// grownPlan (cells.js:282-288): past the measured requirement by a quarter, and at least 32
+// more than before, as a row capacity.
+static int grown_capacity(int capacity, int required) {
+  return row_capacity(std::max(capacity + 32, (int)std::ceil(required * 1.25)));
+}
+
 // How a force evaluation treats the neighbour lists.
 enum RebuildMode { REBUILD_NONE = 0, REBUILD_FORCED = 1, REBUILD_IF_STALE = 2 };
 
@@ -247,6 +257,10 @@ struct Engine {
   int n_molecules_total = 0;
   bool any_pressure = false;
   bool supplied_noise_any = false;
+  // true while `energies` holds the potential at the current positions and box because the
+  // last step graph ended with an energy-enabled evaluation; a volume move then needs no
+  // evaluation of its own first. Every other evaluation or change of state clears it.
+  bool energy_fresh = false;
 
   std::map<std::string, cudaGraphExec_t> graphs;
   std::map<std::string, long long> graph_launches;  // kernels recorded in each graph
@@ -264,7 +278,7 @@ struct Engine {
 
   // ---------------------------------------------------------------- construction
   void build(int count, const rmd_system *systems, const rmd_options *options);
-  void plan_system(HostSystem &h, const rmd_system &s);
+  static void plan_system(HostSystem &h, const rmd_system &s);
   void upload_all(const std::vector<const rmd_system *> &src);
   void allocate_neighbours();
   LaunchCtx ctx() const;
@@ -366,7 +380,7 @@ void Engine::plan_system(HostSystem &h, const rmd_system &s) {
   const double slack = o.neighbour_slack > 0 ? o.neighbour_slack : 2.0;
   h.capacity = o.max_neighbours > 0 ? o.max_neighbours
                                     : std::max(32, (int)std::ceil(h.estimated_neighbours * slack));
-  h.capacity = (h.capacity + 3) & ~3;  // rows start on 16-byte boundaries
+  h.capacity = row_capacity(h.capacity);
   // pmeParameters (parameters.js:227-252)
   const double tol = o.ewald_tolerance > 0 ? o.ewald_tolerance : 5e-4;
   h.alpha = o.alpha > 0 ? o.alpha : alpha_from_tolerance(h.cutoff, tol);
@@ -1395,6 +1409,7 @@ void Engine::record_conditional_rebuild(const LaunchCtx &c) {
 }
 
 void Engine::evaluate(bool rebuild, bool energy) {
+  energy_fresh = false;
   const long long before = recorded;
   record_forces(rebuild, energy);
   kernel_launches += recorded - before;
@@ -1412,6 +1427,7 @@ void Engine::record_barostat() {
 }
 
 void Engine::set_state(int s, const double *pos, const double *vel_in, int64_t step, int supplied) {
+  energy_fresh = false;
   HostSystem &h = hs[s];
   // constraintToleranceFloor (clusters.js:136-148)
   double span = 0;
@@ -1452,8 +1468,8 @@ int Engine::check_capacity() {
     hs[s].last_required = req[s];
     hs[s].worst_required = std::max(hs[s].worst_required, most);
     worst = std::max(worst, most);
-    if (most > hs[s].capacity) {  // grownPlan (cells.js:282-288)
-      hs[s].capacity = (std::max(hs[s].capacity + 32, (int)std::ceil(most * 1.25)) + 3) & ~3;
+    if (most > hs[s].capacity) {
+      hs[s].capacity = grown_capacity(hs[s].capacity, most);
       hs[s].neighbour_growths++;
       grow = true;
     }
@@ -1498,6 +1514,12 @@ std::map<std::string, std::array<int, 3>> g_tuned;
 // shape (atoms, systems, cells, PME grids and order, accumulation mode).
 void Engine::autotune() {
   if (!(tune_group || tune_lanes || tune_spread)) return;
+  // captured step graphs hold the shapes they were recorded with: they stay valid (and are
+  // replayed without re-capture by the next run) unless the tuned shapes change
+  const std::array<int, 3> before = {group_atoms, nb_lanes, spread_atoms};
+  auto keep_or_drop_graphs = [&]() {
+    if (std::array<int, 3>{group_atoms, nb_lanes, spread_atoms} != before) drop_graphs();
+  };
   std::string key = std::to_string(S) + ":" + std::to_string(N) + ":" + std::to_string(n_cells_total) + ":" +
                     std::to_string(pme_order) + ":" + std::to_string(pair_fixed);
   for (auto &h : hs) key += ":" + std::to_string(h.grid[0] * 100000LL + h.grid[1] * 1000LL + h.grid[2]);
@@ -1508,7 +1530,7 @@ void Engine::autotune() {
       if (tune_group) group_atoms = it->second[0];
       if (tune_lanes) nb_lanes = it->second[1];
       if (tune_spread) spread_atoms = it->second[2];
-      drop_graphs();
+      keep_or_drop_graphs();
       return;
     }
   }
@@ -1571,7 +1593,7 @@ void Engine::autotune() {
     std::lock_guard<std::mutex> lock(g_tune_mutex);
     g_tuned[key] = {group_atoms, nb_lanes, spread_atoms};
   }
-  drop_graphs();
+  keep_or_drop_graphs();
 }
 
 void Engine::initialise() {
@@ -1639,19 +1661,9 @@ void Engine::run_block(int n, bool barostat, bool energy_last) {
     CUDA_OK(cudaGraphDestroy(graph));
     it = graphs.emplace(key, exec).first;
   }
-  if (timing) {
-    if (flush) CUDA_OK(cudaMemsetAsync(flush_buffer.p, (int)(kernel_launches & 0xff), flush_buffer.n, stream));
-    CUDA_OK(cudaEventRecord(ev_a, stream));
-  }
   CUDA_OK(cudaGraphLaunch(it->second, stream));
-  if (timing) {
-    CUDA_OK(cudaEventRecord(ev_b, stream));
-    CUDA_OK(cudaEventSynchronize(ev_b));
-    float ms = 0.f;
-    CUDA_OK(cudaEventElapsedTime(&ms, ev_a, ev_b));
-    timed_ms += ms;
-  }
   kernel_launches += graph_launches[key];
+  energy_fresh = energy_last;
   // host bookkeeping mirrors the device
   for (auto &h : hs) {
     int64_t s2 = barostat ? (1LL << 40) : h.steps_since_rebuild;
@@ -1743,15 +1755,30 @@ void Engine::run(int64_t count, int block, const volatile int32_t *stop) {
     for (auto &h : hs)
       if (h.has_pressure && (due ? 0 : h.steps_since_barostat) + n >= h.barostat_interval) next_due = true;
     bool exact_move = due;
+    // timed runs (rmd_bench_run): L2 is flushed before each block, outside the events, and
+    // the events bracket all of the block's device work: the energy evaluation and the
+    // surrogate screening before a volume move, the block's graph and the training after it
+    if (timing) {
+      if (flush) CUDA_OK(cudaMemsetAsync(flush_buffer.p, (int)(kernel_launches & 0xff), flush_buffer.n, stream));
+      CUDA_OK(cudaEventRecord(ev_a, stream));
+    }
     if (due) {
-      // the move needs the energy at the current positions
-      evaluate(false, true);
+      // the move needs the energy at the current positions: the previous block's last
+      // evaluation computed it when this move was due at its end
+      if (!energy_fresh) evaluate(false, true);
       // with the learned barostat, stage 1 may screen every system's move out: the block
       // then runs without the exact trial evaluation
       if (learned) exact_move = surrogate_stage1();
     }
     run_block(n, exact_move, next_due);
     if (due && learned && exact_move) surrogate_train();
+    if (timing) {
+      CUDA_OK(cudaEventRecord(ev_b, stream));
+      CUDA_OK(cudaEventSynchronize(ev_b));
+      float ms = 0.f;
+      CUDA_OK(cudaEventElapsedTime(&ms, ev_a, ev_b));
+      timed_ms += ms;
+    }
     sync();
     if (due) {
       for (auto &h : hs) h.steps_since_barostat = 0;
@@ -1872,6 +1899,7 @@ void Engine::attempt_volume_change() {
 }
 
 double Engine::scale_volume(int s, double ls) {
+  energy_fresh = false;
   // scaleVolume (simulation.js:801-811): centroid scaling and the box, then the potential
   std::vector<double> scales(S, 1.0);
   scales[s] = ls;
@@ -1912,6 +1940,7 @@ std::vector<float> Engine::max_forces() {
 // rejected trial, so the next trial moves along the accepted gradient.
 void Engine::minimise(int max_iterations, double force_tolerance, double max_step, double cap,
                       rmd_minimise_result *out) {
+  energy_fresh = false;
   if (max_iterations <= 0) max_iterations = 200;
   if (!(force_tolerance > 0)) force_tolerance = 500;
   if (!(max_step > 0)) max_step = 0.002;
@@ -2100,6 +2129,44 @@ void rmd_default_options(rmd_options *o) {
   o->neighbour_slack = 2.0;
   o->ewald_tolerance = 5e-4;
   o->pme_order = 5;
+}
+
+rmd_status rmd_plan_system(const rmd_system *system, const rmd_options *options, rmd_plan *out) {
+  if (!system || !out) return RMD_ERR_INVALID;
+  return guarded(nullptr, [&]() {
+    rmd::HostSystem h;
+    if (options) {
+      h.opt = *options;
+    } else {
+      rmd_default_options(&h.opt);
+    }
+    rmd::Engine::plan_system(h, *system);
+    memset(out, 0, sizeof *out);
+    out->skin = h.skin;
+    out->cutoff = h.cutoff;
+    out->list_cutoff = h.list_cutoff;
+    out->cell_count = 1;
+    out->stencil_cells = 1;
+    for (int d = 0; d < 3; ++d) {
+      out->counts[d] = h.counts[d];
+      out->cell_count *= h.counts[d];
+      out->stencil_cells *= h.counts[d] >= 3 ? 3 : h.counts[d];  // axisOffsets (cells.js:25-29)
+      out->grid[d] = h.grid[d];
+    }
+    out->estimated_neighbours = h.estimated_neighbours;
+    const double slack = h.opt.neighbour_slack > 0 ? h.opt.neighbour_slack : 2.0;
+    out->max_neighbours = h.opt.max_neighbours > 0
+                              ? h.opt.max_neighbours
+                              : std::max(32, (int)std::ceil(h.estimated_neighbours * slack));
+    out->capacity = h.capacity;
+    out->mean_occupancy = (double)h.n / out->cell_count;
+    out->alpha = h.alpha;
+    out->order = h.order;
+  });
+}
+
+int32_t rmd_grown_capacity(int32_t capacity, int32_t required) {
+  return capacity > 0 && required >= 0 ? rmd::grown_capacity(capacity, required) : 0;
 }
 
 rmd_status rmd_create_batch(int32_t count, const rmd_system *systems, const rmd_options *options,
@@ -2442,8 +2509,16 @@ rmd_status rmd_debug_read(rmd_sim *sim, int32_t s, int32_t which, double *out) {
         out[2 * k] = g[k].x;
         out[2 * k + 1] = g[k].y;
       }
+    } else if (which == 2) {  // the positions the current neighbour list was built from
+      std::vector<float4> o(h.n);
+      CUDA_OK(cudaMemcpy(o.data(), e.origin.p + h.atom_start, sizeof(float4) * h.n, cudaMemcpyDeviceToHost));
+      for (int k = 0; k < h.n; ++k) {
+        out[3 * k] = o[k].x;
+        out[3 * k + 1] = o[k].y;
+        out[3 * k + 2] = o[k].z;
+      }
     } else {
-      throw rmd::Error(RMD_ERR_INVALID, "buffer is 0 (real grid) or 1 (half spectrum)");
+      throw rmd::Error(RMD_ERR_INVALID, "buffer is 0 (real grid), 1 (half spectrum) or 2 (list origin)");
     }
   });
 }
@@ -2543,6 +2618,23 @@ rmd_status rmd_debug_time_kernel(rmd_sim *sim, int32_t which, int32_t reps, doub
     keep_pos.release();
     keep_vel.release();
     keep_spos.release();
+  });
+}
+
+rmd_status rmd_debug_draws(uint32_t seed, uint32_t atom0, int32_t count, uint32_t step, float *uniforms,
+                           float *normals) {
+  if (count < 0 || (count > 0 && (!uniforms || !normals))) return RMD_ERR_INVALID;
+  return guarded(nullptr, [&]() {
+    if (count == 0) return;
+    rmd::DevArray<float> u, g;
+    u.alloc((size_t)count * 4);
+    g.alloc((size_t)count * 3);
+    rmd::launch_draws(seed, atom0, count, step, u.p, g.p, nullptr);
+    CUDA_OK(cudaGetLastError());
+    CUDA_OK(cudaMemcpy(uniforms, u.p, u.bytes(), cudaMemcpyDeviceToHost));
+    CUDA_OK(cudaMemcpy(normals, g.p, g.bytes(), cudaMemcpyDeviceToHost));
+    u.release();
+    g.release();
   });
 }
 

@@ -501,4 +501,26 @@ void launch_integrate(const IntegrateArgs &a, int mode, cudaStream_t stream) {
   launch_chained(kernel, blocks, tb, 0, stream, a);
 }
 
+// The thermostat's draws for atoms [atom0, atom0 + count) at `step`, through the same device
+// functions k_integrate calls (random.js:59 uniformAt for c = 0..3, and the Box-Muller triple
+// built from them): four uniforms and three normals per atom.
+__global__ void k_draws(uint32_t seed, uint32_t atom0, int count, uint32_t step, float *__restrict__ uniforms,
+                        float *__restrict__ normals) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= count) return;
+  const uint32_t atom = atom0 + (uint32_t)k;
+#pragma unroll
+  for (uint32_t c = 0; c < 4; ++c) uniforms[4 * (long long)k + c] = rng_uniform(seed, atom, step, c);
+  const float3 g = rng_gaussian3(seed, atom, step);
+  normals[3 * (long long)k] = g.x;
+  normals[3 * (long long)k + 1] = g.y;
+  normals[3 * (long long)k + 2] = g.z;
+}
+
+void launch_draws(uint32_t seed, uint32_t atom0, int count, uint32_t step, float *uniforms, float *normals,
+                  cudaStream_t stream) {
+  if (count <= 0) return;
+  k_draws<<<(count + 127) / 128, 128, 0, stream>>>(seed, atom0, count, step, uniforms, normals);
+}
+
 }  // namespace rmd

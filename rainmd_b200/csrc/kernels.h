@@ -187,6 +187,8 @@ void launch_fft_forward(const LaunchCtx &c, cudaStream_t stream);
 void launch_spread_only(const LaunchCtx &c, cudaStream_t stream);
 void launch_fft_inverse(const LaunchCtx &c, cudaStream_t stream);
 void launch_integrate(const IntegrateArgs &a, int mode, cudaStream_t stream);
+void launch_draws(uint32_t seed, uint32_t atom0, int count, uint32_t step, float *uniforms, float *normals,
+                  cudaStream_t stream);
 
 // Energy segments reduced per system (reduce.cu). Each segment is [start, end) of one
 // per-item FP64 array; the result lands in energies[sys * N_ENERGY + term].

@@ -18,8 +18,15 @@
 //     clears the part it uses before spreading. Calls that overlap on the GPU (different
 //     streams, or different host threads, without ordering between them) race on it;
 //   - the first call on a device looks up the array's device address with
-//     cudaGetSymbolAddress (with that device current) and caches it; that first call should
-//     come before any stream capture begins.
+//     cudaGetSymbolAddress (with that device current), loads every kernel this entry point
+//     launches (both spline orders and the conversion), and caches the address; that first
+//     call should come before any stream capture begins, so that a later call, captured or
+//     not, neither resolves a symbol nor loads a module. The cached address belongs to the
+//     device's primary context: after cudaDeviceReset on that device it is stale, and the
+//     library must not be called on that device again in this process;
+//   - an error already pending on the calling thread (an earlier launch that failed) is
+//     returned as RMD_ERR_CUDA before anything is launched, so a failure reported by a call
+//     is that call's own.
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -92,16 +99,19 @@ extern "C" rmd_status rmd_spread_charges_noalloc(const void *posq, int32_t atom_
   using namespace rmd;
   if (!posq || !grid_out || !box_vectors || !grid || atom_count < 0 || (order != 4 && order != 5))
     return RMD_ERR_INVALID;
+  // Bound each size before multiplying, so that no product of the three can overflow and
+  // wrap to a small value that would pass the scratch limit (64^3 points).
   long long points = 1;
   for (int d = 0; d < 3; ++d) {
-    if (grid[d] < order) return RMD_ERR_INVALID;
+    if (grid[d] < order || grid[d] > SCRATCH_POINTS) return RMD_ERR_INVALID;
+    if (points > SCRATCH_POINTS / grid[d]) return RMD_ERR_INVALID;
     points *= grid[d];
   }
-  if (points > SCRATCH_POINTS) return RMD_ERR_INVALID;  // beyond the fixed scratch (64^3)
   const double ax = box_vectors[0], bx = box_vectors[3], by = box_vectors[4];
   const double cx = box_vectors[6], cy = box_vectors[7], cz = box_vectors[8];
   if (box_vectors[1] != 0.0 || box_vectors[2] != 0.0 || box_vectors[5] != 0.0 || !(ax > 0) || !(by > 0) || !(cz > 0))
     return RMD_ERR_INVALID;  // reduced upper-triangular boxes only, as the engine
+  if (cudaPeekAtLastError() != cudaSuccess) return RMD_ERR_CUDA;  // an earlier failure, still pending
   int device = 0;
   if (cudaGetDevice(&device) != cudaSuccess || device < 0 || device >= MAX_DEVICES) return RMD_ERR_CUDA;
   unsigned long long *scratch = nullptr;
@@ -110,6 +120,13 @@ extern "C" rmd_status rmd_spread_charges_noalloc(const void *posq, int32_t atom_
     if (!g_scratch_address[device]) {
       void *address = nullptr;
       if (cudaGetSymbolAddress(&address, g_spread_scratch) != cudaSuccess || address == nullptr)
+        return RMD_ERR_CUDA;
+      // load the three kernels now (lazy module loading would otherwise load each at its
+      // first launch, possibly inside a capture)
+      cudaFuncAttributes attributes;
+      if (cudaFuncGetAttributes(&attributes, k_spread_noalloc<4>) != cudaSuccess ||
+          cudaFuncGetAttributes(&attributes, k_spread_noalloc<5>) != cudaSuccess ||
+          cudaFuncGetAttributes(&attributes, k_fixed_to_f64) != cudaSuccess)
         return RMD_ERR_CUDA;
       g_scratch_address[device] = static_cast<unsigned long long *>(address);
     }

@@ -165,6 +165,39 @@ def surrogate_evaluate(params, inputs, targets=None, gradients=False):
     return out, grads, (loss.value if gradients else None)
 
 
+def planSystem(system: dict, options: dict | None = None) -> dict:
+    """The cell plan, skin and PME parameters the engine uses for `system`, computed on the host
+    (no GPU needed): skinFor, planCellList (shared/topology/cells.js:67-171) and pmeParameters
+    (shared/pme/parameters.js:227-252), the fields GpuSimulation exposes as plan.counts,
+    pme.grid and pme.alpha."""
+    lib = L.load()
+    keep: list = []
+    out = L.RmdPlan()
+    status = lib.rmd_plan_system(C.byref(pack_system(system, keep)), C.byref(pack_options(options or {}, keep)),
+                                 C.byref(out))
+    if status != L.RMD_OK:
+        raise _ERRORS.get(status, RainMDError)(lib.rmd_last_error(None).decode())
+    return _struct_dict(out)
+
+
+def grownCapacity(capacity: int, required: int) -> int:
+    """grownPlan (cells.js:282-288) as the engine applies it to its neighbour rows."""
+    return int(L.load().rmd_grown_capacity(int(capacity), int(required)))
+
+
+def deviceDraws(seed: int, atom0: int, count: int, step: int):
+    """The thermostat's counter-based draws computed on the device: (uniforms [count, 4],
+    normals [count, 3]) for atoms atom0 .. atom0 + count - 1 at `step`."""
+    lib = L.load()
+    u = np.zeros((count, 4), np.float32)
+    g = np.zeros((count, 3), np.float32)
+    fp = lambda a: a.ctypes.data_as(C.POINTER(C.c_float))  # noqa: E731
+    status = lib.rmd_debug_draws(seed & 0xffffffff, atom0, count, step & 0xffffffff, fp(u), fp(g))
+    if status != L.RMD_OK:
+        raise _ERRORS.get(status, RainMDError)(lib.rmd_last_error(None).decode())
+    return u, g
+
+
 class BatchSimulation:
     """Many independent systems advanced together; every call takes a system index."""
 
@@ -315,7 +348,7 @@ class BatchSimulation:
         return forces
 
     def debugRead(self, which: str, count: int, index=0):
-        code = {"real_grid": 0, "half": 1}[which]
+        code = {"real_grid": 0, "half": 1, "list_origin": 2}[which]
         out = np.zeros(count)
         self._check(self._lib.rmd_debug_read(self._h, index, code, out.ctypes.data_as(C.POINTER(C.c_double))))
         return out

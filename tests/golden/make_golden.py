@@ -7,7 +7,7 @@ with this package's own reader and stores, per case, the parsed topology arrays,
 coordinates, the box, and the OpenMM energies and forces as one compressed `.npz`, so the
 tests and the GPU box never need the reference tree.
 
-Run from the repository root:  python tests/golden/make_golden.py [reference_root]
+Run from the repository root:  python tests/golden/make_golden.py <root of a RainMD checkout>
 """
 from __future__ import annotations
 
@@ -79,7 +79,9 @@ def save_dump(root: str, dump: str, prefix: str, out: dict, forces: bool):
 
 
 def main():
-    root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) != 2:
+        raise SystemExit("usage: python tests/golden/make_golden.py <root of a RainMD checkout>")
+    root = sys.argv[1]
     cases = {
         "ala-vac": [("ala-vac-nocutoff", True)],
         "ala-wat": [("ala-wat-pme", True), ("ala-wat-pme-free", True), ("ala-wat-pme-tail", False),
