@@ -141,70 +141,95 @@ def batched_block(steps: int, seed: int, single_steps: int = 200):
             "seed": seed}
 
 
-def learned_barostat_study(ps: float, seed: int = 3, warmup_moves: int = 2000):
+def blocking_se(series):
+    """Standard error of the mean of a correlated series by blocking (Flyvbjerg and Petersen,
+    J. Chem. Phys. 91, 461 (1989)): the series is halved into blocks of doubling length and the
+    naive error of the block means is taken at each level; the largest value over the levels
+    that keep at least 8 blocks is returned, so correlations shorter than the blocks are
+    counted."""
+    x = np.asarray(series, dtype=np.float64)
+    best = x.std(ddof=1) / math.sqrt(len(x)) if len(x) > 1 else 0.0
+    while len(x) >= 16:
+        x = 0.5 * (x[: len(x) // 2 * 2: 2] + x[1: len(x) // 2 * 2: 2])
+        best = max(best, x.std(ddof=1) / math.sqrt(len(x)))
+    return float(best)
+
+
+def learned_barostat_study(ps: float, seeds=(3, 4, 5), warmup_moves: int = 2000):
     """23,558 atoms (a 300-atom chain and TIP3P water) started underdense at 0.60 g/cm^3, NPT
-    at 1 bar and 300 K with a volume move every 25 steps, run twice from the same start: the
+    at 1 bar and 300 K with a volume move every 25 steps, run as pairs from the same start: the
     plain exact barostat and the learned one (pre-trained on the first `warmup_moves` exact
-    moves, then screening and training online). Density and isothermal compressibility from
-    the moves after the warm-up (the final four fifths of each run; the density trajectory by
-    tenths shows the relaxation from the underdense start); exact evaluations and wall time."""
+    moves, then screening and training online), one pair per seed. Density and isothermal
+    compressibility from the moves after the learned arm's warm-up (the final four fifths of
+    each run; the density trajectory by tenths shows the relaxation from the underdense start),
+    with the blocking-analysis standard error of each arm's mean density; per pair and pooled
+    over the pairs, the learned-minus-plain density difference in units of its combined
+    standard error; exact evaluations and wall time."""
     from rainmd_b200 import synthetic
     from rainmd_b200.simulation import GpuSimulation
     from rainmd_b200.topology import build_system
 
-    topo, pos = synthetic.solvated_chain(23558, 300, density=0.60, seed=seed)
-    system = build_system(topo, cutoff=0.9)
-    box = system["boxVectors"]
-    grid = [smooth_at_least(math.ceil(box[4 * d] / 0.1)) for d in range(3)]
-    mass = float(np.sum(system["topology"]["masses"]))
     steps = int(round(ps / TIMESTEP_PS))
     moves = steps // 25
     kT = 0.0083144626 * 300.0
-    out = {"study": "learned-barostat", "atoms": system["topology"]["atomCount"], "grid": grid,
-           "start_density_g_cm3": 0.60, "ps": ps, "moves": moves, "warmup_moves": warmup_moves,
-           "seed": seed}
-    for learned in (False, True):
-        options = options_for(grid, seed=seed)
-        options.update({"pressure": 1.0, "barostatInterval": 25, "learnedBarostat": 1 if learned else 0,
-                        "learnedWarmupMoves": warmup_moves})
-        sim = GpuSimulation(system, options)
-        sim.setState(pos)
-        sim.initialise()
-        sim.minimise(maxIterations=200, forceTolerance=1000.0)
-        volumes = []
-        t0 = time.perf_counter()
-        for _ in range(moves):
-            sim.run(25)
-            volumes.append(sim.diagnostics()["volume"])
-        wall = time.perf_counter() - t0
-        trajectory = mass / np.array(volumes) * 1.66053906660e-3  # g/cm^3 per move
-        # the moves after the learned arm's warm-up (the first fifth of the run; the density has
-        # relaxed from the underdense start well before that), the same window in both arms
-        v = np.array(volumes[len(volumes) // 5:])
-        density = mass / v * 1.66053906660e-3
-        blocks = np.array([b.mean() for b in np.array_split(density, 16)])
-        d = sim.diagnostics()
-        arm = {"density_by_tenth_of_run": [round(float(x.mean()), 4) for x in np.array_split(trajectory, 10)],
-               "density_g_cm3": float(density.mean()),
-               "density_se": float(blocks.std(ddof=1) / math.sqrt(len(blocks))),
-               # kappa_T = <dV^2> / (kT <V>): nm^3 / (kJ/mol) -> 1/bar is x 6.0221e-2
-               "compressibility_per_bar": float(v.var() / (kT * v.mean()) * 6.02214076e-2),
-               "attempts": d["barostat_attempts"], "accepted": d["barostat_accepted"],
-               "exact_evaluations": d["barostat_exact_evaluations"], "screened": d["barostat_screened"],
-               "window_nm3": d["volume_scale"], "wall_s": wall,
-               "ns_per_day_wall": ns_per_day(wall / (moves * 25))}
-        if learned:
-            r = sim.surrogateReport()
-            after = max(1, r["attempts"] - warmup_moves)
-            arm.update({"surrogate_prediction_error_kT": r["prediction_error_kT"],
-                        "surrogate_train_steps": r["train_steps"],
-                        "exact_saved_after_warmup": 1.0 - (r["exact_evaluations"] - warmup_moves) / after,
-                        "exact_saved_overall": 1.0 - r["exact_evaluations"] / max(1, r["attempts"])})
-        out["learned" if learned else "plain"] = arm
-        sim.release()
-    p, l = out["plain"], out["learned"]
-    out["density_difference_sigma"] = abs(p["density_g_cm3"] - l["density_g_cm3"]) / math.hypot(
-        p["density_se"], l["density_se"])
+    out = {"study": "learned-barostat", "ps": ps, "moves": moves, "warmup_moves": warmup_moves,
+           "seeds": list(seeds), "pairs": []}
+    for seed in seeds:
+        topo, pos = synthetic.solvated_chain(23558, 300, density=0.60, seed=seed)
+        system = build_system(topo, cutoff=0.9)
+        box = system["boxVectors"]
+        grid = [smooth_at_least(math.ceil(box[4 * d] / 0.1)) for d in range(3)]
+        mass = float(np.sum(system["topology"]["masses"]))
+        pair = {"seed": seed, "atoms": system["topology"]["atomCount"], "grid": grid, "start_density_g_cm3": 0.60}
+        for learned in (False, True):
+            options = options_for(grid, seed=seed)
+            options.update({"pressure": 1.0, "barostatInterval": 25, "learnedBarostat": 1 if learned else 0,
+                            "learnedWarmupMoves": warmup_moves})
+            sim = GpuSimulation(system, options)
+            sim.setState(pos)
+            sim.initialise()
+            sim.minimise(maxIterations=200, forceTolerance=1000.0)
+            volumes = []
+            t0 = time.perf_counter()
+            for _ in range(moves):
+                sim.run(25)
+                volumes.append(sim.diagnostics()["volume"])
+            wall = time.perf_counter() - t0
+            trajectory = mass / np.array(volumes) * 1.66053906660e-3  # g/cm^3 per move
+            v = np.array(volumes[len(volumes) // 5:])
+            density = mass / v * 1.66053906660e-3
+            d = sim.diagnostics()
+            arm = {"density_by_tenth_of_run": [round(float(x.mean()), 4) for x in np.array_split(trajectory, 10)],
+                   "density_g_cm3": float(density.mean()),
+                   "density_se": blocking_se(density),
+                   # kappa_T = <dV^2> / (kT <V>): nm^3 / (kJ/mol) -> 1/bar is x 6.0221e-2
+                   "compressibility_per_bar": float(v.var() / (kT * v.mean()) * 6.02214076e-2),
+                   "attempts": d["barostat_attempts"], "accepted": d["barostat_accepted"],
+                   "exact_evaluations": d["barostat_exact_evaluations"], "screened": d["barostat_screened"],
+                   "window_nm3": d["volume_scale"], "wall_s": wall,
+                   "ns_per_day_wall": ns_per_day(wall / (moves * 25))}
+            if learned:
+                r = sim.surrogateReport()
+                after = max(1, r["attempts"] - warmup_moves)
+                arm.update({"surrogate_prediction_error_kT": r["prediction_error_kT"],
+                            "surrogate_train_steps": r["train_steps"],
+                            "exact_saved_after_warmup": 1.0 - (r["exact_evaluations"] - warmup_moves) / after,
+                            "exact_saved_overall": 1.0 - r["exact_evaluations"] / max(1, r["attempts"])})
+            pair["learned" if learned else "plain"] = arm
+            sim.release()
+        p, l = pair["plain"], pair["learned"]
+        pair["difference_g_cm3"] = l["density_g_cm3"] - p["density_g_cm3"]
+        pair["difference_se"] = math.hypot(p["density_se"], l["density_se"])
+        pair["difference_sigma"] = pair["difference_g_cm3"] / pair["difference_se"]
+        out["pairs"].append(pair)
+    count = len(out["pairs"])
+    diff = sum(pp["difference_g_cm3"] for pp in out["pairs"]) / count
+    se = math.sqrt(sum(pp["difference_se"] ** 2 for pp in out["pairs"])) / count
+    out["pooled_difference_g_cm3"] = diff
+    out["pooled_difference_se"] = se
+    out["pooled_difference_sigma"] = diff / se
+    out["exact_saved_after_warmup_mean"] = float(np.mean([pp["learned"]["exact_saved_after_warmup"]
+                                                           for pp in out["pairs"]]))
     return out
 
 
@@ -435,21 +460,22 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
-# The pair kernel's arithmetic ceiling, reported beside its memory roofline. Every pair within
-# the cutoff is evaluated from both of its atoms (full neighbour rows), and one evaluation of the
-# force-only precision form issues, counted from the source of k_nonbonded: 49 FP32 operations,
-# 6 integer operations (three 64-bit fixed-point adds), 3 SFU operations (rsqrt, ex2, rcp) and
-# 3 float-to-int64 conversions. The ceiling is the larger of the issue time (one instruction per
-# lane per clock, 128 lanes per SM) and the SFU-and-conversion time (16 lanes per SM per clock)
-# on 148 SMs at the SM clock sampled during the run. List walking, loads, out-of-cutoff entries
-# and the exception loop are not counted, so the kernel cannot reach it.
+# The pair kernel's arithmetic ceiling, reported beside its memory roofline. The group-pair
+# kernel evaluates every pair within the cutoff once (the per-atom-row kernel twice, once from
+# each atom), and one evaluation of the force-only precision form issues, counted from the
+# kernels' source: 49 FP32 operations, 6 integer operations (three 64-bit fixed-point adds),
+# 3 SFU operations (rsqrt, ex2, rcp) and 3 float-to-int64 conversions. The ceiling is the larger
+# of the issue time (one instruction per lane per clock, 128 lanes per SM) and the
+# SFU-and-conversion time (16 lanes per SM per clock) on 148 SMs at the SM clock sampled during
+# the run. List walking, loads, out-of-cutoff entries, the partner's reduction and atomics and
+# the exception loop are not counted, so the kernel cannot reach it.
 PAIR_LANE_OPS = 49 + 6 + 3 + 3
 PAIR_XU_OPS = 3 + 3
 B200_SMS = 148
 
 
-def pair_arithmetic_ceiling(pairs, kernel_ms, sm_mhz):
-    evaluations = 2 * int(pairs)
+def pair_arithmetic_ceiling(pairs, kernel_ms, sm_mhz, evaluations_per_pair=1):
+    evaluations = evaluations_per_pair * int(pairs)
     clock = float(sm_mhz) * 1e6
     issue_s = evaluations * PAIR_LANE_OPS / (B200_SMS * 128 * clock)
     xu_s = evaluations * PAIR_XU_OPS / (B200_SMS * 16 * clock)
@@ -665,6 +691,8 @@ def main():
                         default=None,
                         help="run a study instead of the benchmark and print its JSON line")
     parser.add_argument("--ps", type=float, default=500.0, help="length of a study run")
+    parser.add_argument("--seeds", type=int, nargs="+", default=[3, 4, 5],
+                        help="seeds of the learned-barostat study's pairs of runs")
     parser.add_argument("--batch-steps", type=int, default=500)
     parser.add_argument("--rebuild-schedule", action="store_true",
                         help="rebuild the lists on the reference's host schedule instead of on demand "
@@ -679,7 +707,7 @@ def main():
         return
     if args.study == "learned-barostat":
         if rank == 0:
-            print(json.dumps(learned_barostat_study(args.ps)), flush=True)
+            print(json.dumps(learned_barostat_study(args.ps, seeds=tuple(args.seeds))), flush=True)
         return
     if args.study == "large-combined":
         if rank == 0:
@@ -737,9 +765,7 @@ def main():
     pairs = unique_pairs_within(out["positions"].astype(np.float64), out["boxVectors"][0], 0.9)
     nb_ms = sim.timeKernel("nonbonded", reps=50)
     shapes = sim.kernelShapes()
-    sim.setNonbonded(shapes["nonbondedLanes"], pairFixed=False)
-    nb_plain_ms = sim.timeKernel("nonbonded", reps=50)
-    sim.setNonbonded(shapes["nonbondedLanes"], pairFixed=True)
+    pair_list = sim.diagnostics()["pair_list"]
     pme_ms = sim.timeKernel("pme", reps=50)
     integ_ms = sim.timeKernel("integrate", reps=50)
     rebuild_ms = sim.timeKernel("rebuild", reps=20)
@@ -750,6 +776,17 @@ def main():
     peak, peak_kind = measured_peaks()
     achieved = bytes_nb / (nb_ms * 1e-3) / 1e9
     sim.release()
+    # the reference's per-atom rows on the same positions: their pair kernel (each pair from both
+    # atoms; the autotuned lanes, and the per-lane f32 form) and their search
+    from rainmd_b200.simulation import GpuSimulation
+    rows = GpuSimulation(system, dict(options_for(grid, seed=7 + rank), pairList=1))
+    rows.setState(out["positions"].astype(np.float64), out["velocities"].astype(np.float64))
+    rows.initialise()
+    atom_rows = {"nonbonded": rows.timeKernel("nonbonded", reps=50), "rebuild_kernels": rows.timeKernel("rebuild", reps=20),
+                 "kernel_shapes": {k: rows.kernelShapes()[k] for k in ("neighbourGroupAtoms", "nonbondedLanes")}}
+    rows.setNonbonded(atom_rows["kernel_shapes"]["nonbondedLanes"], pairFixed=False)
+    atom_rows["nonbonded_per_lane_f32"] = rows.timeKernel("nonbonded", reps=50)
+    rows.release()
 
     extra = {}
     if not args.no_extra:
@@ -772,7 +809,7 @@ def main():
     if not args.no_cpu_baseline:
         base = cpu_baseline(system, pos, grid, seed=1, npt=npt)
         base["single_thread"] = cpu_baseline(system, pos, grid, seed=1, budget_s=12.0, threads=1, npt=npt)
-    traffic = measured_traffic("k_nonbonded", args.workload)
+    traffic = measured_traffic("k_group_pairs" if pair_list != 1 else "k_nonbonded", args.workload)
     clock_summary = clocks.summary()
     clock_summary["window"] = "warm-up blocks (at least 1.5 s) and the timed region"
     sm_clock = clock_summary.get("sm_mhz") or clock_summary.get("sm_max_mhz") or 1965.0
@@ -786,16 +823,19 @@ def main():
                 "d2h_bytes_per_step": d2h / args.steps,
                 "path": "setState(host f64) + initialise + run(K) + readState(host f32)"},
         "gpu_launches": launches,
-        "roofline": {"bound": "hbm", "kernel": "k_nonbonded", "achieved": achieved, "peak": peak,
+        "roofline": {"bound": "hbm", "kernel": "k_group_pairs" if pair_list != 1 else "k_nonbonded",
+                     "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                      "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
                      "algorithmic_bytes": bytes_nb, "unique_pairs_within_cutoff": pairs,
                      "ms_per_launch": nb_ms,
-                     "arithmetic_ceiling": pair_arithmetic_ceiling(pairs, nb_ms, sm_clock)},
-        "kernels_ms": {"nonbonded": nb_ms, "nonbonded_per_lane_f32": nb_plain_ms,
-                       "pme_kernels": pme_ms, "integrate": integ_ms,
+                     "arithmetic_ceiling": pair_arithmetic_ceiling(pairs, nb_ms, sm_clock,
+                                                                   1 if pair_list != 1 else 2)},
+        "kernels_ms": {"nonbonded": nb_ms, "pme_kernels": pme_ms, "integrate": integ_ms,
                        "rebuild_kernels": rebuild_ms,
                        "pme_roofline_frac": bytes_pme / (pme_ms * 1e-3) / 1e9 / peak},
+        "pair_list": {0: "group-pair rows", 1: "per-atom rows", 2: "group-pair rows (+ per-atom rows)"}[pair_list],
+        "per_atom_rows_ms": atom_rows,
         "kernel_shapes": {k: shapes[k] for k in ("neighbourGroupAtoms", "nonbondedLanes", "spreadAtomsPerBlock")},
         "autotune_ms": shapes["tuned"],
         **extra,

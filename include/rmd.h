@@ -103,8 +103,11 @@ typedef struct {
                                    (order-independent, bitwise reproducible; default);
                                    1 = per-lane f32 partial sums, converted once per lane */
   /* kernel shapes; 0 = chosen by the engine's autotuner at initialise() */
-  int32_t neighbour_group_atoms; /* atoms per neighbour-search warp: 4, 8, 16 or 32 */
-  int32_t nonbonded_lanes;       /* lanes per atom in the pair loop: 8, 16 or 32 */
+  int32_t neighbour_group_atoms; /* atoms per neighbour-search warp: 4, 8, 16 or 32 (per-atom rows;
+                                    group-pair rows always search 4-atom groups) */
+  int32_t nonbonded_lanes;       /* lanes per atom in the pair loop: 8, 16 or 32 on per-atom rows;
+                                    on group-pair rows 8 lanes of each of the 1, 2, 4 or 8 warps
+                                    that share a group's row: 8, 16, 32 or 64 */
   int32_t spread_atoms_per_block; /* atoms per PME charge-spreading block: 4, 8 or 16 */
   /* learned barostat (learned_barostat = 1) */
   int32_t learned_warmup_moves;  /* exact moves that train the surrogate before it screens; <= 0: 2000 */
@@ -117,6 +120,15 @@ typedef struct {
    * rebuild_interval steps, adapted between blocks when adaptive_rebuild is set,
    * simulation.js:544-623). No reference counterpart. */
   int32_t rebuild_on_demand;
+  /* Which neighbour structure the pair loop walks. 0 (default): per 4-atom group of
+   * spatially close atoms, the half list of partner atoms within cutoff + skin of the group's
+   * bounding box, each pair evaluated once and its force added to both atoms (64-bit
+   * fixed-point atomics for the partner); needs force_accumulation 0 and at most 2^23 atoms
+   * in the handle, else 1 is used. 1: the reference's full per-atom rows (neighbours.js:46-151),
+   * each pair evaluated from both atoms. 2: as 0, and every build also writes the per-atom
+   * rows (for inspection with rmd_debug_neighbours). Both structures give the same forces
+   * bit for bit. No reference counterpart. */
+  int32_t pair_list;
 } rmd_options;
 
 #define RMD_NO_PRESSURE (-1.0e300)
@@ -182,6 +194,7 @@ typedef struct {
   int64_t device_bytes;
   int64_t list_builds;       /* neighbour-list builds so far (every system of a handle builds together) */
   int32_t rebuild_on_demand; /* the option in effect */
+  int32_t pair_list;         /* the neighbour structure in effect (rmd_options.pair_list) */
 } rmd_diagnostics_report;
 
 /* Fills `options` with the reference's defaults. */
@@ -302,6 +315,16 @@ rmd_status rmd_debug_evaluate(rmd_sim *sim, int32_t system_index, rmd_energy_rep
 /* Forces of one term alone at the current positions and list: 0 direct space with the
  * exceptions, 1 bonded and restraints, 2 PME reciprocal space. */
 rmd_status rmd_debug_force_term(rmd_sim *sim, int32_t system_index, int32_t term, double *forces);
+/* The group-pair rows (pair_list 0 or 2) of one system, mapped to the system's own atom
+ * indices: the number of group slots and the row capacity (call with the arrays NULL for
+ * these), then per group slot its GROUP_ATOMS (4) atoms (-1 past the end of a short group or
+ * for an unused slot), its row length, and per entry [groups x capacity] the partner atom, the
+ * lattice image code (ka+1)*9+(kb+1)*3+(kc+1) of the partner's image (d = x_i - x_j - S) and
+ * the 4-bit mask of group atoms that skip the entry. For parity tests. */
+rmd_status rmd_debug_group_rows(rmd_sim *sim, int32_t system_index, int32_t *groups, int32_t *capacity,
+                                int32_t *atoms, int32_t *counts, int32_t *partners, int32_t *codes,
+                                int32_t *masks);
+
 /* Copy a work buffer: 0 the real grid of the last evaluation after the inverse transform
  * (K^3 doubles), 1 its half spectrum (2*Kx*Ky*(Kz/2+1) doubles), 2 the positions the current
  * neighbour list was built from (3N doubles, the f32 values exactly; the displacement
@@ -365,8 +388,8 @@ rmd_status rmd_surrogate_evaluate(const float *params, const float *inputs, cons
 /* Kernel launch shapes in use: shapes = {atoms per neighbour-search warp, lanes per atom in
  * the pair loop, atoms per PME spreading block}. When the options left a shape at 0,
  * initialise() chose it by timing every candidate (the engine's autotuner); tune_ms (may be
- * NULL) receives those times in ms per launch, in the order group 4/8/16, lanes 8/16/32,
- * spreading 4/8/16, with -1 for shapes that were not tuned. No reference counterpart: the
+ * NULL) receives those times in ms per launch, in the order group 4/8/16, lanes 8/16/32
+ * (16/32/64 on group-pair rows), spreading 4/8/16, with -1 for shapes that were not tuned. No reference counterpart: the
  * reference's WGSL kernels have fixed workgroup sizes. */
 rmd_status rmd_kernel_shapes(const rmd_sim *sim, int32_t shapes[3], double tune_ms[9]);
 /* Set launch shapes by hand (0 keeps the current one). Results do not depend on them, except

@@ -54,7 +54,7 @@ class RmdOptions(C.Structure):
         ("force_accumulation", C.c_int32), ("neighbour_group_atoms", C.c_int32),
         ("nonbonded_lanes", C.c_int32), ("spread_atoms_per_block", C.c_int32),
         ("learned_warmup_moves", C.c_int32), ("learned_steps_per_move", C.c_int32),
-        ("learned_rate", C.c_double), ("rebuild_on_demand", C.c_int32),
+        ("learned_rate", C.c_double), ("rebuild_on_demand", C.c_int32), ("pair_list", C.c_int32),
     ]
 
 
@@ -116,7 +116,7 @@ class RmdDiagnostics(C.Structure):
         ("tolerance_floor", C.c_double), ("cell_counts", C.c_int32 * 3),
         ("pme_grid", C.c_int32 * 3), ("pme_alpha", C.c_double), ("pme_order", C.c_int32),
         ("cluster_count", C.c_int32), ("settle_count", C.c_int32), ("device_bytes", C.c_int64),
-        ("list_builds", C.c_int64), ("rebuild_on_demand", C.c_int32),
+        ("list_builds", C.c_int64), ("rebuild_on_demand", C.c_int32), ("pair_list", C.c_int32),
     ]
 
 
@@ -141,7 +141,7 @@ EXPORTS = [
     "rmd_kernel_shapes", "rmd_set_kernel_shapes", "rmd_surrogate_report_at", "rmd_surrogate_weights",
     "rmd_surrogate_evaluate", "rmd_image_molecules_at", "rmd_dcd_frame_bytes", "rmd_dcd_frame_at",
     "rmd_dcd_header", "rmd_restart_at", "rmd_render_at", "rmd_render_positions", "rmd_plan_system",
-    "rmd_grown_capacity", "rmd_debug_draws",
+    "rmd_grown_capacity", "rmd_debug_draws", "rmd_debug_group_rows",
 ]
 
 _lib = None
@@ -226,6 +226,7 @@ def load():
     lib.rmd_grown_capacity.argtypes = [C.c_int32, C.c_int32]
     lib.rmd_grown_capacity.restype = C.c_int32
     lib.rmd_debug_draws.argtypes = [C.c_uint32, C.c_uint32, C.c_int32, C.c_uint32, _fp, _fp]
+    lib.rmd_debug_group_rows.argtypes = [sim, C.c_int32, _i32p, _i32p, _i32p, _i32p, _i32p, _i32p, _i32p]
     for name in EXPORTS:
         fn = getattr(lib, name)
         if fn.restype is C.c_int and name not in ("rmd_system_count",):

@@ -42,7 +42,8 @@ struct DevSys {
   int cell_capacity;    // cells allocated for this system
   int group_base;       // first neighbour-search group slot of this system
   long long nbr_base;   // offset of row 0 in the neighbour array
-  int nbr_capacity;
+  int nbr_capacity;     // entries a row holds (per-atom rows and group rows alike)
+  long long gnbr_base;  // offset of group slot 0's row in the group-pair array
   int grid[3];
   long long grid_base;  // real grid offset (K^3)
   long long half_base;  // complex half-spectrum offset (Kx*Ky*(Kz/2+1))
@@ -299,6 +300,18 @@ __device__ __forceinline__ void bspline(float u, float *w, float *dw) {
 __device__ __forceinline__ int shift_code(int ka, int kb, int kc) { return (ka + 1) * 9 + (kb + 1) * 3 + (kc + 1); }
 constexpr int NBR_SLOT_BITS = 27;
 constexpr int NBR_SLOT_MASK = (1 << NBR_SLOT_BITS) - 1;
+
+// Group-pair rows (pair_list 0/2): atoms are taken GROUP_ATOMS at a time (a search group: spatially
+// close atoms of one cell in sub-cell order); a group's row lists each partner atom once, as
+// slot | image code << 23 | mask << 28, where bit a of the 4-bit mask says that the group's atom
+// a must skip this partner (an excluded pair, or a pair inside the group seen from its other
+// atom). A pair of atoms in different groups is listed only in the row of the group that comes
+// first in search order, so every pair is evaluated once.
+constexpr int GROUP_ATOMS = 4;
+constexpr int GROUP_SLOT_BITS = 23;
+constexpr int GROUP_SLOT_MASK = (1 << GROUP_SLOT_BITS) - 1;
+constexpr int GROUP_CODE_SHIFT = 23;
+constexpr int GROUP_MASK_SHIFT = 28;
 
 __device__ __forceinline__ int wrap_index(int v, int n) {
   int r = v % n;

@@ -210,6 +210,12 @@ struct Engine {
   DevArray<int> cell_gstart, group_order, group_sys;
   int n_groups_total = 0;
   DevArray<int> nbr, nbr_count, required, required_max, stale;
+  // group-pair rows (pair_list 0 and 2): rows, lengths, first order position and atoms per group
+  // slot; per slot its partner record and order position; per-atom integer energy sums
+  int pair_list = 1;
+  DevArray<int> gnbr, gnbr_count, gfirst, gsize, order_pos;
+  DevArray<int2> slot_info;
+  DevArray<unsigned long long> e_acc;
   // list builds counted on the device: [0] those an IF node took, [1] all of them
   DevArray<unsigned long long> list_builds;
   unsigned long long conditional_builds_seen = 0;
@@ -309,8 +315,10 @@ struct Engine {
   void autotune();
   void drop_graphs();
   int check_capacity();  // returns max required; grows if needed
+  bool capacity_grew = false;  // the last check_capacity grew the lists (and rebuilt them, forces only)
   void run(int64_t count, int block, const volatile int32_t *stop);
   void run_block(int n, bool barostat, bool energy_last);
+  std::map<std::string, cudaGraphExec_t>::iterator block_graph(int n, bool barostat, bool energy_last);
   // timing hooks for run(): events around each block's graph, optional L2 flush between
   cudaEvent_t ev_a = nullptr, ev_b = nullptr;
   bool timing = false, flush = false;
@@ -473,6 +481,11 @@ void Engine::build(int count, const rmd_system *systems, const rmd_options *opti
   }
   pme_order = hs[0].order;
   pair_fixed = options[0].force_accumulation == 1 ? 0 : 1;
+  // the group-pair rows need the precision form (every pair force quantised) and slot indices
+  // that fit their 23 bits; otherwise the per-atom rows
+  pair_list = options[0].pair_list;
+  if (pair_list != 1 && pair_list != 2) pair_list = 0;
+  if (!pair_fixed || N > GROUP_SLOT_MASK) pair_list = 1;
   {
     const rmd_options &o = options[0];
     auto pick = [](int v, int a, int b, int c, int dflt) { return v == a || v == b || v == c ? v : dflt; };
@@ -482,6 +495,11 @@ void Engine::build(int count, const rmd_system *systems, const rmd_options *opti
     tune_group = o.neighbour_group_atoms == 0;
     tune_lanes = o.nonbonded_lanes == 0;
     tune_spread = o.spread_atoms_per_block == 0;
+    if (pair_list != 1) {  // group-pair rows: 4-atom search groups; lanes per group atom 8 x the
+      group_atoms = GROUP_ATOMS;  // warps that share a row (16, 32 or 64)
+      nb_lanes = o.nonbonded_lanes == 64 ? 64 : pick(o.nonbonded_lanes, 8, 16, 32, 32);
+      tune_group = false;
+    }
   }
   for (auto &h : hs)
     if (h.order != pme_order) throw Error(RMD_ERR_INVALID, "every system of a batch must use the same PME order");
@@ -881,9 +899,15 @@ void Engine::upload_all(const std::vector<const rmd_system *> &src) {
   sorted_orig.zero();
   sorted_type.alloc(N);
   sorted_type.zero();
+  slot_info.alloc(N);
+  slot_info.zero();
+  order_pos.alloc(N);
+  order_pos.zero();
+  e_acc.alloc(3 * (size_t)N);
+  e_acc.zero();
   rank.alloc(N);
   rank.zero();
-  required.alloc(S);
+  required.alloc(2 * (size_t)S);  // longest per-atom row, then longest group-pair row, per system
   required.zero();
   required_max.alloc(S);
   required_max.zero();
@@ -1126,22 +1150,33 @@ void Engine::upload_all(const std::vector<const rmd_system *> &src) {
 }
 
 void Engine::allocate_neighbours() {
-  long long total = 0;
+  long long total = 0, group_total = 0;
   for (int s = 0; s < S; ++s) {
     h_sys[s].nbr_base = total;
     h_sys[s].nbr_capacity = hs[s].capacity;
     total += (long long)hs[s].n * hs[s].capacity;
+    const int groups = (s + 1 < S ? h_sys[s + 1].group_base : n_groups_total) - h_sys[s].group_base;
+    h_sys[s].gnbr_base = group_total;
+    if (pair_list != 1) group_total += (long long)groups * hs[s].capacity;
   }
-  nbr.alloc(total);
+  // per-atom rows only where the pair loop or an inspection reads them
+  nbr.alloc(pair_list == 0 ? 1 : total);
   nbr.zero();
   nbr_count.alloc(N);
   nbr_count.zero();
+  gnbr.alloc(std::max<long long>(1, group_total));
+  gnbr.zero();
+  for (auto *a : {&gnbr_count, &gfirst, &gsize}) {
+    a->alloc(std::max(1, n_groups_total));
+    a->zero();
+  }
   // push only the neighbour fields (the box may have been changed on the device)
   std::vector<DevSys> cur(S);
   CUDA_OK(cudaMemcpy(cur.data(), sys.p, sizeof(DevSys) * S, cudaMemcpyDeviceToHost));
   for (int s = 0; s < S; ++s) {
     cur[s].nbr_base = h_sys[s].nbr_base;
     cur[s].nbr_capacity = h_sys[s].nbr_capacity;
+    cur[s].gnbr_base = h_sys[s].gnbr_base;
   }
   CUDA_OK(cudaMemcpy(sys.p, cur.data(), sizeof(DevSys) * S, cudaMemcpyHostToDevice));
   h_sys = cur;
@@ -1176,6 +1211,14 @@ LaunchCtx Engine::ctx() const {
   c.nbr = nbr.p;
   c.nbr_count = nbr_count.p;
   c.required = required.p;
+  c.pair_list = pair_list;
+  c.gnbr = gnbr.p;
+  c.gnbr_count = gnbr_count.p;
+  c.gfirst = gfirst.p;
+  c.gsize = gsize.p;
+  c.slot_info = slot_info.p;
+  c.order_pos = order_pos.p;
+  c.e_acc = e_acc.p;
   c.origin = origin.p;
   c.spos = spos.p;
   c.wrap = wrap.p;
@@ -1355,7 +1398,7 @@ void Engine::record_forces(int rebuild, bool energy) {
   if (rebuild == REBUILD_FORCED) {
     launch_rebuild_reset(required.p, required_max.p, disp.p, S, list_builds.p + 1, nullptr, stream);  // disp slot 0: since rebuild
     launch_rebuild(c, stream);
-    recorded += 6;
+    recorded += 1 + rebuild_launches(c);
   } else if (rebuild == REBUILD_IF_STALE) {
     record_conditional_rebuild(c);
   }
@@ -1365,7 +1408,7 @@ void Engine::record_forces(int rebuild, bool energy) {
     CUDA_OK(cudaStreamWaitEvent(stream, ev_join, 0));
     launch_pme_gather(c, stream);
   }
-  recorded += 1 + (n_bonds + n_angles + n_tors + n_rest > 0 ? 1 : 0) + pme_launches(c);
+  recorded += nonbonded_launches(c, energy) + (n_bonds + n_angles + n_tors + n_rest > 0 ? 1 : 0) + pme_launches(c);
   if (energy) {
     launch_molecular_virial(c, stream);
     launch_energy_reduce(segments.p, n_segments, seg_out.p, energies.p, sysd.p, S, stream);
@@ -1376,7 +1419,7 @@ void Engine::record_forces(int rebuild, bool energy) {
 // The rebuild as the body of an IF node of the graph being captured on `stream`: a one-block
 // kernel sets the condition from the displacement the integrator just reduced, and the body
 // (reset + cell and neighbour kernels) is captured into the node's child graph on `cond`.
-// The body's six kernels are counted when they run (list_builds), not here.
+// The body's kernels are counted when they run (list_builds), not here.
 void Engine::record_conditional_rebuild(const LaunchCtx &c) {
   cudaStreamCaptureStatus status;
   cudaGraph_t graph;
@@ -1456,9 +1499,16 @@ void Engine::set_state(int s, const double *pos, const double *vel_in, int64_t s
 }
 
 int Engine::check_capacity() {
-  // the last build's requirement, and the largest of the builds before it since the last check
+  // the last build's requirement, and the largest of the builds before it since the last check;
+  // the rows the pair loop walks are what diagnostics report
   std::vector<int> req(S), earlier(S);
-  CUDA_OK(cudaMemcpy(req.data(), required.p, sizeof(int) * S, cudaMemcpyDeviceToHost));
+  auto read_required = [&]() {
+    std::vector<int> both(2 * (size_t)S);
+    CUDA_OK(cudaMemcpy(both.data(), required.p, sizeof(int) * both.size(), cudaMemcpyDeviceToHost));
+    for (int s = 0; s < S; ++s) req[s] = std::max(both[s], both[S + s]);
+  };
+  read_required();
+  capacity_grew = false;
   CUDA_OK(cudaMemcpy(earlier.data(), required_max.p, sizeof(int) * S, cudaMemcpyDeviceToHost));
   CUDA_OK(cudaMemset(required_max.p, 0, sizeof(int) * S));
   bool grow = false;
@@ -1479,7 +1529,8 @@ int Engine::check_capacity() {
     evaluate(true, false);
     sync();
     CUDA_OK(cudaMemset(required_max.p, 0, sizeof(int) * S));
-    CUDA_OK(cudaMemcpy(req.data(), required.p, sizeof(int) * S, cudaMemcpyDeviceToHost));
+    read_required();
+    capacity_grew = true;
     for (int s = 0; s < S; ++s) {
       if (req[s] > hs[s].capacity)
         throw Error(RMD_ERR_NEIGHBOUR_OVERFLOW,
@@ -1521,7 +1572,7 @@ void Engine::autotune() {
     if (std::array<int, 3>{group_atoms, nb_lanes, spread_atoms} != before) drop_graphs();
   };
   std::string key = std::to_string(S) + ":" + std::to_string(N) + ":" + std::to_string(n_cells_total) + ":" +
-                    std::to_string(pme_order) + ":" + std::to_string(pair_fixed);
+                    std::to_string(pme_order) + ":" + std::to_string(pair_fixed) + ":" + std::to_string(pair_list);
   for (auto &h : hs) key += ":" + std::to_string(h.grid[0] * 100000LL + h.grid[1] * 1000LL + h.grid[2]);
   {
     std::lock_guard<std::mutex> lock(g_tune_mutex);
@@ -1548,7 +1599,9 @@ void Engine::autotune() {
     CUDA_OK(cudaEventElapsedTime(&ms, a, b));
     return (double)ms / reps;
   };
-  const int groups[3] = {4, 8, 16}, lanes[3] = {8, 16, 32}, spreads[3] = {4, 8, 16};
+  const int groups[3] = {4, 8, 16}, spreads[3] = {4, 8, 16};
+  int lanes[3] = {8, 16, 32};
+  if (pair_list != 1) lanes[0] = 16, lanes[1] = 32, lanes[2] = 64;  // 2, 4 or 8 warps a group row
   if (tune_group) {
     double best = 1e30;
     int pick = group_atoms;
@@ -1611,7 +1664,9 @@ void Engine::initialise() {
   sync();
 }
 
-void Engine::run_block(int n, bool barostat, bool energy_last) {
+// The captured graph of a block of n steps (with a volume move first, and an energy-enabled
+// last evaluation), captured and instantiated on first use and kept by its rebuild pattern.
+std::map<std::string, cudaGraphExec_t>::iterator Engine::block_graph(int n, bool barostat, bool energy_last) {
   // rebuild pattern, identical for every system of the batch (the smallest interval wins)
   int interval = 1 << 30;
   int64_t since = 1LL << 40;
@@ -1619,14 +1674,18 @@ void Engine::run_block(int n, bool barostat, bool energy_last) {
     interval = std::min(interval, h.rebuild_interval);
     since = std::min<int64_t>(since, h.steps_since_rebuild);
   }
-  if (barostat) since = 1LL << 40;
+  // A volume move's trial evaluation rebuilds the lists at the scaled positions and restarts
+  // the displacement check from them: an accepted move keeps them, and after a rejected one the
+  // check sees the restored positions' distance from the trial ones, so on demand the step after
+  // a move asks the device like any other. The host schedule rebuilds after every move.
+  if (barostat && !on_demand) since = 1LL << 40;
   std::string key = "n" + std::to_string(n) + (barostat ? "B" : "") + (energy_last ? "E" : "") + ":";
   std::vector<char> rebuild(n, REBUILD_NONE);
   if (on_demand) {
     // a list from before a box change, a new state or a capacity change is not measured by
     // the displacement check: build it; every other step asks the device
     for (int k = 0; k < n; ++k) rebuild[k] = REBUILD_IF_STALE;
-    if (since >= (1LL << 39)) rebuild[0] = REBUILD_FORCED;
+    if (since >= (1LL << 39) && !barostat) rebuild[0] = REBUILD_FORCED;
     key += rebuild[0] == REBUILD_FORCED ? "F" : "C";
   } else {
     for (int k = 0; k < n; ++k) {
@@ -1661,10 +1720,18 @@ void Engine::run_block(int n, bool barostat, bool energy_last) {
     CUDA_OK(cudaGraphDestroy(graph));
     it = graphs.emplace(key, exec).first;
   }
+  return it;
+}
+
+void Engine::run_block(int n, bool barostat, bool energy_last) {
+  auto it = block_graph(n, barostat, energy_last);
+  const std::string key = it->first;
   CUDA_OK(cudaGraphLaunch(it->second, stream));
   kernel_launches += graph_launches[key];
   energy_fresh = energy_last;
   // host bookkeeping mirrors the device
+  int interval = 1 << 30;
+  for (auto &h : hs) interval = std::min(interval, h.rebuild_interval);
   for (auto &h : hs) {
     int64_t s2 = barostat ? (1LL << 40) : h.steps_since_rebuild;
     if (on_demand) {
@@ -1689,7 +1756,7 @@ void Engine::check_block(int steps) {
   if (on_demand) {  // the rebuild bodies that ran inside the block's graph
     unsigned long long taken = 0;
     CUDA_OK(cudaMemcpy(&taken, list_builds.p, sizeof taken, cudaMemcpyDeviceToHost));
-    kernel_launches += 6LL * (long long)(taken - conditional_builds_seen);
+    kernel_launches += (1LL + rebuild_launches(ctx())) * (long long)(taken - conditional_builds_seen);
     conditional_builds_seen = taken;
   }
   for (int s = 0; s < S; ++s) {
@@ -1759,6 +1826,9 @@ void Engine::run(int64_t count, int block, const volatile int32_t *stop) {
     // the events bracket all of the block's device work: the energy evaluation and the
     // surrogate screening before a volume move, the block's graph and the training after it
     if (timing) {
+      // the block's graph is captured (on first use) before the events, so host-side capture
+      // and instantiation are never timed as device work
+      block_graph(n, exact_move, next_due);
       if (flush) CUDA_OK(cudaMemsetAsync(flush_buffer.p, (int)(kernel_launches & 0xff), flush_buffer.n, stream));
       CUDA_OK(cudaEventRecord(ev_a, stream));
     }
@@ -1914,6 +1984,10 @@ double Engine::scale_volume(int s, double ls) {
   sync();
   for (auto &h : hs) h.steps_since_rebuild = 0;
   check_capacity();
+  if (capacity_grew) {  // the first evaluation dropped pairs: its energy is not the potential
+    evaluate(false, true);
+    sync();
+  }
   return read_energies()[(size_t)s * N_ENERGY + E_POTENTIAL];
 }
 
@@ -2129,6 +2203,7 @@ void rmd_default_options(rmd_options *o) {
   o->neighbour_slack = 2.0;
   o->ewald_tolerance = 5e-4;
   o->pme_order = 5;
+  o->pair_list = 1;
 }
 
 rmd_status rmd_plan_system(const rmd_system *system, const rmd_options *options, rmd_plan *out) {
@@ -2370,13 +2445,14 @@ rmd_status rmd_diagnostics_at(rmd_sim *sim, int32_t s, rmd_diagnostics_report *o
     out->cluster_count = h.n_clusters;
     out->settle_count = h.n_settle;
     size_t bytes = 0;
-    bytes += e.posq.bytes() * 4 + e.force.bytes() * 2 + e.nbr.bytes() + e.fixed_grid.bytes() + e.half.bytes() +
+    bytes += e.posq.bytes() * 4 + e.force.bytes() * 2 + e.nbr.bytes() + e.gnbr.bytes() + e.fixed_grid.bytes() + e.half.bytes() +
              e.real_grid.bytes() + e.cell_atoms.bytes() * 2 + e.e_lj.bytes() * 4;
     out->device_bytes = (int64_t)bytes;
     unsigned long long builds[2] = {0, 0};
     CUDA_OK(cudaMemcpy(builds, e.list_builds.p, sizeof builds, cudaMemcpyDeviceToHost));
     out->list_builds = (int64_t)builds[1];
     out->rebuild_on_demand = e.on_demand ? 1 : 0;
+    out->pair_list = e.pair_list;
   });
 }
 
@@ -2418,6 +2494,9 @@ rmd_status rmd_debug_neighbours(rmd_sim *sim, int32_t s, int32_t *capacity, int3
   return guarded(sim, [&]() {
     auto &e = sim->engine;
     e.sync();
+    if (e.pair_list == 0)
+      throw rmd::Error(RMD_ERR_INVALID, "the per-atom rows are not built with pair_list 0 (group-pair rows); create "
+                                        "the simulation with pair_list 2 to build and inspect them");
     const auto &h = e.hs[s];
     const auto &ds = e.h_sys[s];
     if (capacity) *capacity = ds.nbr_capacity;
@@ -2439,6 +2518,48 @@ rmd_status rmd_debug_neighbours(rmd_sim *sim, int32_t s, int32_t *capacity, int3
         }
     }
     if (req) CUDA_OK(cudaMemcpy(req, e.required.p + s, sizeof(int), cudaMemcpyDeviceToHost));
+  });
+}
+
+rmd_status rmd_debug_group_rows(rmd_sim *sim, int32_t s, int32_t *groups, int32_t *capacity, int32_t *atoms,
+                                int32_t *counts, int32_t *partners, int32_t *codes, int32_t *masks) {
+  if (rmd_status c = check_index(sim, s)) return c;
+  return guarded(sim, [&]() {
+    auto &e = sim->engine;
+    e.sync();
+    if (e.pair_list == 1)
+      throw rmd::Error(RMD_ERR_INVALID, "this simulation walks per-atom rows (pair_list 1): it has no group-pair rows");
+    const auto &h = e.hs[s];
+    const auto &ds = e.h_sys[s];
+    const int first = ds.group_base;
+    const int n = (s + 1 < e.S ? e.h_sys[s + 1].group_base : e.n_groups_total) - first;
+    const int cap = ds.nbr_capacity;
+    if (groups) *groups = n;
+    if (capacity) *capacity = cap;
+    if (!atoms && !counts && !partners) return;
+    std::vector<int> size(n), start(n), cnt(n), order(h.n), orig(h.n), raw((size_t)n * cap);
+    CUDA_OK(cudaMemcpy(size.data(), e.gsize.p + first, sizeof(int) * n, cudaMemcpyDeviceToHost));
+    CUDA_OK(cudaMemcpy(start.data(), e.gfirst.p + first, sizeof(int) * n, cudaMemcpyDeviceToHost));
+    CUDA_OK(cudaMemcpy(cnt.data(), e.gnbr_count.p + first, sizeof(int) * n, cudaMemcpyDeviceToHost));
+    CUDA_OK(cudaMemcpy(order.data(), e.group_order.p + h.atom_start, sizeof(int) * h.n, cudaMemcpyDeviceToHost));
+    CUDA_OK(cudaMemcpy(orig.data(), e.sorted_orig.p + h.atom_start, sizeof(int) * h.n, cudaMemcpyDeviceToHost));
+    CUDA_OK(cudaMemcpy(raw.data(), e.gnbr.p + ds.gnbr_base, sizeof(int) * raw.size(), cudaMemcpyDeviceToHost));
+    // slots and order positions are global: map both back to the system's own atom indices
+    auto atom_of_slot = [&](int slot) { return orig[slot - h.atom_start] - h.atom_start; };
+    for (int q = 0; q < n; ++q) {
+      for (int a = 0; a < rmd::GROUP_ATOMS; ++a)
+        if (atoms)
+          atoms[q * rmd::GROUP_ATOMS + a] =
+              a < size[q] ? atom_of_slot(order[start[q] + a - h.atom_start]) : -1;
+      if (counts) counts[q] = size[q] > 0 ? cnt[q] : 0;
+      for (int k = 0; k < cap; ++k) {
+        const bool used = size[q] > 0 && k < cnt[q];
+        const unsigned entry = (unsigned)raw[(size_t)q * cap + k];
+        if (partners) partners[(size_t)q * cap + k] = used ? atom_of_slot((int)(entry & rmd::GROUP_SLOT_MASK)) : -1;
+        if (codes) codes[(size_t)q * cap + k] = used ? (int)((entry >> rmd::GROUP_CODE_SHIFT) & 31u) : 0;
+        if (masks) masks[(size_t)q * cap + k] = used ? (int)(entry >> rmd::GROUP_MASK_SHIFT) : 0;
+      }
+    }
   });
 }
 
@@ -2726,10 +2847,14 @@ rmd_status rmd_set_kernel_shapes(rmd_sim *sim, int32_t group_atoms, int32_t nonb
                                  int32_t spread_atoms) {
   if (!sim) return RMD_ERR_INVALID;
   auto ok = [](int v, int a, int b, int c) { return v == 0 || v == a || v == b || v == c; };
-  if (!(ok(group_atoms, 4, 8, 16) || group_atoms == 32) || !ok(nonbonded_lanes, 8, 16, 32) ||
+  if (!(ok(group_atoms, 4, 8, 16) || group_atoms == 32) || !(ok(nonbonded_lanes, 8, 16, 32) || nonbonded_lanes == 64) ||
       !ok(spread_atoms, 4, 8, 16))
     return RMD_ERR_INVALID;
   auto &e = sim->engine;
+  if (e.pair_list != 1 && group_atoms && group_atoms != rmd::GROUP_ATOMS) {
+    e.last_error = "with group-pair rows the search groups hold 4 atoms";
+    return RMD_ERR_INVALID;
+  }
   if (group_atoms) e.group_atoms = group_atoms;
   if (nonbonded_lanes) e.nb_lanes = nonbonded_lanes;
   if (spread_atoms) e.spread_atoms = spread_atoms;
@@ -2740,6 +2865,10 @@ rmd_status rmd_set_kernel_shapes(rmd_sim *sim, int32_t group_atoms, int32_t nonb
 rmd_status rmd_debug_set_nonbonded(rmd_sim *sim, int32_t lanes, int32_t pair_fixed) {
   if (!sim || (lanes != 8 && lanes != 16 && lanes != 32)) return RMD_ERR_INVALID;
   auto &e = sim->engine;
+  if (e.pair_list != 1) {
+    e.last_error = "the pair-loop shape and accumulation form can only be changed on per-atom rows (pair_list 1)";
+    return RMD_ERR_INVALID;
+  }
   e.nb_lanes = lanes;
   e.pair_fixed = pair_fixed ? 1 : 0;
   for (auto &kv : e.graphs) cudaGraphExecDestroy(kv.second);

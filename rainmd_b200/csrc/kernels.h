@@ -93,6 +93,14 @@ struct LaunchCtx {
   const int *excl_start, *excl_partners;
   int *nbr, *nbr_count, *required;
   float4 *origin;
+  // 0: the pair loop walks group-pair rows; 1: per-atom rows; 2: group-pair rows, and every
+  // build also writes the per-atom rows (rmd_options.pair_list)
+  int pair_list;
+  int *gnbr, *gnbr_count;  // group-pair rows and their lengths, per group slot
+  int *gfirst, *gsize;     // per group slot: its first position in group_order, its atoms (0: unused)
+  int2 *slot_info;         // per slot: LJ type, original index
+  int *order_pos;          // per slot: its position in group_order
+  unsigned long long *e_acc;  // per-atom integer energy sums of the group-pair kernel (3 N)
   // cell-ordered copies written at each rebuild and kept current by the integrator:
   // spos[slot] = position minus the atom's wrap shift (w = charge), the original index,
   // the LJ type; rank[atom] = slot and wrap[atom] = that shift
@@ -155,6 +163,7 @@ struct LaunchCtx {
 };
 
 void launch_rebuild(const LaunchCtx &c, cudaStream_t stream);
+int rebuild_launches(const LaunchCtx &c);  // kernels launch_rebuild issues (without the reset)
 // Rebuild on demand (lists.cu): flag the systems that have moved past half their skin since
 // their last build and set `handle` (an IF node's condition) when any has; and the reset every
 // rebuild starts with (of the flagged systems, or of all when `only` is null).
@@ -165,6 +174,7 @@ void launch_rebuild_reset(int *required, int *required_max, unsigned *disp, int 
 // group slots a system needs for a given group size (its search groups never exceed this)
 int neighbour_group_slots(int atoms, int cells, int group_atoms);
 void launch_nonbonded(const LaunchCtx &c, bool energy, int lanes, cudaStream_t stream);
+int nonbonded_launches(const LaunchCtx &c, bool energy);  // kernels launch_nonbonded issues
 void launch_bonded(const LaunchCtx &c, bool energy, cudaStream_t stream);
 void launch_molecular_virial(const LaunchCtx &c, cudaStream_t stream);
 void launch_pme(const LaunchCtx &c, bool energy, cudaStream_t stream);

@@ -26,6 +26,8 @@ struct LaunchCtxView {
   float4 *wrap;
   int *sorted_orig, *sorted_type, *rank;
   int *group_order;
+  int2 *slot_info;  // per slot: LJ type, original index (the group-pair kernel's partner record)
+  int *order_pos;   // per slot: its position in group_order
 };
 
 __global__ void k_cells_assign(const float4 *__restrict__ posq, const int *__restrict__ sys_of_atom,
@@ -114,9 +116,45 @@ __global__ void k_cells_scatter(const int *__restrict__ sys_of_atom, const DevSy
   cell_atoms[s.atom_start + slot] = i;
 }
 
+// Index of sub-cell (x, y, z) of a 4x4x4 grid along a 3D Hilbert curve (J. Skilling, "Programming
+// the Hilbert curve", AIP Conf. Proc. 707, 381 (2004): axes to transposed index, then the bits
+// interleaved): consecutive indices are face-adjacent sub-cells, so consecutive atoms in this
+// order stay close (a Z-order curve jumps across the cell between its octants, which made some
+// 4-atom search groups a cell wide).
+__device__ __forceinline__ int hilbert_key(int x, int y, int z) {
+  constexpr int BITS = 2;
+  int X[3] = {x, y, z};
+#pragma unroll
+  for (int q = 1 << (BITS - 1); q > 1; q >>= 1) {
+    const int p = q - 1;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      if (X[i] & q) {
+        X[0] ^= p;
+      } else {
+        const int t = (X[0] ^ X[i]) & p;
+        X[0] ^= t;
+        X[i] ^= t;
+      }
+    }
+  }
+  X[1] ^= X[0];
+  X[2] ^= X[1];
+  int t = 0;
+#pragma unroll
+  for (int q = 1 << (BITS - 1); q > 1; q >>= 1)
+    if (X[2] & q) t ^= q - 1;
+  int h = 0;
+#pragma unroll
+  for (int b = 0; b < BITS; ++b)
+#pragma unroll
+    for (int i = 0; i < 3; ++i) h |= (((X[i] ^ t) >> b) & 1) << (b * 3 + (2 - i));
+  return h;
+}
+
 // Write slot g's cell-ordered record for atom j: its position shifted into the box by
 // whole box vectors (the shift is kept per atom so the integrator can apply it every step).
-// Returns the atom's sub-cell key: the Morton code of its position on a 4x4x4 grid inside
+// Returns the atom's sub-cell key: the Hilbert index of its position on a 4x4x4 grid inside
 // its cell (the order in which the neighbour search groups a cell's atoms).
 __device__ __forceinline__ int place_sorted(const LaunchCtxView &v, const DevSys &s, int g, int j,
                                             const int cc[3]) {
@@ -139,9 +177,9 @@ __device__ __forceinline__ int place_sorted(const LaunchCtxView &v, const DevSys
   v.wrap[j] = make_float4(wx, wy, wz, 0.f);
   v.sorted_orig[g] = j;
   v.sorted_type[g] = v.atom_type[j];
+  v.slot_info[g] = make_int2(v.atom_type[j], j);
   v.rank[j] = g;
-  auto spread = [](int b) { return (b & 1) | ((b & 2) << 2); };
-  return (spread(sub[0]) << 2) | (spread(sub[1]) << 1) | spread(sub[2]);
+  return hilbert_key(sub[0], sub[1], sub[2]);
 }
 
 // One block per allocated cell: rank-sort the cell's slice ascending, zero the cursor, write
@@ -181,6 +219,7 @@ __global__ void k_cells_sort(const int *__restrict__ cell_sys, const DevSys *__r
       int key = sub_keys[k], rank = 0;
       for (int m = 0; m < n; ++m) rank += sub_keys[m] < key;
       v.group_order[gbase + rank] = gbase + k;
+      v.order_pos[gbase + k] = gbase + rank;
     }
   } else {
     // Oversized cell (only in pathological inputs): serial insertion sort by one thread;
@@ -199,6 +238,7 @@ __global__ void k_cells_sort(const int *__restrict__ cell_sys, const DevSys *__r
     for (int k = threadIdx.x; k < n; k += blockDim.x) {
       place_sorted(v, s, gbase + k, slice[k], cc);
       v.group_order[gbase + k] = gbase + k;
+      v.order_pos[gbase + k] = gbase + k;
     }
   }
 }
@@ -504,6 +544,208 @@ __global__ void __launch_bounds__(SPLIT == 1 ? 32 * NBR_WARPS : 32 * SPLIT)
   if (lane == 0) atomicMax(&required[sidx], most);
 }
 
+// ---------------------------------------------------------------- group-pair rows
+// One WARP per search group of GROUP_ATOMS atoms (the groups of k_neighbours<4, 1>): the
+// group's row lists every partner atom that lies within the list cutoff of the group's
+// bounding box through some lattice image, once per such image, and only if the pair belongs
+// to this group: the partner comes later in search order (order_pos beyond the group), or it
+// is one of the group's own atoms, when the entry's mask keeps only the pairs seen from the
+// group's earlier atoms. Mask bits also mark the excluded pairs (cells.js:191-227) and the
+// atoms past the end of a short group. Every pair within the list cutoff of its two atoms is
+// therefore listed exactly once over all rows (the bounding box contains the atom), and an
+// atom is never paired with its own image.
+//
+// With at least three cells on every axis the stencil reaches each cell through one lattice
+// shift, as in k_neighbours; otherwise every visited cell is searched through each of the
+// lattice images -1, 0, +1 of the axes with fewer than three cells, so that every image of a
+// partner within the list cutoff is found.
+//
+// A block of GROUP_ROW_WARPS warps builds one group's row: the stencil's cells are dealt out to
+// the warps in turn, and each warp appends its survivors behind a shared-memory counter, so the
+// row is several short serial walks instead of one long one. The order of a row's entries then
+// depends on the warps' timing; its contents do not, and neither does any force (every pair's
+// fixed-point force is added whatever the order).
+constexpr int GROUP_ROW_WARPS = 4;
+__global__ void __launch_bounds__(32 * GROUP_ROW_WARPS)
+    k_group_rows(const float4 *__restrict__ posq, const int *__restrict__ group_sys,
+                 const DevSys *__restrict__ sys, const int *__restrict__ cell_start,
+                 const int *__restrict__ cell_gstart, const int *__restrict__ group_order,
+                 const int *__restrict__ excl_start, const int *__restrict__ excl_partners,
+                 const float4 *__restrict__ spos, const int2 *__restrict__ slot_info,
+                 const int *__restrict__ order_pos, int *__restrict__ gnbr, int *__restrict__ gnbr_count,
+                 int *__restrict__ gfirst, int *__restrict__ gsize, int *__restrict__ required,
+                 float4 *__restrict__ origin, int n_groups, const int *__restrict__ only) {
+  constexpr int G = GROUP_ATOMS;
+  __shared__ int row_count;
+  const int warp = blockIdx.x;  // the group slot (every exit before the barriers is the block's)
+  const int wib = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
+  if (warp >= n_groups) return;
+  const int sidx = group_sys[warp];
+  if (only && !only[sidx]) return;  // this system's lists are still valid
+  const DevSys &s = sys[sidx];
+  const int q = warp - s.group_base;
+  const int counts[3] = {s.cell_counts[0], s.cell_counts[1], s.cell_counts[2]};
+  const int cells = counts[0] * counts[1] * counts[2];
+  const int *gstart = cell_gstart + s.cell_start_base;
+  if (q >= gstart[cells]) {  // an unused slot (the cells hold fewer groups than allocated)
+    if (threadIdx.x == 0) {
+      gsize[warp] = 0;
+      gnbr_count[warp] = 0;
+    }
+    return;
+  }
+  if (threadIdx.x == 0) row_count = 0;
+  __syncthreads();
+  int lo = 0, hi = cells;
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (gstart[mid] <= q) lo = mid; else hi = mid;
+  }
+  const int cell0 = lo;
+  const int cbegin = s.atom_start + cell_start[s.cell_start_base + cell0];
+  const int cend = s.atom_start + cell_start[s.cell_start_base + cell0 + 1];
+  const int o0 = cbegin + (q - gstart[cell0]) * G;
+  const int size = min(G, cend - o0);
+  // every lane holds atom lane % G of the group
+  const int a = lane % G;
+  const bool valid = a < size;
+  const int si = valid ? group_order[o0 + a] : group_order[o0];
+  const int i = slot_info[si].y;
+  const float4 pw = spos[si];
+  if (valid && threadIdx.x < G) origin[i] = posq[i];  // skin check origin
+  const int e_lo = valid ? excl_start[i] : 0, e_hi = valid ? excl_start[i + 1] : 0;
+  const int p_min = e_lo < e_hi ? excl_partners[e_lo] : INT_MAX;
+  const int p_max = e_lo < e_hi ? excl_partners[e_hi - 1] : INT_MIN;
+  int atom_i[G], atom_lo[G], atom_hi[G];
+#pragma unroll
+  for (int b = 0; b < G; ++b) {
+    atom_i[b] = __shfl_sync(0xffffffffu, i, b);
+    atom_lo[b] = __shfl_sync(0xffffffffu, p_min, b);
+    atom_hi[b] = __shfl_sync(0xffffffffu, p_max, b);
+  }
+  const unsigned absent = 0xFu & ~((1u << size) - 1u);  // atoms past the end of a short group
+  // the group's bounding box (wrapped coordinates)
+  float blo[3], bhi[3];
+  {
+    const float c[3] = {pw.x, pw.y, pw.z};
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      float lo_d = valid ? c[d] : INFINITY, hi_d = valid ? c[d] : -INFINITY;
+#pragma unroll
+      for (int o = G / 2; o > 0; o >>= 1) {
+        lo_d = fminf(lo_d, __shfl_xor_sync(0xffffffffu, lo_d, o));
+        hi_d = fmaxf(hi_d, __shfl_xor_sync(0xffffffffu, hi_d, o));
+      }
+      blo[d] = lo_d;
+      bhi[d] = hi_d;
+    }
+  }
+  const int cc[3] = {cell0 / (counts[1] * counts[2]), (cell0 / counts[2]) % counts[1], cell0 % counts[2]};
+  int base[3], count[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    base[d] = counts[d] >= 3 ? -1 : 0;
+    count[d] = counts[d] >= 3 ? 3 : (counts[d] == 2 ? 2 : 1);
+  }
+  const bool stencil_shift = counts[0] >= 3 && counts[1] >= 3 && counts[2] >= 3;
+  const bool rectangular = s.box[3] == 0.f && s.box[6] == 0.f && s.box[7] == 0.f;
+  const float wcell[3] = {s.box[0] / counts[0], s.box[4] / counts[1], s.box[8] / counts[2]};
+  const float cull2 = s.list_cutoff2 * 1.00004f * 1.0001f;  // the margin k_neighbours culls with
+  const int cap = s.nbr_capacity;
+  int *row = gnbr + s.gnbr_base + (long long)q * cap;
+  const int stencil_cells = count[0] * count[1] * count[2];
+  for (int sc = wib; sc < stencil_cells; sc += GROUP_ROW_WARPS) {
+    const int ox = sc / (count[1] * count[2]), oy = (sc / count[2]) % count[1], oz = sc % count[2];
+    {
+      const int rx = cc[0] + base[0] + ox;
+      const int wx = rx < 0 ? -1 : (rx >= counts[0] ? 1 : 0);
+      const int cx = rx - wx * counts[0];
+      const int ry = cc[1] + base[1] + oy;
+      const int wy = ry < 0 ? -1 : (ry >= counts[1] ? 1 : 0);
+      const int cy = ry - wy * counts[1];
+      {
+        const int rz = cc[2] + base[2] + oz;
+        const int wz = rz < 0 ? -1 : (rz >= counts[2] ? 1 : 0);
+        const int cz = rz - wz * counts[2];
+        const int cell = (cx * counts[1] + cy) * counts[2] + cz;
+        const int begin = s.atom_start + cell_start[s.cell_start_base + cell];
+        const int end = s.atom_start + cell_start[s.cell_start_base + cell + 1];
+        // the lattice images to search this cell through: the stencil's own wrap on an axis
+        // with three cells or more, each of -1, 0, +1 on the others
+        const int na = counts[0] >= 3 ? 1 : 3, nb = counts[1] >= 3 ? 1 : 3, nc = counts[2] >= 3 ? 1 : 3;
+        for (int image = 0; image < na * nb * nc; ++image) {
+          const int ka = counts[0] >= 3 ? wx : image / (nb * nc) - 1;
+          const int kb = counts[1] >= 3 ? wy : (image / nc) % nb - 1;
+          const int kc = counts[2] >= 3 ? wz : image % nc - 1;
+          const int code = shift_code(ka, kb, kc);
+          const float4 S = s.shift[code];
+          if (stencil_shift && rectangular) {  // skip a cell whose box is beyond the list cutoff
+            const float r[3] = {(float)rx, (float)ry, (float)rz};
+            float d2 = 0.f;
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+              const float clo = r[d] * wcell[d], chi = clo + wcell[d];
+              const float e = fmaxf(fmaxf(clo - bhi[d], blo[d] - chi), 0.f);
+              d2 = fmaf(e, e, d2);
+            }
+            if (d2 > cull2) continue;
+          }
+          const float slo[3] = {blo[0] - S.x, blo[1] - S.y, blo[2] - S.z};
+          const float shi[3] = {bhi[0] - S.x, bhi[1] - S.y, bhi[2] - S.z};
+          for (int b = begin; b < end; b += 32) {
+            const int g = b + lane;
+            bool keep = g < end;
+            unsigned mask = 0;
+            if (keep) {
+              const float4 pj = spos[g];
+              const float c[3] = {pj.x, pj.y, pj.z};
+              float d2 = 0.f;
+#pragma unroll
+              for (int d = 0; d < 3; ++d) {
+                const float e = fmaxf(fmaxf(slo[d] - c[d], c[d] - shi[d]), 0.f);
+                d2 = fmaf(e, e, d2);
+              }
+              keep = d2 <= cull2;
+            }
+            if (keep) {
+              const int opos = order_pos[g];
+              if (opos < o0) {
+                keep = false;  // an earlier group of this cell lists the pair
+              } else {
+                if (opos < o0 + G) mask = 0xFu & ~((1u << (opos - o0)) - 1u);  // own atom: earlier atoms only
+                const int j = slot_info[g].y;
+#pragma unroll
+                for (int t = 0; t < G; ++t)
+                  if (j >= atom_lo[t] && j <= atom_hi[t] && is_excluded(excl_start, excl_partners, atom_i[t], j))
+                    mask |= 1u << t;
+                mask |= absent;
+                keep = mask != 0xFu;
+              }
+            }
+            const unsigned hits = __ballot_sync(0xffffffffu, keep);
+            if (hits) {
+              int at = 0;
+              if (lane == 0) at = atomicAdd(&row_count, __popc(hits));
+              at = __shfl_sync(0xffffffffu, at, 0) + __popc(hits & ((1u << lane) - 1u));
+              if (keep && at < cap)
+                row[at] = (int)((unsigned)g | ((unsigned)code << GROUP_CODE_SHIFT) | (mask << GROUP_MASK_SHIFT));
+            }
+          }
+        }
+      }
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const int found = row_count;
+    gnbr_count[warp] = min(found, cap);
+    gfirst[warp] = o0;
+    gsize[warp] = size;
+    atomicMax(&required[sidx], found);
+  }
+}
+
 // ---------------------------------------------------------------- rebuild on demand
 // A list built with cutoff rc + skin holds every pair that is within rc while no atom has
 // moved more than skin / 2 from where it was at the build (two atoms close by at most the sum
@@ -530,17 +772,19 @@ __global__ void k_rebuild_decide(cudaGraphConditionalHandle handle, const unsign
   }
 }
 
-// Start of every rebuild: fold the previous build's requirement into the running maximum the
-// host reads after each block (so an overflow at a rebuild inside a block is seen too), then
-// clear the requirement and the displacement since the build, and count the build.
+// Start of every rebuild: fold the previous build's requirement (entries of the longest per-atom
+// row in required[s], of the longest group-pair row in required[S + s]) into the running
+// maximum the host reads after each block (so an overflow at a rebuild inside a block is seen
+// too), then clear the requirement and the displacement since the build, and count the build.
 __global__ void k_rebuild_reset(int *__restrict__ required, int *__restrict__ required_max,
                                 unsigned *__restrict__ disp, int S, unsigned long long *__restrict__ builds,
                                 const int *__restrict__ only) {
   if (blockIdx.x == 0 && threadIdx.x == 0) *builds += 1;
   for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < S; s += gridDim.x * blockDim.x) {
     if (only && !only[s]) continue;
-    required_max[s] = max(required_max[s], required[s]);
+    required_max[s] = max(required_max[s], max(required[s], required[S + s]));
     required[s] = 0;
+    required[S + s] = 0;
     disp[s] = 0u;
   }
 }
@@ -559,6 +803,8 @@ int neighbour_group_slots(int atoms, int cells, int group_atoms) {
   return (atoms + group_atoms - 1) / group_atoms + cells;
 }
 
+int rebuild_launches(const LaunchCtx &ctx) { return ctx.pair_list == 2 ? 6 : 5; }
+
 void launch_rebuild(const LaunchCtx &ctx, cudaStream_t stream) {
   const int n = ctx.n_atoms;
   const int tb = 128;
@@ -572,10 +818,17 @@ void launch_rebuild(const LaunchCtx &ctx, cudaStream_t stream) {
                                                          ctx.cell_start, ctx.cell_count,
                                                          ctx.cell_atoms, n, only);
   LaunchCtxView v{ctx.posq, ctx.atom_type, ctx.spos, ctx.wrap, ctx.sorted_orig, ctx.sorted_type, ctx.rank,
-                  ctx.group_order};
+                  ctx.group_order, ctx.slot_info, ctx.order_pos};
   k_cells_sort<<<ctx.n_cells_total, 128, 0, stream>>>(ctx.cell_sys, ctx.sys, ctx.cell_start,
                                                       ctx.cell_count, ctx.cell_atoms, v, only);
   const int blocks = (ctx.n_groups_total + NBR_WARPS - 1) / NBR_WARPS;
+  if (ctx.pair_list != 1) {  // group-pair rows (the cell scan counted 4-atom groups)
+    k_group_rows<<<ctx.n_groups_total, 32 * GROUP_ROW_WARPS, 0, stream>>>(
+        ctx.posq, ctx.group_sys, ctx.sys, ctx.cell_start, ctx.cell_gstart, ctx.group_order, ctx.excl_start,
+        ctx.excl_partners, ctx.spos, ctx.slot_info, ctx.order_pos, ctx.gnbr, ctx.gnbr_count, ctx.gfirst, ctx.gsize,
+        ctx.required + ctx.n_systems, ctx.origin, ctx.n_groups_total, only);
+    if (ctx.pair_list != 2) return;
+  }
 #define RMD_NBR_ARGS                                                                                      \
   ctx.posq, ctx.group_sys, ctx.sys, ctx.cell_start, ctx.cell_gstart, ctx.group_order, ctx.excl_start,  \
       ctx.excl_partners, ctx.spos, ctx.sorted_orig, ctx.nbr, ctx.nbr_count, ctx.required, ctx.origin, \

@@ -109,7 +109,7 @@ __global__ void k_min_decide(MinState *__restrict__ st, const double *__restrict
   if (s >= S) return;
   MinState m = st[s];
   if (!m.trial) return;
-  const int req = required[s];
+  const int req = max(required[s], required[S + s]);  // per-atom rows, group-pair rows
   if (req > sys[s].nbr_capacity) {
     m.overflow = 1;
     m.need = max(m.need, req);

@@ -63,7 +63,6 @@ __global__ void __launch_bounds__(128) k_nonbonded(
   const int i = sorted_orig[si];
   const DevSys &s = sys[sys_of_atom[i]];
   const float4 pw = spos[si];
-  const float qik = (float)ONE_4PI_EPS0 * pw.w;
   const int ti = sorted_type[si];
   const float2 *ljrow = (lj_in_smem ? lj_shared : lj) + s.lj_base + ti * s.type_count;
   const float alpha = s.alpha;
@@ -109,7 +108,7 @@ __global__ void __launch_bounds__(128) k_nonbonded(
       const float2 ab = ljrow[tj];
       const float a12 = ab.x * inv_r6 * inv_r6, b6 = ab.y * inv_r6;
       float scalar = (12.0f * a12 - 6.0f * b6) * inv_r2;
-      const float qq = qik * pj.w;
+      const float qq = (float)ONE_4PI_EPS0 * (pw.w * pj.w);  // symmetric in i and j
       const float r = r2 * inv_r;
       float gauss;
       const float screened = erfc_and_gauss(alpha * r, gauss);
@@ -220,6 +219,218 @@ __global__ void __launch_bounds__(128) k_nonbonded(
   }
 }
 
+// ------------------------------------------------------------------ group-pair kernel
+// The same pair physics over the group-pair rows (lists.cu k_group_rows): one WARP per group of
+// GROUP_ATOMS atoms, lane = 8 * a + t for the group's atom a and partner slot t, so that a pass
+// over 8 row entries evaluates 32 pairs and each entry's partner record is loaded once for the
+// group's atoms. Each pair is evaluated once, from the group that lists it: its force is
+// quantised to 64-bit fixed point (as the atom-row kernel's precision form does), added to the
+// group atom's registers, and its negation summed over the group's four atoms with integer
+// shuffles and added to the partner's force with one 64-bit atomic per component. Because the
+// pair force is computed from the same f32 operands in the same order as the atom-row kernel
+// computes it from either atom (the charge product is symmetric, the image shifts of opposite
+// codes are exact negatives, and rounding to nearest is odd), every atom's force is the same
+// sum of the same integers as there, bit for bit. Energies (ENERGY) are accumulated the same
+// way into per-atom integer sums that hold each pair's full energy for both of its atoms, then
+// halved, which is the atom-row kernel's per-atom value exactly. The force array (and, for
+// ENERGY, the energy sums) must be zero when the kernel starts; the exceptions of each group
+// atom are evaluated by its eight lanes, as in the atom-row kernel.
+
+// Sum four 64-bit values (v0..v3) over the 4 lanes that differ in lane bits (b_hi, b_lo); on
+// return lane (bit_hi, bit_lo) holds the sum of value 2 * bit_hi + bit_lo. Three shuffles of
+// 64-bit words instead of eight.
+template <int B_HI, int B_LO>
+__device__ __forceinline__ long long reduce_four(long long v0, long long v1, long long v2, long long v3, int lane) {
+  const bool hi = (lane >> B_HI) & 1;
+  const long long send0 = hi ? v0 : v2, send1 = hi ? v1 : v3;
+  const long long keep0 = hi ? v2 : v0, keep1 = hi ? v3 : v1;
+  const long long a = keep0 + __shfl_xor_sync(0xffffffffu, send0, 1 << B_HI);
+  const long long b = keep1 + __shfl_xor_sync(0xffffffffu, send1, 1 << B_HI);
+  const bool low = (lane >> B_LO) & 1;
+  return (low ? b : a) + __shfl_xor_sync(0xffffffffu, low ? a : b, 1 << B_LO);
+}
+
+template <bool ENERGY>
+__global__ void __launch_bounds__(128) k_group_pairs(
+    const float4 *__restrict__ posq, const float4 *__restrict__ spos, const int2 *__restrict__ slot_info,
+    const int *__restrict__ group_order, const int *__restrict__ group_sys, const DevSys *__restrict__ sys,
+    const float2 *__restrict__ lj, const int *__restrict__ gnbr, const int *__restrict__ gnbr_count,
+    const int *__restrict__ gfirst, const int *__restrict__ gsize, const int *__restrict__ exc_start,
+    const int *__restrict__ exc_partner, const float4 *__restrict__ exc_param,
+    unsigned long long *__restrict__ force, unsigned long long *__restrict__ e_acc, int n_atoms, int n_groups,
+    int lj_entries, int split) {
+  extern __shared__ float2 lj_shared[];
+  const bool lj_in_smem = lj_entries > 0;
+  for (int k = threadIdx.x; k < lj_entries; k += blockDim.x) lj_shared[k] = lj[k];
+  if (lj_in_smem) __syncthreads();
+  // `split` warps share a group's row, warp r taking passes r, r + split, ...: a long row is
+  // several short serial chains rather than one (each warp's passes are latency-bound)
+  const int task = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int warp = task / split, part = task - warp * split;  // the group slot, this warp's share
+  const int lane = threadIdx.x & 31, a = lane >> 3, t = lane & 7;
+  if (warp >= n_groups) return;
+  const int size = gsize[warp];
+  if (size == 0) return;  // an unused slot (the whole warp leaves)
+  const DevSys &s = sys[group_sys[warp]];
+  const bool vi = a < size;
+  const int si = group_order[gfirst[warp] + (vi ? a : 0)];
+  const int2 info_i = slot_info[si];
+  const float4 pw = spos[si];
+  const float2 *ljrow = (lj_in_smem ? lj_shared : lj) + s.lj_base + info_i.x * s.type_count;
+  const float alpha = s.alpha;
+  const float gauss_k = 2.0f * alpha * 0.5641895835477563f;  // 2a/sqrt(pi)
+  const float cut2 = s.cutoff2;
+  const int count = gnbr_count[warp];
+  const int *row = gnbr + s.gnbr_base + (long long)(warp - s.group_base) * s.nbr_capacity;
+  long long qx = 0, qy = 0, qz = 0, qlj = 0, qcoul = 0, qvir = 0;
+  // software pipeline: the next pass's entry and partner record are loaded while this pass's
+  // pairs are computed
+  const int stride = 8 * split;
+  int k0 = 8 * part;
+  unsigned e1 = k0 + t < count ? (unsigned)__ldg(row + k0 + t) : (0xFu << GROUP_MASK_SHIFT);
+  float4 pj1 = __ldg(spos + (e1 & GROUP_SLOT_MASK));
+  int2 info1 = __ldg(slot_info + (e1 & GROUP_SLOT_MASK));
+  for (; k0 < count; k0 += stride) {
+    const unsigned e = e1;
+    const float4 pj = pj1;
+    const int2 info_j = info1;
+    if (k0 + stride < count) {
+      e1 = k0 + stride + t < count ? (unsigned)__ldg(row + k0 + stride + t) : (0xFu << GROUP_MASK_SHIFT);
+      pj1 = __ldg(spos + (e1 & GROUP_SLOT_MASK));
+      info1 = __ldg(slot_info + (e1 & GROUP_SLOT_MASK));
+    }
+    const float4 S = s.shift[(e >> GROUP_CODE_SHIFT) & 31u];
+    const float3 d = make_float3(pw.x - pj.x - S.x, pw.y - pj.y - S.y, pw.z - pj.z - S.z);
+    const float r2 = fmaf(d.x, d.x, fmaf(d.y, d.y, d.z * d.z));
+    long long fx = 0, fy = 0, fz = 0, el = 0, ec = 0, ev = 0;
+    if (vi && !((e >> (GROUP_MASK_SHIFT + a)) & 1u) && r2 <= cut2) {
+      const float inv_r = rsqrt_refined(r2);
+      const float inv_r2 = inv_r * inv_r;
+      const float inv_r6 = inv_r2 * inv_r2 * inv_r2;
+      const float2 ab = ljrow[info_j.x];
+      const float a12 = ab.x * inv_r6 * inv_r6, b6 = ab.y * inv_r6;
+      float scalar = (12.0f * a12 - 6.0f * b6) * inv_r2;
+      const float qq = (float)ONE_4PI_EPS0 * (pw.w * pj.w);
+      const float r = r2 * inv_r;
+      float gauss;
+      const float screened = erfc_and_gauss(alpha * r, gauss);
+      scalar = fmaf(qq * fmaf(screened, inv_r, gauss_k * gauss), inv_r2, scalar);
+      fx = (long long)to_fixed(scalar * d.x);
+      fy = (long long)to_fixed(scalar * d.y);
+      fz = (long long)to_fixed(scalar * d.z);
+      qx += fx;
+      qy += fy;
+      qz += fz;
+      if (ENERGY) {
+        el = (long long)to_fixed(a12 - b6);
+        ec = (long long)to_fixed(qq * screened * inv_r);
+        ev = (long long)to_fixed(scalar * r2);
+        qlj += el;
+        qcoul += ec;
+        qvir += ev;
+      }
+    }
+    // the partner's share, summed over the group's four atoms (lane bits 4 and 3): lane a then
+    // holds component a of it
+    const long long fj = reduce_four<4, 3>(-fx, -fy, -fz, 0, lane);
+    if (a < 3 && fj != 0) atomicAdd(force + a * (long long)n_atoms + info_j.y, (unsigned long long)fj);
+    if (ENERGY) {
+      const long long ej = reduce_four<4, 3>(el, ec, ev, 0, lane);
+      if (a < 3 && ej != 0) atomicAdd(e_acc + a * (long long)n_atoms + info_j.y, (unsigned long long)ej);
+    }
+  }
+  // Exceptions of the group atom: 1-4 scaled LJ/Coulomb and -q_i q_j erf(a r)/r, no cutoff,
+  // exactly as the atom-row kernel evaluates them.
+  const int i = info_i.y;
+  const int eb = exc_start[i], ee = vi && part == 0 ? exc_start[i + 1] : eb;
+  const float4 pi = posq[i];
+  for (int e = eb + t; e < ee; e += 8) {
+    float pair_lj = 0.f, pair_coul = 0.f;
+    const int j = exc_partner[e];
+    const float4 prm = exc_param[e];  // chargeProduct, ljA, ljB, fullProduct
+    const float4 pj = posq[j];
+    float3 d = min_image(make_float3(pi.x - pj.x, pi.y - pj.y, pi.z - pj.z), s);
+    const float r2 = fmaf(d.x, d.x, fmaf(d.y, d.y, d.z * d.z));
+    const float inv_r = rsqrt_refined(r2);
+    const float inv_r2 = inv_r * inv_r, inv_r6 = inv_r2 * inv_r2 * inv_r2;
+    float scalar = 0.f;
+    if (prm.y != 0.f || prm.z != 0.f) {
+      const float a12 = prm.y * inv_r6 * inv_r6, b6 = prm.z * inv_r6;
+      scalar += (12.0f * a12 - 6.0f * b6) * inv_r2;
+      if (ENERGY) pair_lj += a12 - b6;
+    }
+    if (prm.x != 0.f) {
+      const float qq = (float)ONE_4PI_EPS0 * prm.x;
+      scalar += qq * inv_r * inv_r2;
+      if (ENERGY) pair_coul += qq * inv_r;
+    }
+    if (alpha > 0.f && prm.w != 0.f) {
+      const float qq = (float)ONE_4PI_EPS0 * prm.w;
+      float gauss;
+      const float r = r2 * inv_r;
+      const float unscreened = 1.0f - erfc_and_gauss(alpha * r, gauss);
+      scalar -= qq * (unscreened * inv_r - gauss_k * gauss) * inv_r2;
+      if (ENERGY) pair_coul -= qq * unscreened * inv_r;
+    }
+    if (ENERGY) {
+      qlj += (long long)to_fixed(pair_lj);
+      qcoul += (long long)to_fixed(pair_coul);
+      qvir += (long long)to_fixed(scalar * r2);
+    }
+    qx += (long long)to_fixed(scalar * d.x);
+    qy += (long long)to_fixed(scalar * d.y);
+    qz += (long long)to_fixed(scalar * d.z);
+  }
+  // the group atom's sums over its eight lanes (lane bits 2, 1 and 0): lanes 2c and 2c + 1
+  // then hold component c
+  long long fi = reduce_four<2, 1>(qx, qy, qz, 0, lane);
+  fi += __shfl_xor_sync(0xffffffffu, fi, 1);
+  const int comp = (lane >> 1) & 3;
+  if (vi && (lane & 1) == 0 && comp < 3 && fi != 0)
+    atomicAdd(force + comp * (long long)n_atoms + i, (unsigned long long)fi);
+  if (ENERGY) {
+    long long ei = reduce_four<2, 1>(qlj, qcoul, qvir, 0, lane);
+    ei += __shfl_xor_sync(0xffffffffu, ei, 1);
+    if (vi && (lane & 1) == 0 && comp < 3 && ei != 0)
+      atomicAdd(e_acc + comp * (long long)n_atoms + i, (unsigned long long)ei);
+  }
+}
+
+// Per-atom pair energies from the integer sums: half of each (every pair's energy was added to
+// both of its atoms), as the atom-row kernel stores them.
+__global__ void k_group_pair_energies(const unsigned long long *__restrict__ e_acc, double *__restrict__ e_lj,
+                                      double *__restrict__ e_coul, double *__restrict__ e_vir, int n_atoms) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_atoms) return;
+  e_lj[i] = 0.5 * ((double)(long long)e_acc[i] / FORCE_SCALE);
+  e_coul[i] = 0.5 * ((double)(long long)e_acc[n_atoms + i] / FORCE_SCALE);
+  e_vir[i] = 0.5 * ((double)(long long)e_acc[2 * (long long)n_atoms + i] / FORCE_SCALE);
+}
+
+static void launch_group_pairs(const LaunchCtx &c, bool energy, int lanes, cudaStream_t stream) {
+  const int split = lanes >= 64 ? 8 : lanes >= 32 ? 4 : lanes >= 16 ? 2 : 1;  // 8 lanes per group atom per warp
+  // (errors of these calls surface in the caller's cudaGetLastError, as the launches' do)
+  (void)cudaMemsetAsync(c.force, 0, sizeof(unsigned long long) * 3 * (size_t)c.n_atoms, stream);
+  if (energy) (void)cudaMemsetAsync(c.e_acc, 0, sizeof(unsigned long long) * 3 * (size_t)c.n_atoms, stream);
+  const int threads = 128;
+  const int blocks = (int)(((long long)c.n_groups_total * split * 32 + threads - 1) / threads);
+  constexpr int LJ_SMEM_MAX = 4096;
+  const int lj_entries = c.lj_entries <= LJ_SMEM_MAX ? c.lj_entries : 0;
+  const size_t smem = sizeof(float2) * lj_entries;
+  if (energy) {
+    k_group_pairs<true><<<blocks, threads, smem, stream>>>(
+        c.posq, c.spos, c.slot_info, c.group_order, c.group_sys, c.sys, c.lj, c.gnbr, c.gnbr_count, c.gfirst,
+        c.gsize, c.exc_start, c.exc_partner, c.exc_param, c.force, c.e_acc, c.n_atoms, c.n_groups_total, lj_entries,
+        split);
+    k_group_pair_energies<<<(c.n_atoms + 255) / 256, 256, 0, stream>>>(c.e_acc, c.e_lj, c.e_coul, c.e_vir, c.n_atoms);
+  } else {
+    k_group_pairs<false><<<blocks, threads, smem, stream>>>(
+        c.posq, c.spos, c.slot_info, c.group_order, c.group_sys, c.sys, c.lj, c.gnbr, c.gnbr_count, c.gfirst,
+        c.gsize, c.exc_start, c.exc_partner, c.exc_param, c.force, c.e_acc, c.n_atoms, c.n_groups_total, lj_entries,
+        split);
+  }
+}
+
 template <bool ENERGY, int LANES, bool PAIR_FIXED>
 static void launch_nb(const LaunchCtx &c, cudaStream_t stream) {
   const int threads = 128;
@@ -246,9 +457,12 @@ static void launch_nb_lanes(const LaunchCtx &c, bool energy, int lanes, cudaStre
 }
 
 void launch_nonbonded(const LaunchCtx &c, bool energy, int lanes, cudaStream_t stream) {
-  if (c.pair_fixed) launch_nb_lanes<true>(c, energy, lanes, stream);
+  if (c.pair_list != 1) launch_group_pairs(c, energy, lanes, stream);
+  else if (c.pair_fixed) launch_nb_lanes<true>(c, energy, lanes, stream);
   else launch_nb_lanes<false>(c, energy, lanes, stream);
 }
+
+int nonbonded_launches(const LaunchCtx &c, bool energy) { return c.pair_list != 1 && energy ? 2 : 1; }
 
 // ------------------------------------------------------------------ bonded + restraints
 // One thread per term (bonds | angles | torsions | restraints); forces are added to the

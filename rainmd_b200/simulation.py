@@ -57,7 +57,7 @@ _OPTION_NAMES = {
     "forceAccumulation": "force_accumulation", "neighbourGroupAtoms": "neighbour_group_atoms",
     "nonbondedLanes": "nonbonded_lanes", "spreadAtomsPerBlock": "spread_atoms_per_block",
     "learnedWarmupMoves": "learned_warmup_moves", "learnedStepsPerMove": "learned_steps_per_move",
-    "learnedRate": "learned_rate", "rebuildOnDemand": "rebuild_on_demand",
+    "learnedRate": "learned_rate", "rebuildOnDemand": "rebuild_on_demand", "pairList": "pair_list",
 }
 
 
@@ -333,6 +333,22 @@ class BatchSimulation:
                                                    C.byref(req)))
         return cap.value, counts, rows.reshape(n, cap.value), req.value
 
+    def debugGroupRows(self, index=0) -> dict:
+        """The group-pair rows: atoms [groups, 4] (-1 = none), counts [groups], and per entry
+        [groups, capacity] partner, image code and skip mask, in the system's atom indices."""
+        groups, cap = C.c_int32(0), C.c_int32(0)
+        self._check(self._lib.rmd_debug_group_rows(self._h, index, C.byref(groups), C.byref(cap), None, None,
+                                                   None, None, None))
+        g, c = groups.value, cap.value
+        atoms = np.zeros((g, 4), np.int32)
+        counts = np.zeros(g, np.int32)
+        partners, codes, masks = (np.zeros((g, c), np.int32) for _ in range(3))
+        p = lambda a: a.ctypes.data_as(C.POINTER(C.c_int32))  # noqa: E731
+        self._check(self._lib.rmd_debug_group_rows(self._h, index, C.byref(groups), C.byref(cap), p(atoms),
+                                                   p(counts), p(partners), p(codes), p(masks)))
+        return {"atoms": atoms, "counts": counts, "partners": partners, "codes": codes, "masks": masks,
+                "capacity": c}
+
     def debugEvaluate(self, index=0):
         out = L.RmdEnergyReport()
         forces = np.zeros(3 * self.atom_counts[index])
@@ -398,10 +414,11 @@ class BatchSimulation:
         def table(row, keys):
             return {k: float(v) for k, v in zip(keys, row) if v >= 0}
 
+        lanes = (8, 16, 32) if self.diagnostics()["pair_list"] == 1 else (16, 32, 64)
         return {"neighbourGroupAtoms": int(shapes[0]), "nonbondedLanes": int(shapes[1]),
                 "spreadAtomsPerBlock": int(shapes[2]),
                 "tuned": {"neighbourGroupAtoms": table(ms[0:3], (4, 8, 16)),
-                          "nonbondedLanes": table(ms[3:6], (8, 16, 32)),
+                          "nonbondedLanes": table(ms[3:6], lanes),
                           "spreadAtomsPerBlock": table(ms[6:9], (4, 8, 16))}}
 
     def surrogateReport(self, index=0) -> dict:

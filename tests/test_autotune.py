@@ -18,7 +18,9 @@ def water(n=2854, seed=3):
 
 
 def make(system, pos, **shapes):
-    opts = {"pmeOrder": 4, "grid": [32, 32, 32], "skin": 0.1, "temperature": 300.0, "seed": 5}
+    """Per-atom rows (pair_list 1), the form whose search-group size and pair-loop lanes are
+    tuned; the group-pair rows have one shape of each."""
+    opts = {"pmeOrder": 4, "grid": [32, 32, 32], "skin": 0.1, "temperature": 300.0, "seed": 5, "pairList": 1}
     opts.update(shapes)
     sim = GpuSimulation(system, opts)
     sim.setState(pos)
@@ -67,3 +69,44 @@ def test_every_shape_gives_bitwise_identical_results():
         assert all(np.array_equal(a, b) for a, b in zip(got[2], reference[2]))
         assert np.array_equal(got[3], reference[3])
         sim.release()
+
+
+def test_group_pair_rows_tune_the_row_split_and_the_spreading():
+    """Group-pair rows: 4-atom search groups always; the warps sharing a row (2, 4 or 8: 16, 32
+    or 64 lanes per group atom) and the spreading block are timed and the fastest kept."""
+    system, pos = water()
+    sim = make(system, pos, pairList=0)
+    shapes = sim.kernelShapes()
+    assert shapes["neighbourGroupAtoms"] == 4 and shapes["tuned"]["neighbourGroupAtoms"] == {}
+    for name, candidates in (("nonbondedLanes", [16, 32, 64]), ("spreadAtomsPerBlock", [4, 8, 16])):
+        tuned = shapes["tuned"][name]
+        assert sorted(tuned) == candidates, name
+        assert shapes[name] == min(tuned, key=tuned.get), name
+    sim.release()
+
+
+def test_group_pair_rows_give_the_per_atom_rows_results_bit_for_bit():
+    """Each pair's force is quantised from the same f32 operands whichever structure lists it,
+    so both structures sum the same integers: forces, energies, a minimisation and a run agree
+    bit for bit, and so does a group-pair run whose builds also write the per-atom rows."""
+    system, pos = water()
+    results = []
+    for form, lanes in ((1, 16), (0, 16), (2, 64), (0, 8)):
+        sim = make(system, pos, pairList=form, spreadAtomsPerBlock=8, nonbondedLanes=lanes)
+        energy, forces = sim.debugEvaluate()
+        sim.minimise(maxIterations=20)
+        sim.run(40, blockSize=10)
+        e = sim.energy()
+        state = sim.readState()
+        results.append((energy, forces, e, state))
+        sim.release()
+    (e1, f1, end1, s1) = results[0]
+    for (e2, f2, end2, s2) in results[1:]:
+        assert np.array_equal(f1, f2)
+        for key in ("lennard_jones", "coulomb_direct", "coulomb_reciprocal", "potential"):
+            assert e1[key] == e2[key], key
+        for key in ("lennardJones", "coulombDirect", "coulombReciprocal", "potential", "kinetic"):
+            assert end1[key] == end2[key], key
+        assert np.array_equal(s1["positions"], s2["positions"])
+        assert np.array_equal(s1["velocities"], s2["velocities"])
+        assert np.array_equal(s1["forces"], s2["forces"])

@@ -106,6 +106,60 @@ def assert_lists_match_oracle(sim, system, index=0, skin=0.15):
     return int(nc.sum())
 
 
+def assert_group_rows_cover(sim, system, index=0, skin=0.15):
+    """The group-pair rows the device holds, expanded to atom pairs, against the oracle's rows
+    from the positions they were built from: every non-excluded pair within the list cutoff is
+    listed, through an image within the list cutoff, exactly once unless the box has fewer than
+    three cells on an axis (then once per image within the list cutoff of the group); no
+    excluded pair and no atom with itself is listed. Returns the number of listed pairs."""
+    n = system["topology"]["atomCount"]
+    box = np.asarray(system["boxVectors"], dtype=np.float64)
+    cutoff = system["options"]["cutoff"]
+    plan = oracle.plan_cell_list(n, box, cutoff, skin=skin)
+    origin = sim.debugRead("list_origin", 3 * n, index).astype(np.float32)
+    P = oracle.pack_params(box, cutoff, float(np.float32(cutoff + skin)), 1.0)
+    _, cs, ca = oracle.cell_list_f32(origin, P, plan["counts"])
+    es, ep = exclusion_gather(system)
+    nb, nc, _ = oracle.neighbour_list_f32(origin, P, plan["counts"], cs, ca, es, ep, 4096)
+    rows = np.repeat(np.arange(n), nc)
+    cols = nb[np.arange(4096)[None, :] < nc[:, None]]
+    expect = np.unique(np.minimum(rows, cols).astype(np.int64) * n + np.maximum(rows, cols))
+    g = sim.debugGroupRows(index)
+    cap = g["capacity"]
+    used = np.arange(cap)[None, :] < g["counts"][:, None]
+    q_idx, k_idx = np.nonzero(used)
+    partner, code, mask = g["partners"][q_idx, k_idx], g["codes"][q_idx, k_idx], g["masks"][q_idx, k_idx]
+    pairs_i, pairs_j, pairs_code = [], [], []
+    for a in range(4):
+        atom = g["atoms"][q_idx, a]
+        keep = (atom >= 0) & (((mask >> a) & 1) == 0)
+        pairs_i.append(atom[keep])
+        pairs_j.append(partner[keep])
+        pairs_code.append(code[keep])
+    pi, pj, pc = np.concatenate(pairs_i), np.concatenate(pairs_j), np.concatenate(pairs_code)
+    assert not np.any(pi == pj)
+    key = np.minimum(pi, pj).astype(np.int64) * n + np.maximum(pi, pj)
+    excluded = np.unique(np.minimum(np.repeat(np.arange(n), np.diff(es)), ep).astype(np.int64) * n +
+                         np.maximum(np.repeat(np.arange(n), np.diff(es)), ep))
+    assert not np.any(np.isin(key, excluded))
+    listed = np.unique(key)
+    assert np.all(np.isin(expect, listed))
+    stencil = all(c >= 3 for c in plan["counts"])
+    if stencil:
+        assert len(listed) == len(key)  # each pair once
+    # the listed image of every pair within the list cutoff is one within it
+    ka, kb, kc = pc // 9 - 1, (pc // 3) % 3 - 1, pc % 3 - 1
+    shift = (ka[:, None] * box[0:3] + kb[:, None] * box[3:6] + kc[:, None] * box[6:9])
+    x = origin.astype(np.float64).reshape(-1, 3)
+    d2 = np.sum((x[pi] - x[pj] - shift) ** 2, axis=1)
+    within = np.isin(key, expect)
+    lc = cutoff + skin
+    best = np.full(len(listed), np.inf)
+    np.minimum.at(best, np.searchsorted(listed, key[within]), d2[within])
+    assert np.all(best[np.isin(listed, expect)] <= lc * lc * 1.0002)
+    return int(len(key))
+
+
 @pytest.fixture(scope="module")
 def bench_box():
     system, pos, grid = water(23558)
@@ -118,13 +172,15 @@ def bench_box():
     return system, relaxed, grid
 
 
-@pytest.mark.parametrize("group", [None, 4, 16])
-def test_benchmark_lists_bit_exact_after_on_demand_rebuilds(bench_box, group):
+@pytest.mark.parametrize("form,group", [(2, None), (1, None), (1, 4), (1, 16)])
+def test_benchmark_lists_bit_exact_after_on_demand_rebuilds(bench_box, form, group):
     """23,558 atoms, 5^3 cells (the shifted stencil and bounding-box culls), ~6,000 4-atom groups
     (the one-warp search, not the split one) or the autotuned shape; the lists compared are the
-    ones the IF node of the step graph last rebuilt, mid-run."""
+    ones the IF node of the step graph last rebuilt, mid-run. With pair_list 2 the same builds
+    wrote the group-pair rows the pair kernel walks: they cover every pair of the per-atom
+    rows once."""
     system, pos, grid = bench_box
-    options = bench_options(grid)
+    options = bench_options(grid, pairList=form)
     if group is not None:
         options["neighbourGroupAtoms"] = group
     sim = GpuSimulation(system, options)
@@ -139,6 +195,20 @@ def test_benchmark_lists_bit_exact_after_on_demand_rebuilds(bench_box, group):
         assert sim.kernelShapes()["neighbourGroupAtoms"] == group
     pairs = assert_lists_match_oracle(sim, system)
     assert pairs > 23558 * 400
+    if form == 2:
+        assert assert_group_rows_cover(sim, system) >= pairs // 2
+    sim.release()
+
+
+@pytest.mark.parametrize("cutoff", [1.25, 1.0, 0.7, 0.5])
+def test_group_rows_cover_every_pair(cutoff):
+    """The 1,190-atom fixture at four cutoffs: 2 x 2 x 1 cells (every image of a partner searched)
+    to 5^3 (the stencil), the chain's exclusions masked."""
+    s, pos, _ = system_for("ala-wat", cutoff=cutoff)
+    sim = GpuSimulation(s, {"skin": 0.1, "dispersionCorrection": False, "pairList": 0})
+    sim.setState(pos)
+    sim.initialise()
+    assert assert_group_rows_cover(sim, s, skin=0.1) > 0
     sim.release()
 
 
@@ -148,7 +218,7 @@ def test_batch_lists_bit_exact_per_system(bench_box):
     rebuilds equal the oracle's for that system alone."""
     items = [chain1190(), water(2854), bench_box]
     systems = [s for s, _, _ in items]
-    batch = BatchSimulation(systems, [bench_options(g, seed=5 + k) for k, (_, _, g) in enumerate(items)])
+    batch = BatchSimulation(systems, [bench_options(g, seed=5 + k, pairList=2) for k, (_, _, g) in enumerate(items)])
     for k, (_, p, _) in enumerate(items):
         batch.setState(k, p)
     batch.initialise()
@@ -156,6 +226,7 @@ def test_batch_lists_bit_exact_per_system(bench_box):
     batch.run(120, blockSize=40)
     for k, system in enumerate(systems):
         assert_lists_match_oracle(batch, system, index=k)
+        assert_group_rows_cover(batch, system, index=k)
     batch.release()
 
 
@@ -177,21 +248,27 @@ def test_cell_plan_is_the_engines(bench_box):
     sim.release()
 
 
-def test_capacity_grows_by_grown_plan():
+@pytest.mark.parametrize("form", [1, 0])
+def test_capacity_grows_by_grown_plan(form):
     """A forced capacity of 64 on the 1,190-atom fixture overflows at the first build; the engine
-    grows it once by grownPlan (cells.js:282-288) from the measured requirement."""
+    grows it once by grownPlan (cells.js:282-288) from the measured requirement: the longest
+    per-atom row (the oracle's), or with group-pair rows the longest group row."""
     s, pos, _ = system_for("ala-wat")
     sim = GpuSimulation(s, {"alpha": 2.6282608939112584, "grid": [24, 24, 24], "skin": 0.1,
-                            "dispersionCorrection": False, "maxNeighbours": 64})
+                            "dispersionCorrection": False, "maxNeighbours": 64, "pairList": form})
     sim.setState(pos)
     sim.initialise()
     d = sim.diagnostics()
     assert d["neighbour_growths"] == 1
-    P = oracle.pack_params(s["boxVectors"], 1.0, float(np.float32(1.1)), 1.0)
-    plan = oracle.plan_cell_list(s["topology"]["atomCount"], s["boxVectors"], 1.0, skin=0.1)
-    _, cs, ca = oracle.cell_list_f32(pos.astype(np.float32), P, plan["counts"])
-    es, ep = exclusion_gather(s)
-    _, _, req = oracle.neighbour_list_f32(pos.astype(np.float32), P, plan["counts"], cs, ca, es, ep, 2048)
+    if form == 1:
+        P = oracle.pack_params(s["boxVectors"], 1.0, float(np.float32(1.1)), 1.0)
+        plan = oracle.plan_cell_list(s["topology"]["atomCount"], s["boxVectors"], 1.0, skin=0.1)
+        _, cs, ca = oracle.cell_list_f32(pos.astype(np.float32), P, plan["counts"])
+        es, ep = exclusion_gather(s)
+        _, _, req = oracle.neighbour_list_f32(pos.astype(np.float32), P, plan["counts"], cs, ca, es, ep, 2048)
+    else:
+        req = int(sim.debugGroupRows()["counts"].max())
+        assert d["neighbour_required"] == req
     assert d["neighbour_capacity"] == (oracle.grown_plan(64, req) + 3) // 4 * 4
     sim.release()
 

@@ -66,7 +66,7 @@ def test_cell_and_neighbour_lists_bit_exact(cutoff, group):
     warps a group, hits staged per x-slab); at 1.25 nm (2 x 2 x 1 cells) some atoms have more
     than 512 partners in one slab, which overflows the staging and takes its fallback."""
     s, pos, _ = system_for("ala-wat", cutoff=cutoff)
-    sim = engine_for(s, pos, alpha=None, grid=None, neighbourGroupAtoms=group)
+    sim = engine_for(s, pos, alpha=None, grid=None, neighbourGroupAtoms=group, pairList=1)
     counts, start, atoms = sim.debugCells()
     lc = np.float32(cutoff) + np.float32(0.1)
     P = oracle.pack_params(s["boxVectors"], cutoff, float(np.float32(cutoff + 0.1)), 1.0)
