@@ -587,6 +587,8 @@ def prepare(system, pos, grid, seed, npt, args):
     from rainmd_b200.simulation import GpuSimulation
 
     opts = options_for(grid, seed=seed)
+    if args.pair_list is not None:
+        opts["pairList"] = args.pair_list
     if npt:
         opts.update({"pressure": 1.0, "barostatInterval": BAROSTAT_INTERVAL})
     if args.rebuild_schedule:
@@ -694,6 +696,9 @@ def main():
     parser.add_argument("--seeds", type=int, nargs="+", default=[3, 4, 5],
                         help="seeds of the learned-barostat study's pairs of runs")
     parser.add_argument("--batch-steps", type=int, default=500)
+    parser.add_argument("--pair-list", type=int, choices=[0, 1], default=None,
+                        help="neighbour structure of the pair loop: 0 group-pair rows, 1 per-atom rows "
+                             "(default: the engine's)")
     parser.add_argument("--rebuild-schedule", action="store_true",
                         help="rebuild the lists on the reference's host schedule instead of on demand "
                              "(the same kernels; ncu profiles no kernel of a graph with conditional nodes)")

@@ -105,9 +105,9 @@ typedef struct {
   /* kernel shapes; 0 = chosen by the engine's autotuner at initialise() */
   int32_t neighbour_group_atoms; /* atoms per neighbour-search warp: 4, 8, 16 or 32 (per-atom rows;
                                     group-pair rows always search 4-atom groups) */
-  int32_t nonbonded_lanes;       /* lanes per atom in the pair loop: 8, 16 or 32 on per-atom rows;
-                                    on group-pair rows 8 lanes of each of the 1, 2, 4 or 8 warps
-                                    that share a group's row: 8, 16, 32 or 64 */
+  int32_t nonbonded_lanes;       /* pair-loop lanes: per atom on per-atom rows (8, 16 or 32); per
+                                    group row on group-pair rows (32, 64 or 128: one partner a
+                                    lane, the row shared by 1, 2 or 4 warps) */
   int32_t spread_atoms_per_block; /* atoms per PME charge-spreading block: 4, 8 or 16 */
   /* learned barostat (learned_barostat = 1) */
   int32_t learned_warmup_moves;  /* exact moves that train the surrogate before it screens; <= 0: 2000 */
@@ -389,7 +389,7 @@ rmd_status rmd_surrogate_evaluate(const float *params, const float *inputs, cons
  * the pair loop, atoms per PME spreading block}. When the options left a shape at 0,
  * initialise() chose it by timing every candidate (the engine's autotuner); tune_ms (may be
  * NULL) receives those times in ms per launch, in the order group 4/8/16, lanes 8/16/32
- * (16/32/64 on group-pair rows), spreading 4/8/16, with -1 for shapes that were not tuned. No reference counterpart: the
+ * (32/64/128 on group-pair rows), spreading 4/8/16, with -1 for shapes that were not tuned. No reference counterpart: the
  * reference's WGSL kernels have fixed workgroup sizes. */
 rmd_status rmd_kernel_shapes(const rmd_sim *sim, int32_t shapes[3], double tune_ms[9]);
 /* Set launch shapes by hand (0 keeps the current one). Results do not depend on them, except

@@ -495,9 +495,9 @@ void Engine::build(int count, const rmd_system *systems, const rmd_options *opti
     tune_group = o.neighbour_group_atoms == 0;
     tune_lanes = o.nonbonded_lanes == 0;
     tune_spread = o.spread_atoms_per_block == 0;
-    if (pair_list != 1) {  // group-pair rows: 4-atom search groups; lanes per group atom 8 x the
-      group_atoms = GROUP_ATOMS;  // warps that share a row (16, 32 or 64)
-      nb_lanes = o.nonbonded_lanes == 64 ? 64 : pick(o.nonbonded_lanes, 8, 16, 32, 32);
+    if (pair_list != 1) {  // group-pair rows: 4-atom search groups; lanes per group row 32 x the
+      group_atoms = GROUP_ATOMS;  // warps that share it (32, 64 or 128)
+      nb_lanes = pick(o.nonbonded_lanes, 32, 64, 128, 64);
       tune_group = false;
     }
   }
@@ -1379,6 +1379,7 @@ BaroArgs Engine::bargs() const {
   a.energies = energies.p;
   a.saved_energies = saved_energies.p;
   a.masses = masses.p;
+  a.disp = disp.p;
   return a;
 }
 
@@ -1601,7 +1602,7 @@ void Engine::autotune() {
   };
   const int groups[3] = {4, 8, 16}, spreads[3] = {4, 8, 16};
   int lanes[3] = {8, 16, 32};
-  if (pair_list != 1) lanes[0] = 16, lanes[1] = 32, lanes[2] = 64;  // 2, 4 or 8 warps a group row
+  if (pair_list != 1) lanes[0] = 32, lanes[1] = 64, lanes[2] = 128;  // 1, 2 or 4 warps a group row
   if (tune_group) {
     double best = 1e30;
     int pick = group_atoms;
@@ -1944,6 +1945,18 @@ void Engine::attempt_volume_change() {
   for (auto &h : hs) h.steps_since_rebuild = 1LL << 40;
   std::vector<double> bb((size_t)S * N_BARO);
   CUDA_OK(cudaMemcpy(bb.data(), baro.p, sizeof(double) * bb.size(), cudaMemcpyDeviceToHost));
+  // a rejected move leaves lists built in the trial box: rebuild them at the restored state
+  // before anything evaluates (the reference evaluates the restored state, simulation.js:1049-1056)
+  bool rejected = false;
+  for (int s = 0; s < S; ++s) {
+    const double *x = bb.data() + (size_t)s * N_BARO;
+    if (exact_move && hs[s].has_pressure && x[B_REFUSED] == 0.0 && x[B_SCREENED] == 0.0 && x[B_ACCEPT] == 0.0)
+      rejected = true;
+  }
+  if (rejected) {
+    evaluate(true, false);
+    sync();
+  }
   std::vector<DevSysD> dd(S);
   CUDA_OK(cudaMemcpy(dd.data(), sysd.p, sizeof(DevSysD) * S, cudaMemcpyDeviceToHost));
   (void)b;
@@ -2847,12 +2860,18 @@ rmd_status rmd_set_kernel_shapes(rmd_sim *sim, int32_t group_atoms, int32_t nonb
                                  int32_t spread_atoms) {
   if (!sim) return RMD_ERR_INVALID;
   auto ok = [](int v, int a, int b, int c) { return v == 0 || v == a || v == b || v == c; };
-  if (!(ok(group_atoms, 4, 8, 16) || group_atoms == 32) || !(ok(nonbonded_lanes, 8, 16, 32) || nonbonded_lanes == 64) ||
+  if (!(ok(group_atoms, 4, 8, 16) || group_atoms == 32) || !(ok(nonbonded_lanes, 8, 16, 32) || ok(nonbonded_lanes, 32, 64, 128)) ||
       !ok(spread_atoms, 4, 8, 16))
     return RMD_ERR_INVALID;
   auto &e = sim->engine;
-  if (e.pair_list != 1 && group_atoms && group_atoms != rmd::GROUP_ATOMS) {
-    e.last_error = "with group-pair rows the search groups hold 4 atoms";
+  if (e.pair_list != 1 && ((group_atoms && group_atoms != rmd::GROUP_ATOMS) ||
+                            (nonbonded_lanes && nonbonded_lanes != 32 && nonbonded_lanes != 64 &&
+                             nonbonded_lanes != 128))) {
+    e.last_error = "with group-pair rows the search groups hold 4 atoms and a row is shared by 32, 64 or 128 lanes";
+    return RMD_ERR_INVALID;
+  }
+  if (e.pair_list == 1 && nonbonded_lanes > 32) {
+    e.last_error = "per-atom rows take 8, 16 or 32 lanes an atom";
     return RMD_ERR_INVALID;
   }
   if (group_atoms) e.group_atoms = group_atoms;

@@ -235,6 +235,7 @@ struct BaroArgs {
   double *energies;  // per system N_ENERGY
   double *saved_energies;
   const float *masses;
+  unsigned *disp;    // per system: largest squared displacement since the lists were built (f32 bits)
 };
 enum BaroSlot {
   B_ACTIVE = 0, B_PRESSURE, B_KT, B_NMOL, B_SEED, B_ATTEMPTS, B_ACCEPTED, B_WINDOW_ATT, B_WINDOW_ACC,

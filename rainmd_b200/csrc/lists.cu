@@ -669,6 +669,9 @@ __global__ void __launch_bounds__(32 * GROUP_ROW_WARPS)
         const int wz = rz < 0 ? -1 : (rz >= counts[2] ? 1 : 0);
         const int cz = rz - wz * counts[2];
         const int cell = (cx * counts[1] + cy) * counts[2] + cz;
+        // a cell before the group's own holds only atoms earlier in search order: the groups
+        // they belong to list those pairs
+        if (cell < cell0) continue;
         const int begin = s.atom_start + cell_start[s.cell_start_base + cell];
         const int end = s.atom_start + cell_start[s.cell_start_base + cell + 1];
         // the lattice images to search this cell through: the stencil's own wrap on an axis

@@ -220,34 +220,40 @@ __global__ void __launch_bounds__(128) k_nonbonded(
 }
 
 // ------------------------------------------------------------------ group-pair kernel
-// The same pair physics over the group-pair rows (lists.cu k_group_rows): one WARP per group of
-// GROUP_ATOMS atoms, lane = 8 * a + t for the group's atom a and partner slot t, so that a pass
-// over 8 row entries evaluates 32 pairs and each entry's partner record is loaded once for the
-// group's atoms. Each pair is evaluated once, from the group that lists it: its force is
-// quantised to 64-bit fixed point (as the atom-row kernel's precision form does), added to the
-// group atom's registers, and its negation summed over the group's four atoms with integer
-// shuffles and added to the partner's force with one 64-bit atomic per component. Because the
-// pair force is computed from the same f32 operands in the same order as the atom-row kernel
-// computes it from either atom (the charge product is symmetric, the image shifts of opposite
-// codes are exact negatives, and rounding to nearest is odd), every atom's force is the same
-// sum of the same integers as there, bit for bit. Energies (ENERGY) are accumulated the same
-// way into per-atom integer sums that hold each pair's full energy for both of its atoms, then
-// halved, which is the atom-row kernel's per-atom value exactly. The force array (and, for
-// ENERGY, the energy sums) must be zero when the kernel starts; the exceptions of each group
-// atom are evaluated by its eight lanes, as in the atom-row kernel.
+// The same pair physics over the group-pair rows (lists.cu k_group_rows). A row's entries are
+// dealt to the lanes of `split` warps, one partner a lane, and each lane evaluates its partner
+// against the group's GROUP_ATOMS atoms in turn (their positions, charges and LJ rows are held
+// in every lane's registers), so a pass of a warp over 32 entries evaluates 128 pairs. Each pair
+// is evaluated once, from the group that lists it. Its force is quantised to 64-bit fixed point
+// (as the atom-row kernel's precision form does) and added to two integer sums in the lane's
+// registers: the group atom's (one per group atom, reduced over the warp once, at the end of
+// the row) and the partner's (its negation, added to the force array with one 64-bit atomic per
+// component at the end of the lane's entry). Because the pair force is computed from the same
+// f32 operands in the same order as the atom-row kernel computes it from either atom (the
+// charge product is symmetric, the image shifts of opposite codes are exact negatives, and
+// rounding to nearest is odd), every atom's force is the same sum of the same integers as
+// there, bit for bit. Energies (ENERGY) are accumulated the same way into per-atom integer sums
+// that hold each pair's full energy for both of its atoms, then halved, which is the atom-row
+// kernel's per-atom value exactly. The force array (and, for ENERGY, the energy sums) must be
+// zero when the kernel starts. The exceptions of each group atom are evaluated by 8 lanes of the
+// row's first warp, as in the atom-row kernel.
 
-// Sum four 64-bit values (v0..v3) over the 4 lanes that differ in lane bits (b_hi, b_lo); on
-// return lane (bit_hi, bit_lo) holds the sum of value 2 * bit_hi + bit_lo. Three shuffles of
-// 64-bit words instead of eight.
-template <int B_HI, int B_LO>
-__device__ __forceinline__ long long reduce_four(long long v0, long long v1, long long v2, long long v3, int lane) {
-  const bool hi = (lane >> B_HI) & 1;
-  const long long send0 = hi ? v0 : v2, send1 = hi ? v1 : v3;
-  const long long keep0 = hi ? v2 : v0, keep1 = hi ? v3 : v1;
-  const long long a = keep0 + __shfl_xor_sync(0xffffffffu, send0, 1 << B_HI);
-  const long long b = keep1 + __shfl_xor_sync(0xffffffffu, send1, 1 << B_HI);
-  const bool low = (lane >> B_LO) & 1;
-  return (low ? b : a) + __shfl_xor_sync(0xffffffffu, low ? a : b, 1 << B_LO);
+// Warp sum of 16 64-bit values (v[0..15]): returns in lane l the sum over all 32 lanes of
+// v[(l >> 1) & 15] (the lane pair 2k, 2k + 1 holds value k). Five exchange levels that halve the
+// values each lane carries, 16 + 8 + 4 + 2 + 1 shuffles of 64-bit words instead of 80.
+__device__ __forceinline__ long long warp_sum_sixteen(long long (&v)[16], int lane) {
+#pragma unroll
+  for (int level = 0, width = 16; level < 4; ++level, width >>= 1) {
+    const int bit = 4 - level;  // exchange across lane bit 4, then 3, 2, 1
+    const bool hi = (lane >> bit) & 1;
+#pragma unroll
+    for (int k = 0; k < width / 2; ++k) {
+      const long long send = hi ? v[k] : v[k + width / 2];
+      const long long keep = hi ? v[k + width / 2] : v[k];
+      v[k] = keep + __shfl_xor_sync(0xffffffffu, send, 1 << bit);
+    }
+  }
+  return v[0] + __shfl_xor_sync(0xffffffffu, v[0], 1);
 }
 
 template <bool ENERGY>
@@ -259,140 +265,211 @@ __global__ void __launch_bounds__(128) k_group_pairs(
     const int *__restrict__ exc_partner, const float4 *__restrict__ exc_param,
     unsigned long long *__restrict__ force, unsigned long long *__restrict__ e_acc, int n_atoms, int n_groups,
     int lj_entries, int split) {
+  constexpr int G = GROUP_ATOMS;
   extern __shared__ float2 lj_shared[];
   const bool lj_in_smem = lj_entries > 0;
   for (int k = threadIdx.x; k < lj_entries; k += blockDim.x) lj_shared[k] = lj[k];
   if (lj_in_smem) __syncthreads();
-  // `split` warps share a group's row, warp r taking passes r, r + split, ...: a long row is
-  // several short serial chains rather than one (each warp's passes are latency-bound)
+  // `split` warps share a group's row, warp r taking the passes r, r + split, ...
   const int task = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int warp = task / split, part = task - warp * split;  // the group slot, this warp's share
-  const int lane = threadIdx.x & 31, a = lane >> 3, t = lane & 7;
+  const int lane = threadIdx.x & 31;
   if (warp >= n_groups) return;
   const int size = gsize[warp];
   if (size == 0) return;  // an unused slot (the whole warp leaves)
   const DevSys &s = sys[group_sys[warp]];
-  const bool vi = a < size;
-  const int si = group_order[gfirst[warp] + (vi ? a : 0)];
-  const int2 info_i = slot_info[si];
-  const float4 pw = spos[si];
-  const float2 *ljrow = (lj_in_smem ? lj_shared : lj) + s.lj_base + info_i.x * s.type_count;
+  const float2 *ljtab = (lj_in_smem ? lj_shared : lj) + s.lj_base;
+  // the group's atoms, the same in every lane (an absent atom is masked by every entry)
+  float4 pa[G];
+  int ta[G], ia[G];
+  const int first = gfirst[warp];
+#pragma unroll
+  for (int a = 0; a < G; ++a) {
+    const int si = group_order[first + (a < size ? a : 0)];
+    const int2 info = slot_info[si];
+    pa[a] = spos[si];
+    ta[a] = info.x * s.type_count;
+    ia[a] = info.y;
+  }
   const float alpha = s.alpha;
   const float gauss_k = 2.0f * alpha * 0.5641895835477563f;  // 2a/sqrt(pi)
   const float cut2 = s.cutoff2;
   const int count = gnbr_count[warp];
   const int *row = gnbr + s.gnbr_base + (long long)(warp - s.group_base) * s.nbr_capacity;
-  long long qx = 0, qy = 0, qz = 0, qlj = 0, qcoul = 0, qvir = 0;
+  // per group atom: force x, y, z (and energies lj, coulomb, virial) in fixed point
+  long long acc[G][ENERGY ? 6 : 3];
+#pragma unroll
+  for (int a = 0; a < G; ++a)
+#pragma unroll
+    for (int c = 0; c < (ENERGY ? 6 : 3); ++c) acc[a][c] = 0;
+  const int stride = 32 * split;
+  int k = 32 * part + lane;
   // software pipeline: the next pass's entry and partner record are loaded while this pass's
   // pairs are computed
-  const int stride = 8 * split;
-  int k0 = 8 * part;
-  unsigned e1 = k0 + t < count ? (unsigned)__ldg(row + k0 + t) : (0xFu << GROUP_MASK_SHIFT);
+  unsigned e1 = k < count ? (unsigned)__ldg(row + k) : (0xFu << GROUP_MASK_SHIFT);
   float4 pj1 = __ldg(spos + (e1 & GROUP_SLOT_MASK));
   int2 info1 = __ldg(slot_info + (e1 & GROUP_SLOT_MASK));
-  for (; k0 < count; k0 += stride) {
+  float4 S1 = s.shift[(e1 >> GROUP_CODE_SHIFT) & 31u];
+  for (int k0 = 32 * part; k0 < count; k0 += stride, k += stride) {
     const unsigned e = e1;
-    const float4 pj = pj1;
+    const float4 pj = pj1, S = S1;
     const int2 info_j = info1;
     if (k0 + stride < count) {
-      e1 = k0 + stride + t < count ? (unsigned)__ldg(row + k0 + stride + t) : (0xFu << GROUP_MASK_SHIFT);
+      e1 = k + stride < count ? (unsigned)__ldg(row + k + stride) : (0xFu << GROUP_MASK_SHIFT);
       pj1 = __ldg(spos + (e1 & GROUP_SLOT_MASK));
       info1 = __ldg(slot_info + (e1 & GROUP_SLOT_MASK));
+      S1 = s.shift[(e1 >> GROUP_CODE_SHIFT) & 31u];
     }
-    const float4 S = s.shift[(e >> GROUP_CODE_SHIFT) & 31u];
-    const float3 d = make_float3(pw.x - pj.x - S.x, pw.y - pj.y - S.y, pw.z - pj.z - S.z);
-    const float r2 = fmaf(d.x, d.x, fmaf(d.y, d.y, d.z * d.z));
-    long long fx = 0, fy = 0, fz = 0, el = 0, ec = 0, ev = 0;
-    if (vi && !((e >> (GROUP_MASK_SHIFT + a)) & 1u) && r2 <= cut2) {
-      const float inv_r = rsqrt_refined(r2);
-      const float inv_r2 = inv_r * inv_r;
-      const float inv_r6 = inv_r2 * inv_r2 * inv_r2;
-      const float2 ab = ljrow[info_j.x];
-      const float a12 = ab.x * inv_r6 * inv_r6, b6 = ab.y * inv_r6;
-      float scalar = (12.0f * a12 - 6.0f * b6) * inv_r2;
-      const float qq = (float)ONE_4PI_EPS0 * (pw.w * pj.w);
-      const float r = r2 * inv_r;
-      float gauss;
-      const float screened = erfc_and_gauss(alpha * r, gauss);
-      scalar = fmaf(qq * fmaf(screened, inv_r, gauss_k * gauss), inv_r2, scalar);
-      fx = (long long)to_fixed(scalar * d.x);
-      fy = (long long)to_fixed(scalar * d.y);
-      fz = (long long)to_fixed(scalar * d.z);
-      qx += fx;
-      qy += fy;
-      qz += fz;
-      if (ENERGY) {
-        el = (long long)to_fixed(a12 - b6);
-        ec = (long long)to_fixed(qq * screened * inv_r);
-        ev = (long long)to_fixed(scalar * r2);
-        qlj += el;
-        qcoul += ec;
-        qvir += ev;
+    long long jx = 0, jy = 0, jz = 0, jl = 0, jc = 0, jv = 0;
+    // The four pairs are evaluated without branches (a pair that is masked or beyond the cutoff
+    // is evaluated at r = 1 nm and contributes zero), so their chains can interleave.
+#pragma unroll
+    for (int a = 0; a < G; ++a) {
+      const float3 d = make_float3(pa[a].x - pj.x - S.x, pa[a].y - pj.y - S.y, pa[a].z - pj.z - S.z);
+      const float r2d = fmaf(d.x, d.x, fmaf(d.y, d.y, d.z * d.z));
+      const bool in = !((e >> (GROUP_MASK_SHIFT + a)) & 1u) && r2d <= cut2;
+      const float r2 = in ? r2d : 1.0f;
+      {
+        const float inv_r = rsqrt_refined(r2);
+        const float inv_r2 = inv_r * inv_r;
+        const float inv_r6 = inv_r2 * inv_r2 * inv_r2;
+        const float2 ab = ljtab[ta[a] + info_j.x];
+        const float a12 = ab.x * inv_r6 * inv_r6, b6 = ab.y * inv_r6;
+        float scalar = (12.0f * a12 - 6.0f * b6) * inv_r2;
+        const float qq = (float)ONE_4PI_EPS0 * (pa[a].w * pj.w);
+        const float r = r2 * inv_r;
+        float gauss;
+        const float screened = erfc_and_gauss(alpha * r, gauss);
+        scalar = fmaf(qq * fmaf(screened, inv_r, gauss_k * gauss), inv_r2, scalar);
+        scalar = in ? scalar : 0.0f;
+        const long long fx = (long long)to_fixed(scalar * d.x);
+        const long long fy = (long long)to_fixed(scalar * d.y);
+        const long long fz = (long long)to_fixed(scalar * d.z);
+        acc[a][0] += fx;
+        acc[a][1] += fy;
+        acc[a][2] += fz;
+        jx += fx;
+        jy += fy;
+        jz += fz;
+        if (ENERGY) {
+          const long long el = in ? (long long)to_fixed(a12 - b6) : 0;
+          const long long ec = in ? (long long)to_fixed(qq * screened * inv_r) : 0;
+          const long long ev = (long long)to_fixed(scalar * r2);
+          acc[a][ENERGY ? 3 : 0] += el;
+          acc[a][ENERGY ? 4 : 0] += ec;
+          acc[a][ENERGY ? 5 : 0] += ev;
+          jl += el;
+          jc += ec;
+          jv += ev;
+        }
       }
     }
-    // the partner's share, summed over the group's four atoms (lane bits 4 and 3): lane a then
-    // holds component a of it
-    const long long fj = reduce_four<4, 3>(-fx, -fy, -fz, 0, lane);
-    if (a < 3 && fj != 0) atomicAdd(force + a * (long long)n_atoms + info_j.y, (unsigned long long)fj);
+    // the partner's share: the negated pair forces (the energies as they are)
+    const int j = info_j.y;
+    if (jx != 0) atomicAdd(force + j, (unsigned long long)(-jx));
+    if (jy != 0) atomicAdd(force + n_atoms + j, (unsigned long long)(-jy));
+    if (jz != 0) atomicAdd(force + 2 * (long long)n_atoms + j, (unsigned long long)(-jz));
     if (ENERGY) {
-      const long long ej = reduce_four<4, 3>(el, ec, ev, 0, lane);
-      if (a < 3 && ej != 0) atomicAdd(e_acc + a * (long long)n_atoms + info_j.y, (unsigned long long)ej);
+      if (jl != 0) atomicAdd(e_acc + j, (unsigned long long)jl);
+      if (jc != 0) atomicAdd(e_acc + n_atoms + j, (unsigned long long)jc);
+      if (jv != 0) atomicAdd(e_acc + 2 * (long long)n_atoms + j, (unsigned long long)jv);
     }
   }
-  // Exceptions of the group atom: 1-4 scaled LJ/Coulomb and -q_i q_j erf(a r)/r, no cutoff,
-  // exactly as the atom-row kernel evaluates them.
-  const int i = info_i.y;
-  const int eb = exc_start[i], ee = vi && part == 0 ? exc_start[i + 1] : eb;
-  const float4 pi = posq[i];
-  for (int e = eb + t; e < ee; e += 8) {
-    float pair_lj = 0.f, pair_coul = 0.f;
-    const int j = exc_partner[e];
-    const float4 prm = exc_param[e];  // chargeProduct, ljA, ljB, fullProduct
-    const float4 pj = posq[j];
-    float3 d = min_image(make_float3(pi.x - pj.x, pi.y - pj.y, pi.z - pj.z), s);
-    const float r2 = fmaf(d.x, d.x, fmaf(d.y, d.y, d.z * d.z));
-    const float inv_r = rsqrt_refined(r2);
-    const float inv_r2 = inv_r * inv_r, inv_r6 = inv_r2 * inv_r2 * inv_r2;
-    float scalar = 0.f;
-    if (prm.y != 0.f || prm.z != 0.f) {
-      const float a12 = prm.y * inv_r6 * inv_r6, b6 = prm.z * inv_r6;
-      scalar += (12.0f * a12 - 6.0f * b6) * inv_r2;
-      if (ENERGY) pair_lj += a12 - b6;
+  // Exceptions of the group atoms (first warp of the row: lanes 8a .. 8a + 7 for atom a): 1-4
+  // scaled LJ/Coulomb and -q_i q_j erf(a r)/r, no cutoff, exactly as the atom-row kernel
+  // evaluates them.
+  {
+    const int a = lane >> 3, t = lane & 7;
+    const bool vi = a < size && part == 0;
+    const int i = vi ? ia[0] : 0;
+    int ii = ia[0];
+#pragma unroll
+    for (int b = 1; b < G; ++b)
+      if (a == b) ii = ia[b];
+    const int eb = vi ? exc_start[ii] : 0, ee = vi ? exc_start[ii + 1] : 0;
+    (void)i;
+    const float4 pi = posq[ii];
+    long long ex = 0, ey = 0, ez = 0, el = 0, ec = 0, ev = 0;
+    for (int e = eb + t; e < ee; e += 8) {
+      float pair_lj = 0.f, pair_coul = 0.f;
+      const int jj = exc_partner[e];
+      const float4 prm = exc_param[e];  // chargeProduct, ljA, ljB, fullProduct
+      const float4 pk = posq[jj];
+      float3 d = min_image(make_float3(pi.x - pk.x, pi.y - pk.y, pi.z - pk.z), s);
+      const float r2 = fmaf(d.x, d.x, fmaf(d.y, d.y, d.z * d.z));
+      const float inv_r = rsqrt_refined(r2);
+      const float inv_r2 = inv_r * inv_r, inv_r6 = inv_r2 * inv_r2 * inv_r2;
+      float scalar = 0.f;
+      if (prm.y != 0.f || prm.z != 0.f) {
+        const float a12 = prm.y * inv_r6 * inv_r6, b6 = prm.z * inv_r6;
+        scalar += (12.0f * a12 - 6.0f * b6) * inv_r2;
+        if (ENERGY) pair_lj += a12 - b6;
+      }
+      if (prm.x != 0.f) {
+        const float qq = (float)ONE_4PI_EPS0 * prm.x;
+        scalar += qq * inv_r * inv_r2;
+        if (ENERGY) pair_coul += qq * inv_r;
+      }
+      if (alpha > 0.f && prm.w != 0.f) {
+        const float qq = (float)ONE_4PI_EPS0 * prm.w;
+        float gauss;
+        const float r = r2 * inv_r;
+        const float unscreened = 1.0f - erfc_and_gauss(alpha * r, gauss);
+        scalar -= qq * (unscreened * inv_r - gauss_k * gauss) * inv_r2;
+        if (ENERGY) pair_coul -= qq * unscreened * inv_r;
+      }
+      if (ENERGY) {
+        el += (long long)to_fixed(pair_lj);
+        ec += (long long)to_fixed(pair_coul);
+        ev += (long long)to_fixed(scalar * r2);
+      }
+      ex += (long long)to_fixed(scalar * d.x);
+      ey += (long long)to_fixed(scalar * d.y);
+      ez += (long long)to_fixed(scalar * d.z);
     }
-    if (prm.x != 0.f) {
-      const float qq = (float)ONE_4PI_EPS0 * prm.x;
-      scalar += qq * inv_r * inv_r2;
-      if (ENERGY) pair_coul += qq * inv_r;
+#pragma unroll
+    for (int b = 0; b < G; ++b) {
+      if (a == b) {
+        acc[b][0] += ex;
+        acc[b][1] += ey;
+        acc[b][2] += ez;
+        if (ENERGY) {
+          acc[b][ENERGY ? 3 : 0] += el;
+          acc[b][ENERGY ? 4 : 0] += ec;
+          acc[b][ENERGY ? 5 : 0] += ev;
+        }
+      }
     }
-    if (alpha > 0.f && prm.w != 0.f) {
-      const float qq = (float)ONE_4PI_EPS0 * prm.w;
-      float gauss;
-      const float r = r2 * inv_r;
-      const float unscreened = 1.0f - erfc_and_gauss(alpha * r, gauss);
-      scalar -= qq * (unscreened * inv_r - gauss_k * gauss) * inv_r2;
-      if (ENERGY) pair_coul -= qq * unscreened * inv_r;
-    }
-    if (ENERGY) {
-      qlj += (long long)to_fixed(pair_lj);
-      qcoul += (long long)to_fixed(pair_coul);
-      qvir += (long long)to_fixed(scalar * r2);
-    }
-    qx += (long long)to_fixed(scalar * d.x);
-    qy += (long long)to_fixed(scalar * d.y);
-    qz += (long long)to_fixed(scalar * d.z);
   }
-  // the group atom's sums over its eight lanes (lane bits 2, 1 and 0): lanes 2c and 2c + 1
-  // then hold component c
-  long long fi = reduce_four<2, 1>(qx, qy, qz, 0, lane);
-  fi += __shfl_xor_sync(0xffffffffu, fi, 1);
-  const int comp = (lane >> 1) & 3;
-  if (vi && (lane & 1) == 0 && comp < 3 && fi != 0)
-    atomicAdd(force + comp * (long long)n_atoms + i, (unsigned long long)fi);
-  if (ENERGY) {
-    long long ei = reduce_four<2, 1>(qlj, qcoul, qvir, 0, lane);
-    ei += __shfl_xor_sync(0xffffffffu, ei, 1);
-    if (vi && (lane & 1) == 0 && comp < 3 && ei != 0)
-      atomicAdd(e_acc + comp * (long long)n_atoms + i, (unsigned long long)ei);
+  // the group atoms' sums over the warp: value 4a + c (component c of atom a) ends in lanes
+  // 2(4a + c) and 2(4a + c) + 1; the lane with the even index adds it to the atom
+  {
+    long long v[16];
+#pragma unroll
+    for (int a = 0; a < G; ++a) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) v[4 * a + c] = acc[a][c];
+      v[4 * a + 3] = 0;
+    }
+    const long long sum = warp_sum_sixteen(v, lane);
+    const int slot = (lane >> 1) & 15, a = slot >> 2, c = slot & 3;
+    int ii = ia[0];
+#pragma unroll
+    for (int b = 1; b < G; ++b)
+      if (a == b) ii = ia[b];
+    if ((lane & 1) == 0 && c < 3 && a < size && sum != 0)
+      atomicAdd(force + c * (long long)n_atoms + ii, (unsigned long long)sum);
+    if (ENERGY) {
+#pragma unroll
+      for (int b = 0; b < G; ++b) {
+#pragma unroll
+        for (int q = 0; q < 3; ++q) v[4 * b + q] = acc[b][ENERGY ? 3 + q : 0];
+        v[4 * b + 3] = 0;
+      }
+      const long long esum = warp_sum_sixteen(v, lane);
+      if ((lane & 1) == 0 && c < 3 && a < size && esum != 0)
+        atomicAdd(e_acc + c * (long long)n_atoms + ii, (unsigned long long)esum);
+    }
   }
 }
 
@@ -408,7 +485,7 @@ __global__ void k_group_pair_energies(const unsigned long long *__restrict__ e_a
 }
 
 static void launch_group_pairs(const LaunchCtx &c, bool energy, int lanes, cudaStream_t stream) {
-  const int split = lanes >= 64 ? 8 : lanes >= 32 ? 4 : lanes >= 16 ? 2 : 1;  // 8 lanes per group atom per warp
+  const int split = lanes >= 128 ? 4 : lanes >= 64 ? 2 : 1;  // lanes per group row: warps sharing it x 32
   // (errors of these calls surface in the caller's cudaGetLastError, as the launches' do)
   (void)cudaMemsetAsync(c.force, 0, sizeof(unsigned long long) * 3 * (size_t)c.n_atoms, stream);
   if (energy) (void)cudaMemsetAsync(c.e_acc, 0, sizeof(unsigned long long) * 3 * (size_t)c.n_atoms, stream);

@@ -293,6 +293,11 @@ __global__ void k_baro_decide(BaroArgs a) {
     set_box(a.sys[s], d, ob);
     for (int k = 0; k < 3; ++k) a.sys[s].cell_counts[k] = d.saved_counts[k];
     for (int k = 0; k < N_ENERGY; ++k) a.energies[s * N_ENERGY + k] = a.saved_energies[s * N_ENERGY + k];
+    // The lists of the trial evaluation were built in the trial box, with wrap shifts that are
+    // multiples of its vectors: they do not describe the restored positions in the restored
+    // box. Mark them stale (the largest finite displacement), so that the next rebuild
+    // decision rebuilds this system before its next force evaluation.
+    a.disp[s] = 0x7f7fffffu;
   }
   if (!learned && b[B_WINDOW_ATT] >= 10.0) {  // simulation.js:1058-1063 (stage 1 does it when learned)
     const double rate = b[B_WINDOW_ACC] / b[B_WINDOW_ATT];

@@ -414,7 +414,7 @@ class BatchSimulation:
         def table(row, keys):
             return {k: float(v) for k, v in zip(keys, row) if v >= 0}
 
-        lanes = (8, 16, 32) if self.diagnostics()["pair_list"] == 1 else (16, 32, 64)
+        lanes = (8, 16, 32) if self.diagnostics()["pair_list"] == 1 else (32, 64, 128)
         return {"neighbourGroupAtoms": int(shapes[0]), "nonbondedLanes": int(shapes[1]),
                 "spreadAtomsPerBlock": int(shapes[2]),
                 "tuned": {"neighbourGroupAtoms": table(ms[0:3], (4, 8, 16)),

@@ -72,13 +72,13 @@ def test_every_shape_gives_bitwise_identical_results():
 
 
 def test_group_pair_rows_tune_the_row_split_and_the_spreading():
-    """Group-pair rows: 4-atom search groups always; the warps sharing a row (2, 4 or 8: 16, 32
-    or 64 lanes per group atom) and the spreading block are timed and the fastest kept."""
+    """Group-pair rows: 4-atom search groups always; the warps sharing a row (1, 2 or 4: 32, 64
+    or 128 lanes a row) and the spreading block are timed and the fastest kept."""
     system, pos = water()
     sim = make(system, pos, pairList=0)
     shapes = sim.kernelShapes()
     assert shapes["neighbourGroupAtoms"] == 4 and shapes["tuned"]["neighbourGroupAtoms"] == {}
-    for name, candidates in (("nonbondedLanes", [16, 32, 64]), ("spreadAtomsPerBlock", [4, 8, 16])):
+    for name, candidates in (("nonbondedLanes", [32, 64, 128]), ("spreadAtomsPerBlock", [4, 8, 16])):
         tuned = shapes["tuned"][name]
         assert sorted(tuned) == candidates, name
         assert shapes[name] == min(tuned, key=tuned.get), name
@@ -91,7 +91,7 @@ def test_group_pair_rows_give_the_per_atom_rows_results_bit_for_bit():
     bit for bit, and so does a group-pair run whose builds also write the per-atom rows."""
     system, pos = water()
     results = []
-    for form, lanes in ((1, 16), (0, 16), (2, 64), (0, 8)):
+    for form, lanes in ((1, 16), (0, 32), (2, 128), (0, 64)):
         sim = make(system, pos, pairList=form, spreadAtomsPerBlock=8, nonbondedLanes=lanes)
         energy, forces = sim.debugEvaluate()
         sim.minimise(maxIterations=20)

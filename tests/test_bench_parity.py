@@ -147,10 +147,13 @@ def assert_group_rows_cover(sim, system, index=0, skin=0.15):
     stencil = all(c >= 3 for c in plan["counts"])
     if stencil:
         assert len(listed) == len(key)  # each pair once
-    # the listed image of every pair within the list cutoff is one within it
+    # the listed image of every pair within the list cutoff is one within it; image codes refer
+    # to the positions wrapped into the box at the build (whole box vectors subtracted)
     ka, kb, kc = pc // 9 - 1, (pc // 3) % 3 - 1, pc % 3 - 1
     shift = (ka[:, None] * box[0:3] + kb[:, None] * box[3:6] + kc[:, None] * box[6:9])
+    rows3 = box.reshape(3, 3)
     x = origin.astype(np.float64).reshape(-1, 3)
+    x = x - np.floor(x @ np.linalg.inv(rows3)) @ rows3
     d2 = np.sum((x[pi] - x[pj] - shift) ** 2, axis=1)
     within = np.isin(key, expect)
     lc = cutoff + skin
