@@ -214,6 +214,7 @@ struct Engine {
   // slot; per slot its partner record and order position; per-atom integer energy sums
   int pair_list = 1;
   DevArray<int> gnbr, gnbr_count, gfirst, gsize, order_pos;
+  DevArray<float4> group_box;
   DevArray<int2> slot_info;
   DevArray<unsigned long long> e_acc;
   // list builds counted on the device: [0] those an IF node took, [1] all of them
@@ -1170,6 +1171,10 @@ void Engine::allocate_neighbours() {
     a->alloc(std::max(1, n_groups_total));
     a->zero();
   }
+  if (group_box.n < 2 * (size_t)std::max(1, n_groups_total)) {
+    group_box.alloc(2 * (size_t)std::max(1, n_groups_total));
+    group_box.zero();
+  }
   // push only the neighbour fields (the box may have been changed on the device)
   std::vector<DevSys> cur(S);
   CUDA_OK(cudaMemcpy(cur.data(), sys.p, sizeof(DevSys) * S, cudaMemcpyDeviceToHost));
@@ -1218,6 +1223,7 @@ LaunchCtx Engine::ctx() const {
   c.gsize = gsize.p;
   c.slot_info = slot_info.p;
   c.order_pos = order_pos.p;
+  c.group_box = group_box.p;
   c.e_acc = e_acc.p;
   c.origin = origin.p;
   c.spos = spos.p;
@@ -1465,6 +1471,10 @@ void Engine::record_barostat() {
   launch_baro_propose(b, stream);
   launch_baro_scale(b, stream);
   record_forces(true, true);
+  if (learned) {
+    launch_surrogate_reverse(b, sargs(), stream);
+    recorded += 1;
+  }
   launch_baro_decide(b, stream);
   launch_baro_restore(b, stream);
   recorded += 4;
@@ -2216,7 +2226,7 @@ void rmd_default_options(rmd_options *o) {
   o->neighbour_slack = 2.0;
   o->ewald_tolerance = 5e-4;
   o->pme_order = 5;
-  o->pair_list = 1;
+  o->pair_list = 0;
 }
 
 rmd_status rmd_plan_system(const rmd_system *system, const rmd_options *options, rmd_plan *out) {

@@ -100,6 +100,7 @@ struct LaunchCtx {
   int *gfirst, *gsize;     // per group slot: its first position in group_order, its atoms (0: unused)
   int2 *slot_info;         // per slot: LJ type, original index
   int *order_pos;          // per slot: its position in group_order
+  float4 *group_box;       // per group slot: bounding box lo, hi of its atoms' wrapped positions
   unsigned long long *e_acc;  // per-atom integer energy sums of the group-pair kernel (3 N)
   // cell-ordered copies written at each rebuild and kept current by the integrator:
   // spos[slot] = position minus the atom's wrap shift (w = charge), the original index,
@@ -271,6 +272,8 @@ struct SurrogateArgs {
 };
 void launch_surrogate_stage1(const BaroArgs &a, const SurrogateArgs &m, cudaStream_t stream);
 void launch_surrogate_train(const SurrogateArgs &m, cudaStream_t stream);
+// the stage-1 weight of the reverse move around the trial state (after its exact evaluation)
+void launch_surrogate_reverse(const BaroArgs &a, const SurrogateArgs &m, cudaStream_t stream);
 // standalone forward and gradient of one network on given data (for the gradient check)
 void surrogate_predict(const float *params, const float *x, int count, float *out, cudaStream_t stream);
 void surrogate_gradients(const float *params, const float *x, const float *target, int count,

@@ -28,6 +28,10 @@ struct LaunchCtxView {
   int *group_order;
   int2 *slot_info;  // per slot: LJ type, original index (the group-pair kernel's partner record)
   int *order_pos;   // per slot: its position in group_order
+  // group-pair rows only (else null): per 4-atom group slot its bounding box (lo, hi) of wrapped
+  // positions, and the cell scan's first group per cell
+  float4 *group_box;
+  const int *cell_gstart;
 };
 
 __global__ void k_cells_assign(const float4 *__restrict__ posq, const int *__restrict__ sys_of_atom,
@@ -239,6 +243,20 @@ __global__ void k_cells_sort(const int *__restrict__ cell_sys, const DevSys *__r
       place_sorted(v, s, gbase + k, slice[k], cc);
       v.group_order[gbase + k] = gbase + k;
       v.order_pos[gbase + k] = gbase + k;
+    }
+  }
+  if (v.group_box) {  // the bounding box of each 4-atom group of this cell, for the search's cull
+    __syncthreads();
+    const int first_group = s.group_base + v.cell_gstart[s.cell_start_base + c];
+    for (int k = threadIdx.x; 4 * k < n; k += blockDim.x) {
+      float4 lo = make_float4(INFINITY, INFINITY, INFINITY, 0.f), hi = make_float4(-INFINITY, -INFINITY, -INFINITY, 0.f);
+      for (int a = 4 * k; a < min(n, 4 * k + 4); ++a) {
+        const float4 p = v.spos[v.group_order[gbase + a]];
+        lo = make_float4(fminf(lo.x, p.x), fminf(lo.y, p.y), fminf(lo.z, p.z), 0.f);
+        hi = make_float4(fmaxf(hi.x, p.x), fmaxf(hi.y, p.y), fmaxf(hi.z, p.z), 0.f);
+      }
+      v.group_box[2 * (first_group + k)] = lo;
+      v.group_box[2 * (first_group + k) + 1] = hi;
     }
   }
 }
@@ -572,11 +590,12 @@ __global__ void __launch_bounds__(32 * GROUP_ROW_WARPS)
                  const int *__restrict__ cell_gstart, const int *__restrict__ group_order,
                  const int *__restrict__ excl_start, const int *__restrict__ excl_partners,
                  const float4 *__restrict__ spos, const int2 *__restrict__ slot_info,
-                 const int *__restrict__ order_pos, int *__restrict__ gnbr, int *__restrict__ gnbr_count,
+                 const float4 *__restrict__ group_box, int *__restrict__ gnbr, int *__restrict__ gnbr_count,
                  int *__restrict__ gfirst, int *__restrict__ gsize, int *__restrict__ required,
                  float4 *__restrict__ origin, int n_groups, const int *__restrict__ only) {
   constexpr int G = GROUP_ATOMS;
   __shared__ int row_count;
+  __shared__ int survivors[GROUP_ROW_WARPS][32];
   const int warp = blockIdx.x;  // the group slot (every exit before the barriers is the block's)
   const int wib = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
@@ -696,44 +715,70 @@ __global__ void __launch_bounds__(32 * GROUP_ROW_WARPS)
           }
           const float slo[3] = {blo[0] - S.x, blo[1] - S.y, blo[2] - S.z};
           const float shi[3] = {bhi[0] - S.x, bhi[1] - S.y, bhi[2] - S.z};
-          for (int b = begin; b < end; b += 32) {
-            const int g = b + lane;
-            bool keep = g < end;
-            unsigned mask = 0;
-            if (keep) {
-              const float4 pj = spos[g];
-              const float c[3] = {pj.x, pj.y, pj.z};
+          // the cell's groups, 32 at a time: a group before this one (its pairs with this group
+          // are in its own row) or whose box is beyond the list cutoff of this group's box is
+          // dropped whole; the atoms of the others are tested one by one, 8 groups at a time
+          const int gs0 = s.group_base + gstart[cell], gs1 = s.group_base + gstart[cell + 1];
+          for (int gb = max(gs0, warp); gb < gs1; gb += 32) {
+            const int gq = gb + lane;
+            bool near = gq < gs1;
+            if (near) {
+              const float4 lo2 = group_box[2 * gq], hi2 = group_box[2 * gq + 1];
+              const float l2[3] = {lo2.x, lo2.y, lo2.z}, h2[3] = {hi2.x, hi2.y, hi2.z};
               float d2 = 0.f;
 #pragma unroll
               for (int d = 0; d < 3; ++d) {
-                const float e = fmaxf(fmaxf(slo[d] - c[d], c[d] - shi[d]), 0.f);
+                const float e = fmaxf(fmaxf(slo[d] - h2[d], l2[d] - shi[d]), 0.f);
                 d2 = fmaf(e, e, d2);
               }
-              keep = d2 <= cull2;
+              near = d2 <= cull2;
             }
-            if (keep) {
-              const int opos = order_pos[g];
-              if (opos < o0) {
-                keep = false;  // an earlier group of this cell lists the pair
-              } else {
-                if (opos < o0 + G) mask = 0xFu & ~((1u << (opos - o0)) - 1u);  // own atom: earlier atoms only
-                const int j = slot_info[g].y;
+            const unsigned near_mask = __ballot_sync(0xffffffffu, near);
+            if (near) survivors[wib][__popc(near_mask & ((1u << lane) - 1u))] = gq;
+            __syncwarp();
+            const int n_near = __popc(near_mask);
+            for (int t0 = 0; t0 < n_near; t0 += 8) {
+              const int t = t0 + (lane >> 2);
+              bool keep = t < n_near;
+              unsigned mask = 0;
+              int g = 0;
+              if (keep) {
+                const int opos = begin + (survivors[wib][t] - gs0) * G + (lane & 3);
+                keep = opos < end;
+                if (keep) {
+                  g = group_order[opos];
+                  const float4 pj = spos[g];
+                  const float c[3] = {pj.x, pj.y, pj.z};
+                  float d2 = 0.f;
 #pragma unroll
-                for (int t = 0; t < G; ++t)
-                  if (j >= atom_lo[t] && j <= atom_hi[t] && is_excluded(excl_start, excl_partners, atom_i[t], j))
-                    mask |= 1u << t;
-                mask |= absent;
-                keep = mask != 0xFu;
+                  for (int d = 0; d < 3; ++d) {
+                    const float e = fmaxf(fmaxf(slo[d] - c[d], c[d] - shi[d]), 0.f);
+                    d2 = fmaf(e, e, d2);
+                  }
+                  keep = d2 <= cull2;
+                }
+                if (keep) {
+                  // a later group's atom, or one of this group's own: earlier atoms only
+                  if (opos < o0 + G) mask = 0xFu & ~((1u << (opos - o0)) - 1u);
+                  const int j = slot_info[g].y;
+#pragma unroll
+                  for (int u = 0; u < G; ++u)
+                    if (j >= atom_lo[u] && j <= atom_hi[u] && is_excluded(excl_start, excl_partners, atom_i[u], j))
+                      mask |= 1u << u;
+                  mask |= absent;
+                  keep = mask != 0xFu;
+                }
+              }
+              const unsigned hits = __ballot_sync(0xffffffffu, keep);
+              if (hits) {
+                int at = 0;
+                if (lane == 0) at = atomicAdd(&row_count, __popc(hits));
+                at = __shfl_sync(0xffffffffu, at, 0) + __popc(hits & ((1u << lane) - 1u));
+                if (keep && at < cap)
+                  row[at] = (int)((unsigned)g | ((unsigned)code << GROUP_CODE_SHIFT) | (mask << GROUP_MASK_SHIFT));
               }
             }
-            const unsigned hits = __ballot_sync(0xffffffffu, keep);
-            if (hits) {
-              int at = 0;
-              if (lane == 0) at = atomicAdd(&row_count, __popc(hits));
-              at = __shfl_sync(0xffffffffu, at, 0) + __popc(hits & ((1u << lane) - 1u));
-              if (keep && at < cap)
-                row[at] = (int)((unsigned)g | ((unsigned)code << GROUP_CODE_SHIFT) | (mask << GROUP_MASK_SHIFT));
-            }
+            __syncwarp();
           }
         }
       }
@@ -820,15 +865,16 @@ void launch_rebuild(const LaunchCtx &ctx, cudaStream_t stream) {
   k_cells_scatter<<<(n + tb - 1) / tb, tb, 0, stream>>>(ctx.sys_of_atom, ctx.sys, ctx.cell_of_atom,
                                                          ctx.cell_start, ctx.cell_count,
                                                          ctx.cell_atoms, n, only);
-  LaunchCtxView v{ctx.posq, ctx.atom_type, ctx.spos, ctx.wrap, ctx.sorted_orig, ctx.sorted_type, ctx.rank,
-                  ctx.group_order, ctx.slot_info, ctx.order_pos};
+  LaunchCtxView v{ctx.posq,      ctx.atom_type, ctx.spos,      ctx.wrap,      ctx.sorted_orig,
+                  ctx.sorted_type, ctx.rank,   ctx.group_order, ctx.slot_info, ctx.order_pos,
+                  ctx.pair_list != 1 ? ctx.group_box : nullptr, ctx.cell_gstart};
   k_cells_sort<<<ctx.n_cells_total, 128, 0, stream>>>(ctx.cell_sys, ctx.sys, ctx.cell_start,
                                                       ctx.cell_count, ctx.cell_atoms, v, only);
   const int blocks = (ctx.n_groups_total + NBR_WARPS - 1) / NBR_WARPS;
   if (ctx.pair_list != 1) {  // group-pair rows (the cell scan counted 4-atom groups)
     k_group_rows<<<ctx.n_groups_total, 32 * GROUP_ROW_WARPS, 0, stream>>>(
         ctx.posq, ctx.group_sys, ctx.sys, ctx.cell_start, ctx.cell_gstart, ctx.group_order, ctx.excl_start,
-        ctx.excl_partners, ctx.spos, ctx.slot_info, ctx.order_pos, ctx.gnbr, ctx.gnbr_count, ctx.gfirst, ctx.gsize,
+        ctx.excl_partners, ctx.spos, ctx.slot_info, ctx.group_box, ctx.gnbr, ctx.gnbr_count, ctx.gfirst, ctx.gsize,
         ctx.required + ctx.n_systems, ctx.origin, ctx.n_groups_total, only);
     if (ctx.pair_list != 2) return;
   }

@@ -257,7 +257,7 @@ __device__ __forceinline__ long long warp_sum_sixteen(long long (&v)[16], int la
 }
 
 template <bool ENERGY>
-__global__ void __launch_bounds__(128) k_group_pairs(
+__global__ void __launch_bounds__(128, ENERGY ? 4 : 6) k_group_pairs(
     const float4 *__restrict__ posq, const float4 *__restrict__ spos, const int2 *__restrict__ slot_info,
     const int *__restrict__ group_order, const int *__restrict__ group_sys, const DevSys *__restrict__ sys,
     const float2 *__restrict__ lj, const int *__restrict__ gnbr, const int *__restrict__ gnbr_count,
@@ -279,18 +279,23 @@ __global__ void __launch_bounds__(128) k_group_pairs(
   if (size == 0) return;  // an unused slot (the whole warp leaves)
   const DevSys &s = sys[group_sys[warp]];
   const float2 *ljtab = (lj_in_smem ? lj_shared : lj) + s.lj_base;
-  // the group's atoms, the same in every lane (an absent atom is masked by every entry)
-  float4 pa[G];
-  int ta[G], ia[G];
+  // the group's atoms, the same for every lane (an absent atom is masked by every entry): their
+  // records in this warp's shared memory, their original indices in registers
+  __shared__ float4 group_pos[4][G];
+  __shared__ int group_lj[4][G];
+  const int wib = threadIdx.x >> 5;
   const int first = gfirst[warp];
+  int ia[G];
 #pragma unroll
   for (int a = 0; a < G; ++a) {
     const int si = group_order[first + (a < size ? a : 0)];
-    const int2 info = slot_info[si];
-    pa[a] = spos[si];
-    ta[a] = info.x * s.type_count;
-    ia[a] = info.y;
+    ia[a] = slot_info[si].y;
+    if (lane == a) {
+      group_pos[wib][a] = spos[si];
+      group_lj[wib][a] = slot_info[si].x * s.type_count;
+    }
   }
+  __syncwarp();
   const float alpha = s.alpha;
   const float gauss_k = 2.0f * alpha * 0.5641895835477563f;  // 2a/sqrt(pi)
   const float cut2 = s.cutoff2;
@@ -325,7 +330,8 @@ __global__ void __launch_bounds__(128) k_group_pairs(
     // is evaluated at r = 1 nm and contributes zero), so their chains can interleave.
 #pragma unroll
     for (int a = 0; a < G; ++a) {
-      const float3 d = make_float3(pa[a].x - pj.x - S.x, pa[a].y - pj.y - S.y, pa[a].z - pj.z - S.z);
+      const float4 pw = group_pos[wib][a];
+      const float3 d = make_float3(pw.x - pj.x - S.x, pw.y - pj.y - S.y, pw.z - pj.z - S.z);
       const float r2d = fmaf(d.x, d.x, fmaf(d.y, d.y, d.z * d.z));
       const bool in = !((e >> (GROUP_MASK_SHIFT + a)) & 1u) && r2d <= cut2;
       const float r2 = in ? r2d : 1.0f;
@@ -333,10 +339,10 @@ __global__ void __launch_bounds__(128) k_group_pairs(
         const float inv_r = rsqrt_refined(r2);
         const float inv_r2 = inv_r * inv_r;
         const float inv_r6 = inv_r2 * inv_r2 * inv_r2;
-        const float2 ab = ljtab[ta[a] + info_j.x];
+        const float2 ab = ljtab[group_lj[wib][a] + info_j.x];
         const float a12 = ab.x * inv_r6 * inv_r6, b6 = ab.y * inv_r6;
         float scalar = (12.0f * a12 - 6.0f * b6) * inv_r2;
-        const float qq = (float)ONE_4PI_EPS0 * (pa[a].w * pj.w);
+        const float qq = (float)ONE_4PI_EPS0 * (pw.w * pj.w);
         const float r = r2 * inv_r;
         float gauss;
         const float screened = erfc_and_gauss(alpha * r, gauss);

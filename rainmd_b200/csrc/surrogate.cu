@@ -11,23 +11,24 @@
 //   a1(x -> y) = min(1, exp(-w*(x -> y) / kT))
 // and only a passed move gets the exact evaluation; stage 2 accepts it with probability
 //   a2 = min(1, exp(-w / kT) a1(y -> x) / a1(x -> y)),
-// where a1(y -> x) is the surrogate's weight of the reverse move (from V' back to V). For
-// any surrogate this kernel satisfies detailed balance with respect to the exact NPT
-// distribution, so the surrogate's errors cost acceptance, never correctness. Everything
-// the surrogate reads besides the two volumes (kinetic energy, dU/dlnV of the current state,
-// the last four exact energy changes, the network's weights) is fixed before the move and
-// used for both directions, and training happens only after the decision.
+// where a1(y -> x) is the stage-1 probability of the reverse move (from V' back to V) as the
+// chain would compute it at y. For any surrogate this satisfies detailed balance with respect
+// to the exact NPT distribution, so the surrogate's errors cost acceptance, never correctness.
 //
-// The surrogate is an approximate target density pi*(V') ~ exp(-(F(V') + P V')/kT) V'^N_mol
-// around the current state V (Christen and Fox's formulation), so the reverse move's surrogate
-// weight is exactly minus the forward one and stage 2 reduces to min(1, exp(-(w - w*)/kT)):
-//   F(V') - F(V) = dUdlnV(V) ln(V'/V) + kT sqrt(N_mol) g ln(V'/V)-gated MLP(inputs),
+// The surrogate is an approximate target density pi*_x(V') ~ exp(-(F_x(V') + P V')/kT) V'^N_mol
+// built around the current state x (Christen and Fox's state-dependent approximation):
+//   F_x(V') - F_x(V) = dUdlnV(x) ln(V'/V) + kT sqrt(N_mol) g ln(V'/V)-gated MLP(inputs(x)),
 // the first-order term from the virial of the current state (reduce.cu: every term's atomic
 // virial, the reciprocal-space sum and the molecular correction) plus a learned correction
 // that vanishes at V' = V (the network's output is multiplied by input 0). Inputs (8):
 // 100 ln(V'/V), 10 ln(V/V_ref), the kinetic energy over its equipartition value minus 1,
 // dU/dlnV over N_mol kT, and the last four exact energy changes over kT sqrt(N_mol); all but
-// the first are fixed by the current state and history. Two tanh layers of 64, one linear
+// the first are fixed by the current state and history. Because the approximation depends on
+// the state it is built around, a1(y -> x) is not minus the forward weight: it is evaluated
+// around the trial state y after the exact evaluation there (k_surrogate_reverse: the
+// volume and dU/dlnV of y; the kinetic energy, which a volume move does not change, the
+// history and the weights, which only change after the decision, as for the forward move).
+// Two tanh layers of 64, one linear
 // output. BF16 weights (FP32 biases) with FP32 accumulation in every forward pass; FP32 master
 // weights trained by Adam on minibatches of 64 drawn from a per-system replay buffer of
 // (inputs, target) pairs that every exact evaluation appends to. Moves before `warm-up` exact
@@ -298,7 +299,7 @@ __global__ void __launch_bounds__(TPB) k_surrogate_stage1(BaroArgs a, SurrogateA
     const double du = dudlnv * dlnv + kT * root * (double)w.y[0];
     const double wf = du + b[B_PRESSURE] * dv - b[B_NMOL] * kT * log(nv / volume);
     b[B_PRED] = wf;
-    b[B_PRED_REV] = -wf;  // the same surrogate target seen from V': exactly antisymmetric
+    b[B_PRED_REV] = -wf;  // replaced by k_surrogate_reverse once the trial state has been evaluated
     const bool screening = b[B_REPLAY_N] >= b[B_WARMUP];
     b[B_SCREENING] = screening ? 1.0 : 0.0;
     if (screening) {
@@ -315,6 +316,44 @@ __global__ void __launch_bounds__(TPB) k_surrogate_stage1(BaroArgs a, SurrogateA
     }
   }
 }
+
+// --------------------------------------------------------------------- reverse move
+// One block per system whose move passed stage 1 while screening: the surrogate's weight of
+// the reverse move V' -> V around the trial state y, whose energies (dU/dlnV at V') the trial
+// evaluation has just reduced; the move's box has not been restored yet (the decision follows).
+__global__ void __launch_bounds__(TPB) k_surrogate_reverse(BaroArgs a, SurrogateArgs m) {
+  extern __shared__ float smem[];
+  const int s = blockIdx.x;
+  double *b = a.baro + (long long)s * N_BARO;
+  if (b[B_ACTIVE] == 0.0 || b[B_LEARNED] == 0.0 || b[B_SCREENING] == 0.0 || b[B_REFUSED] != 0.0 ||
+      b[B_SCREENED] != 0.0)
+    return;
+  const Work w = carve(smem);
+  if (threadIdx.x == 0) {
+    const double kT = b[B_KT], nmol = fmax(b[B_NMOL], 1.0);
+    const double dlnv = b[B_FEATURE0 + 10];  // ln(V'/V) of the forward move
+    const double v_trial = a.sysd[s].volume;
+    const double dudlnv = a.energies[s * N_ENERGY + E_DUDLNV];
+    float *x = w.x;
+    x[0] = (float)(-100.0 * dlnv);
+    x[1] = (float)(10.0 * log(v_trial / b[B_VOL_REF]));
+    x[2] = (float)b[B_FEATURE0 + 2];
+    x[3] = (float)(dudlnv / (nmol * kT));
+    for (int h = 0; h < 4; ++h) x[4 + h] = (float)b[B_FEATURE0 + 4 + h];
+  }
+  __syncthreads();
+  load_network(w, m.master + (long long)s * MLP_STRIDE, m.wbf + (long long)s * MLP_STRIDE);
+  forward(w, 1);
+  if (threadIdx.x == 0) {
+    const double kT = b[B_KT], nmol = fmax(b[B_NMOL], 1.0), root = sqrt(nmol);
+    const double dlnv = b[B_FEATURE0 + 10];
+    const double dudlnv = a.energies[s * N_ENERGY + E_DUDLNV];
+    const double du = dudlnv * (-dlnv) + kT * root * (double)w.y[0];
+    b[B_PRED_REV] = du - b[B_PRESSURE] * b[B_DV] + b[B_NMOL] * kT * dlnv;
+  }
+}
+
+void launch_surrogate_reverse(const BaroArgs &a, const SurrogateArgs &m, cudaStream_t stream);
 
 // ---------------------------------------------------------------------------- training
 // One block per system: append the pending exact sample (if any) to the replay buffer and
@@ -424,6 +463,11 @@ void set_smem_attr() {
 void launch_surrogate_stage1(const BaroArgs &a, const SurrogateArgs &m, cudaStream_t stream) {
   set_smem_attr();
   k_surrogate_stage1<<<a.n_systems, TPB, WORK_BYTES, stream>>>(a, m);
+}
+
+void launch_surrogate_reverse(const BaroArgs &a, const SurrogateArgs &m, cudaStream_t stream) {
+  set_smem_attr();
+  k_surrogate_reverse<<<a.n_systems, TPB, WORK_BYTES, stream>>>(a, m);
 }
 
 void launch_surrogate_train(const SurrogateArgs &m, cudaStream_t stream) {

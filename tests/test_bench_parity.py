@@ -235,9 +235,10 @@ def test_batch_lists_bit_exact_per_system(bench_box):
 
 def test_cell_plan_is_the_engines(bench_box):
     """The engine plans with the host code rmd_plan_system exposes: skin, cell counts, capacity,
-    alpha and grid agree with the plan and with planCellList."""
+    alpha and grid agree with the plan and with planCellList (per-atom rows, whose longest row
+    planCellList's capacity covers; a group-pair row may be longer and grow it by grownPlan)."""
     system, pos, grid = bench_box
-    options = bench_options(grid)
+    options = bench_options(grid, pairList=1)
     sim = GpuSimulation(system, options)
     sim.setState(pos)
     sim.initialise()
