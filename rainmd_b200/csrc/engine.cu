@@ -215,6 +215,11 @@ struct Engine {
   int pair_list = 1;
   DevArray<int> gnbr, gnbr_count, gfirst, gsize, order_pos;
   DevArray<float4> group_box;
+  // volume moves evaluated on the current lists (reduce.cu k_baro_centroid_scale, k_baro_allow)
+  DevArray<float4> saved_wrap, saved_origin;
+  DevArray<float> list_allow, saved_allow;
+  DevArray<int> list_rebuilt;
+  DevArray<unsigned> spread_bits;
   DevArray<int2> slot_info;
   DevArray<unsigned long long> e_acc;
   // list builds counted on the device: [0] those an IF node took, [1] all of them
@@ -306,7 +311,7 @@ struct Engine {
   // rebuild: REBUILD_NONE, REBUILD_FORCED, or REBUILD_IF_STALE (captured graphs only)
   void record_forces(int rebuild, bool energy);
   void record_conditional_rebuild(const LaunchCtx &c);
-  void record_barostat();
+  void record_barostat(bool keep_lists);
   void evaluate(bool rebuild, bool energy);
   void set_state(int s, const double *pos, const double *vel, int64_t step, int supplied);
   void initialise();
@@ -914,6 +919,16 @@ void Engine::upload_all(const std::vector<const rmd_system *> &src) {
   required_max.zero();
   stale.alloc(S);
   stale.zero();
+  saved_wrap.alloc(N);
+  saved_origin.alloc(N);
+  for (auto *a : {&list_allow, &saved_allow}) {
+    a->alloc(S);
+    a->zero();
+  }
+  list_rebuilt.alloc(S);
+  list_rebuilt.zero();
+  spread_bits.alloc(S);
+  spread_bits.zero();
   list_builds.alloc(2);
   list_builds.zero();
 
@@ -1386,6 +1401,17 @@ BaroArgs Engine::bargs() const {
   a.saved_energies = saved_energies.p;
   a.masses = masses.p;
   a.disp = disp.p;
+  a.keep_lists = 0;
+  a.wrap = wrap.p;
+  a.saved_wrap = saved_wrap.p;
+  a.origin = origin.p;
+  a.saved_origin = saved_origin.p;
+  a.spos = spos.p;
+  a.rank = rank.p;
+  a.allow = list_allow.p;
+  a.saved_allow = saved_allow.p;
+  a.rebuilt = list_rebuilt.p;
+  a.spread_bits = spread_bits.p;
   return a;
 }
 
@@ -1403,7 +1429,8 @@ void Engine::record_forces(int rebuild, bool energy) {
     CUDA_OK(cudaEventRecord(ev_join, side));
   }
   if (rebuild == REBUILD_FORCED) {
-    launch_rebuild_reset(required.p, required_max.p, disp.p, S, list_builds.p + 1, nullptr, stream);  // disp slot 0: since rebuild
+    launch_rebuild_reset(required.p, required_max.p, disp.p, list_allow.p, list_rebuilt.p, S, list_builds.p + 1,
+                         nullptr, stream);  // disp slot 0: since rebuild
     launch_rebuild(c, stream);
     recorded += 1 + rebuild_launches(c);
   } else if (rebuild == REBUILD_IF_STALE) {
@@ -1437,7 +1464,7 @@ void Engine::record_conditional_rebuild(const LaunchCtx &c) {
     throw Error(RMD_ERR_CUDA, "a conditional rebuild can only be recorded into a captured graph");
   cudaGraphConditionalHandle handle;
   CUDA_OK(cudaGraphConditionalHandleCreate(&handle, graph, 0, 0));
-  launch_rebuild_decide(handle, disp.p, sys.p, S, stale.p, list_builds.p, stream);
+  launch_rebuild_decide(handle, disp.p, list_allow.p, sys.p, S, stale.p, list_builds.p, stream);
   recorded += 1;
   CUDA_OK(cudaStreamGetCaptureInfo(stream, &status, nullptr, &graph, &deps, &ndeps));
   cudaGraphNodeParams params = {};
@@ -1452,7 +1479,8 @@ void Engine::record_conditional_rebuild(const LaunchCtx &c) {
   CUDA_OK(cudaStreamBeginCaptureToGraph(cond, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
   LaunchCtx only = c;  // the systems of the batch that have gone stale
   only.rebuild_only = stale.p;
-  launch_rebuild_reset(required.p, required_max.p, disp.p, S, list_builds.p + 1, stale.p, cond);
+  launch_rebuild_reset(required.p, required_max.p, disp.p, list_allow.p, list_rebuilt.p, S, list_builds.p + 1,
+                       stale.p, cond);
   launch_rebuild(only, cond);
   cudaGraph_t captured;
   CUDA_OK(cudaStreamEndCapture(cond, &captured));
@@ -1466,11 +1494,20 @@ void Engine::evaluate(bool rebuild, bool energy) {
   CUDA_OK(cudaGetLastError());
 }
 
-void Engine::record_barostat() {
-  const BaroArgs b = bargs();
+// A volume move. keep_lists (step graphs with lists rebuilt on demand): the trial state is
+// evaluated on the current lists when the displacement check, with the move's allowance,
+// finds them still valid (the atoms' wraps and origins are scaled with them, and restored on
+// a rejection); otherwise, and outside a graph, the trial rebuilds them.
+void Engine::record_barostat(bool keep_lists) {
+  BaroArgs b = bargs();
+  b.keep_lists = keep_lists ? 1 : 0;
   launch_baro_propose(b, stream);
   launch_baro_scale(b, stream);
-  record_forces(true, true);
+  if (keep_lists) {
+    launch_baro_allow(b, stream);
+    recorded += 1;
+  }
+  record_forces(keep_lists ? REBUILD_IF_STALE : REBUILD_FORCED, true);
   if (learned) {
     launch_surrogate_reverse(b, sargs(), stream);
     recorded += 1;
@@ -1714,7 +1751,7 @@ std::map<std::string, cudaGraphExec_t>::iterator Engine::block_graph(int n, bool
     const long long before = recorded;
     CUDA_OK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
     CUDA_OK(cudaMemsetAsync(disp.p + S, 0, sizeof(unsigned) * S, stream));  // slot 1: since block start
-    if (barostat) record_barostat();
+    if (barostat) record_barostat(on_demand);
     for (int k = 0; k < n; ++k) {
       int mode = (k == 0 ? INT_OPEN : (INT_CLOSE | INT_OPEN));
       if (k == n - 1) mode |= INT_OPEN_KINETIC;
@@ -1947,7 +1984,7 @@ void Engine::attempt_volume_change() {
   const BaroArgs b = bargs();
   const bool exact_move = learned ? surrogate_stage1() : true;
   if (exact_move) {
-    record_barostat();
+    record_barostat(false);
     if (learned) surrogate_train();
   }
   CUDA_OK(cudaGetLastError());

@@ -168,10 +168,10 @@ int rebuild_launches(const LaunchCtx &c);  // kernels launch_rebuild issues (wit
 // Rebuild on demand (lists.cu): flag the systems that have moved past half their skin since
 // their last build and set `handle` (an IF node's condition) when any has; and the reset every
 // rebuild starts with (of the flagged systems, or of all when `only` is null).
-void launch_rebuild_decide(cudaGraphConditionalHandle handle, const unsigned *disp, const DevSys *sys, int S,
-                           int *stale, unsigned long long *rebuilds, cudaStream_t stream);
-void launch_rebuild_reset(int *required, int *required_max, unsigned *disp, int S, unsigned long long *builds,
-                          const int *only, cudaStream_t stream);
+void launch_rebuild_decide(cudaGraphConditionalHandle handle, const unsigned *disp, const float *allow,
+                           const DevSys *sys, int S, int *stale, unsigned long long *rebuilds, cudaStream_t stream);
+void launch_rebuild_reset(int *required, int *required_max, unsigned *disp, float *allow, int *rebuilt, int S,
+                          unsigned long long *builds, const int *only, cudaStream_t stream);
 // group slots a system needs for a given group size (its search groups never exceed this)
 int neighbour_group_slots(int atoms, int cells, int group_atoms);
 void launch_nonbonded(const LaunchCtx &c, bool energy, int lanes, cudaStream_t stream);
@@ -237,6 +237,16 @@ struct BaroArgs {
   double *saved_energies;
   const float *masses;
   unsigned *disp;    // per system: largest squared displacement since the lists were built (f32 bits)
+  // A move evaluated on the current lists (keep_lists: the step graphs with lists rebuilt on
+  // demand): the atoms' wrap shifts and displacement origins are scaled with them (saved first),
+  // and `allow` grows by the most the move can change a pair distance by, per atom (saved
+  // first); `rebuilt` tells whether the trial evaluation rebuilt the lists anyway.
+  int keep_lists;
+  float4 *wrap, *saved_wrap, *origin, *saved_origin, *spos;
+  const int *rank;
+  float *allow, *saved_allow;
+  int *rebuilt;
+  unsigned *spread_bits;  // per system: largest distance of an atom from its molecule's centroid (f32 bits)
 };
 enum BaroSlot {
   B_ACTIVE = 0, B_PRESSURE, B_KT, B_NMOL, B_SEED, B_ATTEMPTS, B_ACCEPTED, B_WINDOW_ATT, B_WINDOW_ACC,
@@ -279,6 +289,7 @@ void surrogate_predict(const float *params, const float *x, int count, float *ou
 void surrogate_gradients(const float *params, const float *x, const float *target, int count,
                          float *grads, float *loss, cudaStream_t stream);
 void launch_baro_scale(const BaroArgs &a, cudaStream_t stream);
+void launch_baro_allow(const BaroArgs &a, cudaStream_t stream);  // keep_lists moves: grow `allow`
 void launch_baro_decide(const BaroArgs &a, cudaStream_t stream);
 void launch_baro_restore(const BaroArgs &a, cudaStream_t stream);
 void launch_scale_fixed(const BaroArgs &a, const double *scales, cudaStream_t stream);

@@ -674,7 +674,35 @@ __global__ void __launch_bounds__(32 * GROUP_ROW_WARPS)
   const int cap = s.nbr_capacity;
   int *row = gnbr + s.gnbr_base + (long long)q * cap;
   const int stencil_cells = count[0] * count[1] * count[2];
-  for (int sc = wib; sc < stencil_cells; sc += GROUP_ROW_WARPS) {
+  // the stencil's cells that need a search are dealt to the warps in turn (a cell before the
+  // group's own holds only atoms earlier in search order, whose groups list those pairs; in the
+  // shifted stencil of a rectangular box a cell beyond the list cutoff of the group's box is
+  // skipped), so the warps of a block get even shares: lane sc decides for stencil cell sc
+  // (at most 27), and the needed cells' ranks deal them out
+  bool need = false;
+  if (lane < stencil_cells) {
+    const int ox = lane / (count[1] * count[2]), oy = (lane / count[2]) % count[1], oz = lane % count[2];
+    const int rx = cc[0] + base[0] + ox, ry = cc[1] + base[1] + oy, rz = cc[2] + base[2] + oz;
+    const int cx = rx - (rx < 0 ? -1 : (rx >= counts[0] ? 1 : 0)) * counts[0];
+    const int cy = ry - (ry < 0 ? -1 : (ry >= counts[1] ? 1 : 0)) * counts[1];
+    const int cz = rz - (rz < 0 ? -1 : (rz >= counts[2] ? 1 : 0)) * counts[2];
+    need = (cx * counts[1] + cy) * counts[2] + cz >= cell0;
+    if (need && stencil_shift && rectangular) {
+      const float r[3] = {(float)rx, (float)ry, (float)rz};
+      float d2 = 0.f;
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        const float clo = r[d] * wcell[d], chi = clo + wcell[d];
+        const float e = fmaxf(fmaxf(clo - bhi[d], blo[d] - chi), 0.f);
+        d2 = fmaf(e, e, d2);
+      }
+      need = d2 <= cull2;
+    }
+  }
+  const unsigned need_mask = __ballot_sync(0xffffffffu, need);
+  const int rank = __popc(need_mask & ((1u << lane) - 1u));
+  for (unsigned mine = __ballot_sync(0xffffffffu, need && rank % GROUP_ROW_WARPS == wib); mine; mine &= mine - 1u) {
+    const int sc = __ffs(mine) - 1;
     const int ox = sc / (count[1] * count[2]), oy = (sc / count[2]) % count[1], oz = sc % count[2];
     {
       const int rx = cc[0] + base[0] + ox;
@@ -688,9 +716,6 @@ __global__ void __launch_bounds__(32 * GROUP_ROW_WARPS)
         const int wz = rz < 0 ? -1 : (rz >= counts[2] ? 1 : 0);
         const int cz = rz - wz * counts[2];
         const int cell = (cx * counts[1] + cy) * counts[2] + cz;
-        // a cell before the group's own holds only atoms earlier in search order: the groups
-        // they belong to list those pairs
-        if (cell < cell0) continue;
         const int begin = s.atom_start + cell_start[s.cell_start_base + cell];
         const int end = s.atom_start + cell_start[s.cell_start_base + cell + 1];
         // the lattice images to search this cell through: the stencil's own wrap on an axis
@@ -702,17 +727,6 @@ __global__ void __launch_bounds__(32 * GROUP_ROW_WARPS)
           const int kc = counts[2] >= 3 ? wz : image % nc - 1;
           const int code = shift_code(ka, kb, kc);
           const float4 S = s.shift[code];
-          if (stencil_shift && rectangular) {  // skip a cell whose box is beyond the list cutoff
-            const float r[3] = {(float)rx, (float)ry, (float)rz};
-            float d2 = 0.f;
-#pragma unroll
-            for (int d = 0; d < 3; ++d) {
-              const float clo = r[d] * wcell[d], chi = clo + wcell[d];
-              const float e = fmaxf(fmaxf(clo - bhi[d], blo[d] - chi), 0.f);
-              d2 = fmaf(e, e, d2);
-            }
-            if (d2 > cull2) continue;
-          }
           const float slo[3] = {blo[0] - S.x, blo[1] - S.y, blo[2] - S.z};
           const float shi[3] = {bhi[0] - S.x, bhi[1] - S.y, bhi[2] - S.z};
           // the cell's groups, 32 at a time: a group before this one (its pairs with this group
@@ -797,19 +811,24 @@ __global__ void __launch_bounds__(32 * GROUP_ROW_WARPS)
 // ---------------------------------------------------------------- rebuild on demand
 // A list built with cutoff rc + skin holds every pair that is within rc while no atom has
 // moved more than skin / 2 from where it was at the build (two atoms close by at most the sum
-// of their displacements). The integrator leaves each system's largest squared displacement
+// of their displacements). A volume move evaluated on the current lists (reduce.cu) shifts the
+// origins with the atoms and adds to `allow` the most it can change a pair distance by, per
+// atom, so the test stays a bound. The integrator leaves each system's largest squared displacement
 // since the build in disp[s]; this kernel sets the graph's IF condition so that the rebuild
 // runs exactly when some system of the batch has passed that bound (with a 0.1% margin on the
 // squared distance for the f32 skin), and counts the rebuilds. A non-finite displacement does
 // not trigger one: the host's block check reports it.
 __global__ void k_rebuild_decide(cudaGraphConditionalHandle handle, const unsigned *__restrict__ disp,
-                                 const DevSys *__restrict__ sys, int S, int *__restrict__ stale,
-                                 unsigned long long *__restrict__ rebuilds) {
+                                 const float *__restrict__ allow, const DevSys *__restrict__ sys, int S,
+                                 int *__restrict__ stale, unsigned long long *__restrict__ rebuilds) {
   int need = 0;
   for (int s = threadIdx.x; s < S; s += blockDim.x) {
     const float skin = sys[s].list_cutoff - sys[s].cutoff;
     const float limit2 = 0.25f * skin * skin * 0.999f;
-    const int mine = __uint_as_float(disp[s]) > limit2;
+    // the largest displacement since the build, plus what volume moves kept on these lists
+    // may have changed a pair distance by (counted per atom)
+    const float reach = sqrtf(__uint_as_float(disp[s])) + allow[s];
+    const int mine = !(reach * reach <= limit2);
     stale[s] = mine;
     need |= mine;
   }
@@ -825,8 +844,8 @@ __global__ void k_rebuild_decide(cudaGraphConditionalHandle handle, const unsign
 // maximum the host reads after each block (so an overflow at a rebuild inside a block is seen
 // too), then clear the requirement and the displacement since the build, and count the build.
 __global__ void k_rebuild_reset(int *__restrict__ required, int *__restrict__ required_max,
-                                unsigned *__restrict__ disp, int S, unsigned long long *__restrict__ builds,
-                                const int *__restrict__ only) {
+                                unsigned *__restrict__ disp, float *__restrict__ allow, int *__restrict__ rebuilt,
+                                int S, unsigned long long *__restrict__ builds, const int *__restrict__ only) {
   if (blockIdx.x == 0 && threadIdx.x == 0) *builds += 1;
   for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < S; s += gridDim.x * blockDim.x) {
     if (only && !only[s]) continue;
@@ -834,17 +853,19 @@ __global__ void k_rebuild_reset(int *__restrict__ required, int *__restrict__ re
     required[s] = 0;
     required[S + s] = 0;
     disp[s] = 0u;
+    allow[s] = 0.f;
+    rebuilt[s] = 1;  // (a volume move clears it, to learn whether its trial rebuilt the lists)
   }
 }
 
-void launch_rebuild_decide(cudaGraphConditionalHandle handle, const unsigned *disp, const DevSys *sys, int S,
-                           int *stale, unsigned long long *rebuilds, cudaStream_t stream) {
-  k_rebuild_decide<<<1, 256, 0, stream>>>(handle, disp, sys, S, stale, rebuilds);
+void launch_rebuild_decide(cudaGraphConditionalHandle handle, const unsigned *disp, const float *allow,
+                           const DevSys *sys, int S, int *stale, unsigned long long *rebuilds, cudaStream_t stream) {
+  k_rebuild_decide<<<1, 256, 0, stream>>>(handle, disp, allow, sys, S, stale, rebuilds);
 }
 
-void launch_rebuild_reset(int *required, int *required_max, unsigned *disp, int S, unsigned long long *builds,
-                          const int *only, cudaStream_t stream) {
-  k_rebuild_reset<<<(S + 255) / 256, 256, 0, stream>>>(required, required_max, disp, S, builds, only);
+void launch_rebuild_reset(int *required, int *required_max, unsigned *disp, float *allow, int *rebuilt, int S,
+                          unsigned long long *builds, const int *only, cudaStream_t stream) {
+  k_rebuild_reset<<<(S + 255) / 256, 256, 0, stream>>>(required, required_max, disp, allow, rebuilt, S, builds, only);
 }
 
 int neighbour_group_slots(int atoms, int cells, int group_atoms) {

@@ -221,10 +221,13 @@ __global__ void __launch_bounds__(128) k_nonbonded(
 
 // ------------------------------------------------------------------ group-pair kernel
 // The same pair physics over the group-pair rows (lists.cu k_group_rows). A row's entries are
-// dealt to the lanes of `split` warps, one partner a lane, and each lane evaluates its partner
-// against the group's GROUP_ATOMS atoms in turn (their positions, charges and LJ rows are held
-// in every lane's registers), so a pass of a warp over 32 entries evaluates 128 pairs. Each pair
-// is evaluated once, from the group that lists it. Its force is quantised to 64-bit fixed point
+// dealt to the lanes of `split` warps, one partner a lane. A lane first tests its partner's
+// squared distances to the group's GROUP_ATOMS atoms (their records are in the warp's shared
+// memory); the entries with an unmasked atom within the cutoff queue in a per-warp ring, and
+// each batch of 32 queued entries is evaluated one entry a lane, the partner against the four
+// atoms in turn, so a batch evaluates 128 pairs of which none belongs to an entry beyond the
+// cutoff of all four (about half the rows' entries). Each pair is evaluated once, from the
+// group that lists it. Its force is quantised to 64-bit fixed point
 // (as the atom-row kernel's precision form does) and added to two integer sums in the lane's
 // registers: the group atom's (one per group atom, reduced over the warp once, at the end of
 // the row) and the partner's (its negation, added to the force array with one 64-bit atomic per
@@ -256,8 +259,74 @@ __device__ __forceinline__ long long warp_sum_sixteen(long long (&v)[16], int la
   return v[0] + __shfl_xor_sync(0xffffffffu, v[0], 1);
 }
 
+// One row entry against the group's GROUP_ATOMS atoms: the four pairs are evaluated without
+// branches (a pair that is masked or beyond the cutoff is evaluated at r = 1 nm and contributes
+// zero), so their chains can interleave. Each pair force is quantised (the scale folded into
+// the scalar factor: a power of two, so the product rounds exactly as the scaled force does)
+// and added to the group atom's integer sums in `acc`; the partner gets the negated sum with
+// one 64-bit atomic per component (energies as they are).
 template <bool ENERGY>
-__global__ void __launch_bounds__(128, ENERGY ? 4 : 6) k_group_pairs(
+__device__ __forceinline__ void group_pair_entry(const unsigned e, const float4 pj, const int2 info_j,
+                                                 const float4 *__restrict__ gpos, const int *__restrict__ glj,
+                                                 const float2 *__restrict__ ljtab, const DevSys &s, float alpha,
+                                                 float gauss_k, float cut2, long long (&acc)[GROUP_ATOMS][ENERGY ? 6 : 3],
+                                                 unsigned long long *__restrict__ force,
+                                                 unsigned long long *__restrict__ e_acc, int n_atoms) {
+  const float4 S = s.shift[(e >> GROUP_CODE_SHIFT) & 31u];
+  long long jx = 0, jy = 0, jz = 0, jl = 0, jc = 0, jv = 0;
+#pragma unroll
+  for (int a = 0; a < GROUP_ATOMS; ++a) {
+    const float4 pw = gpos[a];
+    const float3 d = make_float3(pw.x - pj.x - S.x, pw.y - pj.y - S.y, pw.z - pj.z - S.z);
+    const float r2d = fmaf(d.x, d.x, fmaf(d.y, d.y, d.z * d.z));
+    const bool in = !((e >> (GROUP_MASK_SHIFT + a)) & 1u) && r2d <= cut2;
+    const float r2 = in ? r2d : 1.0f;
+    const float inv_r = rsqrt_refined(r2);
+    const float inv_r2 = inv_r * inv_r;
+    const float inv_r6 = inv_r2 * inv_r2 * inv_r2;
+    const float2 ab = ljtab[glj[a] + info_j.x];
+    const float a12 = ab.x * inv_r6 * inv_r6, b6 = ab.y * inv_r6;
+    float scalar = (12.0f * a12 - 6.0f * b6) * inv_r2;
+    const float qq = (float)ONE_4PI_EPS0 * (pw.w * pj.w);
+    const float r = r2 * inv_r;
+    float gauss;
+    const float screened = erfc_and_gauss(alpha * r, gauss);
+    scalar = fmaf(qq * fmaf(screened, inv_r, gauss_k * gauss), inv_r2, scalar);
+    scalar = in ? scalar * FORCE_SCALE_F : 0.0f;
+    const long long fx = __float2ll_rn(scalar * d.x);
+    const long long fy = __float2ll_rn(scalar * d.y);
+    const long long fz = __float2ll_rn(scalar * d.z);
+    acc[a][0] += fx;
+    acc[a][1] += fy;
+    acc[a][2] += fz;
+    jx += fx;
+    jy += fy;
+    jz += fz;
+    if (ENERGY) {
+      const long long el = in ? (long long)to_fixed(a12 - b6) : 0;
+      const long long ec = in ? (long long)to_fixed(qq * screened * inv_r) : 0;
+      const long long ev = __float2ll_rn(scalar * r2);
+      acc[a][ENERGY ? 3 : 0] += el;
+      acc[a][ENERGY ? 4 : 0] += ec;
+      acc[a][ENERGY ? 5 : 0] += ev;
+      jl += el;
+      jc += ec;
+      jv += ev;
+    }
+  }
+  const int j = info_j.y;
+  if (jx != 0) atomicAdd(force + j, (unsigned long long)(-jx));
+  if (jy != 0) atomicAdd(force + n_atoms + j, (unsigned long long)(-jy));
+  if (jz != 0) atomicAdd(force + 2 * (long long)n_atoms + j, (unsigned long long)(-jz));
+  if (ENERGY) {
+    if (jl != 0) atomicAdd(e_acc + j, (unsigned long long)jl);
+    if (jc != 0) atomicAdd(e_acc + n_atoms + j, (unsigned long long)jc);
+    if (jv != 0) atomicAdd(e_acc + 2 * (long long)n_atoms + j, (unsigned long long)jv);
+  }
+}
+
+template <bool ENERGY>
+__global__ void __launch_bounds__(128, ENERGY ? 4 : 5) k_group_pairs(
     const float4 *__restrict__ posq, const float4 *__restrict__ spos, const int2 *__restrict__ slot_info,
     const int *__restrict__ group_order, const int *__restrict__ group_sys, const DevSys *__restrict__ sys,
     const float2 *__restrict__ lj, const int *__restrict__ gnbr, const int *__restrict__ gnbr_count,
@@ -309,81 +378,29 @@ __global__ void __launch_bounds__(128, ENERGY ? 4 : 6) k_group_pairs(
     for (int c = 0; c < (ENERGY ? 6 : 3); ++c) acc[a][c] = 0;
   const int stride = 32 * split;
   int k = 32 * part + lane;
-  // software pipeline: the next pass's entry and partner record are loaded while this pass's
-  // pairs are computed
-  unsigned e1 = k < count ? (unsigned)__ldg(row + k) : (0xFu << GROUP_MASK_SHIFT);
+  // Each pass first tests its 32 entries with the four squared distances alone; an entry with
+  // some unmasked group atom within the cutoff joins this warp's ring in shared memory (about
+  // half of them: the rows hold every partner within the list cutoff of the group's box), and
+  // whenever 32 are queued the warp evaluates them, one entry a lane, so the full pair
+  // arithmetic runs on entries that contribute. The queued entries keep their records, so
+  // the evaluation reads them from shared memory.
+  __shared__ unsigned ring_e[4][64];
+  __shared__ float4 ring_p[4][64];
+  __shared__ int2 ring_i[4][64];
+  int head = 0, queued = 0;
+  // software pipeline, two deep: the entries of the pass after next and the partner records of
+  // the next pass are loaded while this pass's entries are tested, so no load waits on one
+  // issued in the same pass
+  constexpr unsigned NO_ENTRY = 0xFu << GROUP_MASK_SHIFT;
+  unsigned e1 = k < count ? (unsigned)__ldg(row + k) : NO_ENTRY;
+  unsigned e2 = k + stride < count ? (unsigned)__ldg(row + k + stride) : NO_ENTRY;
   float4 pj1 = __ldg(spos + (e1 & GROUP_SLOT_MASK));
   int2 info1 = __ldg(slot_info + (e1 & GROUP_SLOT_MASK));
   float4 S1 = s.shift[(e1 >> GROUP_CODE_SHIFT) & 31u];
-  for (int k0 = 32 * part; k0 < count; k0 += stride, k += stride) {
-    const unsigned e = e1;
-    const float4 pj = pj1, S = S1;
-    const int2 info_j = info1;
-    if (k0 + stride < count) {
-      e1 = k + stride < count ? (unsigned)__ldg(row + k + stride) : (0xFu << GROUP_MASK_SHIFT);
-      pj1 = __ldg(spos + (e1 & GROUP_SLOT_MASK));
-      info1 = __ldg(slot_info + (e1 & GROUP_SLOT_MASK));
-      S1 = s.shift[(e1 >> GROUP_CODE_SHIFT) & 31u];
-    }
-    long long jx = 0, jy = 0, jz = 0, jl = 0, jc = 0, jv = 0;
-    // The four pairs are evaluated without branches (a pair that is masked or beyond the cutoff
-    // is evaluated at r = 1 nm and contributes zero), so their chains can interleave.
-#pragma unroll
-    for (int a = 0; a < G; ++a) {
-      const float4 pw = group_pos[wib][a];
-      const float3 d = make_float3(pw.x - pj.x - S.x, pw.y - pj.y - S.y, pw.z - pj.z - S.z);
-      const float r2d = fmaf(d.x, d.x, fmaf(d.y, d.y, d.z * d.z));
-      const bool in = !((e >> (GROUP_MASK_SHIFT + a)) & 1u) && r2d <= cut2;
-      const float r2 = in ? r2d : 1.0f;
-      {
-        const float inv_r = rsqrt_refined(r2);
-        const float inv_r2 = inv_r * inv_r;
-        const float inv_r6 = inv_r2 * inv_r2 * inv_r2;
-        const float2 ab = ljtab[group_lj[wib][a] + info_j.x];
-        const float a12 = ab.x * inv_r6 * inv_r6, b6 = ab.y * inv_r6;
-        float scalar = (12.0f * a12 - 6.0f * b6) * inv_r2;
-        const float qq = (float)ONE_4PI_EPS0 * (pw.w * pj.w);
-        const float r = r2 * inv_r;
-        float gauss;
-        const float screened = erfc_and_gauss(alpha * r, gauss);
-        scalar = fmaf(qq * fmaf(screened, inv_r, gauss_k * gauss), inv_r2, scalar);
-        scalar = in ? scalar : 0.0f;
-        const long long fx = (long long)to_fixed(scalar * d.x);
-        const long long fy = (long long)to_fixed(scalar * d.y);
-        const long long fz = (long long)to_fixed(scalar * d.z);
-        acc[a][0] += fx;
-        acc[a][1] += fy;
-        acc[a][2] += fz;
-        jx += fx;
-        jy += fy;
-        jz += fz;
-        if (ENERGY) {
-          const long long el = in ? (long long)to_fixed(a12 - b6) : 0;
-          const long long ec = in ? (long long)to_fixed(qq * screened * inv_r) : 0;
-          const long long ev = (long long)to_fixed(scalar * r2);
-          acc[a][ENERGY ? 3 : 0] += el;
-          acc[a][ENERGY ? 4 : 0] += ec;
-          acc[a][ENERGY ? 5 : 0] += ev;
-          jl += el;
-          jc += ec;
-          jv += ev;
-        }
-      }
-    }
-    // the partner's share: the negated pair forces (the energies as they are)
-    const int j = info_j.y;
-    if (jx != 0) atomicAdd(force + j, (unsigned long long)(-jx));
-    if (jy != 0) atomicAdd(force + n_atoms + j, (unsigned long long)(-jy));
-    if (jz != 0) atomicAdd(force + 2 * (long long)n_atoms + j, (unsigned long long)(-jz));
-    if (ENERGY) {
-      if (jl != 0) atomicAdd(e_acc + j, (unsigned long long)jl);
-      if (jc != 0) atomicAdd(e_acc + n_atoms + j, (unsigned long long)jc);
-      if (jv != 0) atomicAdd(e_acc + 2 * (long long)n_atoms + j, (unsigned long long)jv);
-    }
-  }
   // Exceptions of the group atoms (first warp of the row: lanes 8a .. 8a + 7 for atom a): 1-4
   // scaled LJ/Coulomb and -q_i q_j erf(a r)/r, no cutoff, exactly as the atom-row kernel
-  // evaluates them.
+  // evaluates them. They come before the row walk, so their chain of dependent loads overlaps
+  // the walk's first loads instead of following its last pass.
   {
     const int a = lane >> 3, t = lane & 7;
     const bool vi = a < size && part == 0;
@@ -446,6 +463,52 @@ __global__ void __launch_bounds__(128, ENERGY ? 4 : 6) k_group_pairs(
         }
       }
     }
+  }
+  for (int k0 = 32 * part; k0 < count; k0 += stride, k += stride) {
+    const unsigned e = e1;
+    const float4 pj = pj1, S = S1;
+    const int2 info_j = info1;
+    if (k0 + stride < count) {
+      e1 = e2;
+      pj1 = __ldg(spos + (e1 & GROUP_SLOT_MASK));
+      info1 = __ldg(slot_info + (e1 & GROUP_SLOT_MASK));
+      S1 = s.shift[(e1 >> GROUP_CODE_SHIFT) & 31u];
+      e2 = k + 2 * stride < count ? (unsigned)__ldg(row + k + 2 * stride) : NO_ENTRY;
+    }
+    bool any = false;
+#pragma unroll
+    for (int a = 0; a < G; ++a) {
+      const float4 pw = group_pos[wib][a];
+      const float3 d = make_float3(pw.x - pj.x - S.x, pw.y - pj.y - S.y, pw.z - pj.z - S.z);
+      const float r2 = fmaf(d.x, d.x, fmaf(d.y, d.y, d.z * d.z));
+      any |= !((e >> (GROUP_MASK_SHIFT + a)) & 1u) && r2 <= cut2;
+    }
+    const unsigned hits = __ballot_sync(0xffffffffu, any);
+    if (any) {
+      const int slot = (head + queued + __popc(hits & ((1u << lane) - 1u))) & 63;
+      ring_e[wib][slot] = e;
+      ring_p[wib][slot] = pj;
+      ring_i[wib][slot] = info_j;
+    }
+    queued += __popc(hits);
+    if (queued >= 32) {
+      __syncwarp();
+      const int slot = (head + lane) & 63;
+      group_pair_entry<ENERGY>(ring_e[wib][slot], ring_p[wib][slot], ring_i[wib][slot], group_pos[wib],
+                               group_lj[wib], ljtab, s, alpha, gauss_k, cut2, acc, force, e_acc, n_atoms);
+      __syncwarp();  // every lane has read its slot before the next pass refills the ring
+      head = (head + 32) & 63;
+      queued -= 32;
+    }
+  }
+  if (queued > 0) {  // the last, partial batch
+    __syncwarp();
+    const int slot = (head + lane) & 63;
+    const bool mine = lane < queued;
+    group_pair_entry<ENERGY>(mine ? ring_e[wib][slot] : NO_ENTRY,
+                             mine ? ring_p[wib][slot] : make_float4(0.f, 0.f, 0.f, 0.f),
+                             mine ? ring_i[wib][slot] : make_int2(0, 0), group_pos[wib], group_lj[wib], ljtab, s,
+                             alpha, gauss_k, cut2, acc, force, e_acc, n_atoms);
   }
   // the group atoms' sums over the warp: value 4a + c (component c of atom a) ends in lanes
   // 2(4a + c) and 2(4a + c) + 1; the lane with the even index adds it to the atom

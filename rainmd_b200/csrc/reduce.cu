@@ -142,6 +142,10 @@ __global__ void k_baro_propose(BaroArgs a) {
     b[B_LSCALE] = 1.0;
   }
   if (b[B_ACTIVE] == 0.0) return;
+  if (a.keep_lists) {
+    a.rebuilt[s] = 0;
+    a.saved_allow[s] = a.allow[s];
+  }
   DevSysD &d = a.sysd[s];
   const double volume = d.volume;
   for (int k = 0; k < N_ENERGY; ++k) a.saved_energies[s * N_ENERGY + k] = a.energies[s * N_ENERGY + k];
@@ -193,13 +197,19 @@ __global__ void k_baro_centroid_scale(BaroArgs a, int n_molecules, const double 
   const int begin = a.mol_start[m], end = a.mol_start[m + 1];
   const int s = a.sys_of_atom[a.mol_atoms[begin]];
   const double ls = fixed_scales ? fixed_scales[s] : a.baro[(long long)s * N_BARO + B_LSCALE];
-  // Save positions and forces of this molecule's atoms (restored if the move is rejected).
+  // Save positions and forces of this molecule's atoms (restored if the move is rejected), and
+  // for a move on the current lists their wrap shifts and displacement origins.
+  const bool keep = a.keep_lists && !fixed_scales;
   for (int k = begin + lane; k < end; k += 32) {
     const int i = a.mol_atoms[k];
     a.saved_posq[i] = a.posq[i];
     a.saved_force[i] = a.force[i];
     a.saved_force[a.n_atoms + i] = a.force[a.n_atoms + i];
     a.saved_force[2 * (long long)a.n_atoms + i] = a.force[2 * (long long)a.n_atoms + i];
+    if (keep) {
+      a.saved_wrap[i] = a.wrap[i];
+      a.saved_origin[i] = a.origin[i];
+    }
   }
   if (ls == 1.0) return;
   double cx = 0, cy = 0, cz = 0, mt = 0;
@@ -233,14 +243,52 @@ __global__ void k_baro_centroid_scale(BaroArgs a, int n_molecules, const double 
   cy /= mt;
   cz /= mt;
   const double f = ls - 1.0;
+  float spread = 0.f;  // the molecule's largest atom-centroid distance
   for (int k = begin + lane; k < end; k += 32) {
     const int i = a.mol_atoms[k];
     float4 p = a.posq[i];
+    if (keep) {
+      const double ex = (double)p.x - cx, ey = (double)p.y - cy, ez = (double)p.z - cz;
+      spread = fmaxf(spread, (float)sqrt(ex * ex + ey * ey + ez * ez));
+    }
     p.x = (float)((double)p.x + f * cx);
     p.y = (float)((double)p.y + f * cy);
     p.z = (float)((double)p.z + f * cz);
     a.posq[i] = p;
+    if (keep) {
+      // The lists keep describing the scaled state: the wrap shift is the same whole number of
+      // box vectors in the scaled box, the displacement origin moves with the atom (so the
+      // check keeps measuring the motion since the build; what the scaling does to a pair
+      // distance is counted in `allow`), and the cell-ordered copy follows.
+      const float4 w = a.wrap[i], o = a.origin[i];
+      const float4 ws = make_float4((float)((double)w.x * ls), (float)((double)w.y * ls), (float)((double)w.z * ls), 0.f);
+      a.wrap[i] = ws;
+      a.origin[i] = make_float4((float)((double)o.x + f * cx), (float)((double)o.y + f * cy),
+                                (float)((double)o.z + f * cz), o.w);
+      a.spos[a.rank[i]] = make_float4(p.x - ws.x, p.y - ws.y, p.z - ws.z, p.w);
+    }
   }
+  if (keep) {
+    spread = warp_max(spread);
+    if (lane == 0) atomic_max_nonneg(&a.spread_bits[s], spread);
+  }
+}
+
+// One thread per system moving on its current lists: the move changes a pair's vector by
+// (s - 1)(d + c_i - x_i - c_j + x_j) (d the vector before the move, c the molecules'
+// centroids), at most |s - 1| (r_list + 2 spread) for a pair within the list cutoff: half of
+// that per atom is added to the rebuild decision's allowance.
+__global__ void k_baro_allow(BaroArgs a) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= a.n_systems) return;
+  const double *b = a.baro + (long long)s * N_BARO;
+  const float spread = __uint_as_float(a.spread_bits[s]);
+  a.spread_bits[s] = 0u;
+  if (b[B_ACTIVE] == 0.0 || b[B_REFUSED] != 0.0 || b[B_SCREENED] != 0.0) return;
+  const double ls = b[B_LSCALE];
+  if (ls == 1.0) return;
+  const double reach = fabs(ls - 1.0) * ((double)a.sys[s].list_cutoff + 2.0 * (double)spread);
+  a.allow[s] += (float)(0.5 * reach * 1.001);
 }
 
 // One thread per system: the Metropolis test in FP64 (metropolisWeight, barostat.js:158-162)
@@ -293,11 +341,15 @@ __global__ void k_baro_decide(BaroArgs a) {
     set_box(a.sys[s], d, ob);
     for (int k = 0; k < 3; ++k) a.sys[s].cell_counts[k] = d.saved_counts[k];
     for (int k = 0; k < N_ENERGY; ++k) a.energies[s * N_ENERGY + k] = a.saved_energies[s * N_ENERGY + k];
-    // The lists of the trial evaluation were built in the trial box, with wrap shifts that are
-    // multiples of its vectors: they do not describe the restored positions in the restored
-    // box. Mark them stale (the largest finite displacement), so that the next rebuild
-    // decision rebuilds this system before its next force evaluation.
-    a.disp[s] = 0x7f7fffffu;
+    if (!a.keep_lists || a.rebuilt[s]) {
+      // The lists of the trial evaluation were built in the trial box, with wrap shifts that
+      // are multiples of its vectors: they do not describe the restored positions in the
+      // restored box. Mark them stale (the largest finite displacement), so that the next
+      // rebuild decision rebuilds this system before its next force evaluation.
+      a.disp[s] = 0x7f7fffffu;
+    } else {
+      a.allow[s] = a.saved_allow[s];  // the lists from before the move describe the restored state
+    }
   }
   if (!learned && b[B_WINDOW_ATT] >= 10.0) {  // simulation.js:1058-1063 (stage 1 does it when learned)
     const double rate = b[B_WINDOW_ACC] / b[B_WINDOW_ATT];
@@ -313,10 +365,17 @@ __global__ void k_baro_restore(BaroArgs a) {
   if (i >= a.n_atoms) return;
   const int s = a.sys_of_atom[i];
   if (a.baro[(long long)s * N_BARO + B_ACCEPT] != 0.0) return;
-  a.posq[i] = a.saved_posq[i];
+  const float4 p = a.saved_posq[i];
+  a.posq[i] = p;
   a.force[i] = a.saved_force[i];
   a.force[a.n_atoms + i] = a.saved_force[a.n_atoms + i];
   a.force[2 * (long long)a.n_atoms + i] = a.saved_force[2 * (long long)a.n_atoms + i];
+  if (a.keep_lists && !a.rebuilt[s]) {  // the lists stand: their wraps, origins and copy as before
+    const float4 w = a.saved_wrap[i];
+    a.wrap[i] = w;
+    a.origin[i] = a.saved_origin[i];
+    a.spos[a.rank[i]] = make_float4(p.x - w.x, p.y - w.y, p.z - w.z, p.w);
+  }
 }
 
 void launch_baro_propose(const BaroArgs &a, cudaStream_t stream) {
@@ -329,6 +388,9 @@ void launch_baro_scale(const BaroArgs &a, cudaStream_t stream) {
 void launch_scale_fixed(const BaroArgs &a, const double *scales, cudaStream_t stream) {
   const int tb = 128;
   k_baro_centroid_scale<<<(a.n_molecules * 32 + tb - 1) / tb, tb, 0, stream>>>(a, a.n_molecules, scales);
+}
+void launch_baro_allow(const BaroArgs &a, cudaStream_t stream) {
+  k_baro_allow<<<(a.n_systems + 63) / 64, 64, 0, stream>>>(a);
 }
 void launch_baro_decide(const BaroArgs &a, cudaStream_t stream) {
   k_baro_decide<<<(a.n_systems + 63) / 64, 64, 0, stream>>>(a);

@@ -353,8 +353,6 @@ __global__ void __launch_bounds__(TPB) k_surrogate_reverse(BaroArgs a, Surrogate
   }
 }
 
-void launch_surrogate_reverse(const BaroArgs &a, const SurrogateArgs &m, cudaStream_t stream);
-
 // ---------------------------------------------------------------------------- training
 // One block per system: append the pending exact sample (if any) to the replay buffer and
 // the energy-change history, then take `steps` Adam steps on minibatches from the buffer.
@@ -452,6 +450,7 @@ void set_smem_attr() {
   cudaGetDevice(&dev);
   if (dev >= 0 && dev < 64 && !g_attr_set[dev]) {
     cudaFuncSetAttribute(k_surrogate_stage1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)WORK_BYTES);
+    cudaFuncSetAttribute(k_surrogate_reverse, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)WORK_BYTES);
     cudaFuncSetAttribute(k_surrogate_train, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)WORK_BYTES);
     cudaFuncSetAttribute(k_surrogate_eval, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)WORK_BYTES);
     g_attr_set[dev] = true;

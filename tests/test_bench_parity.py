@@ -399,3 +399,46 @@ def test_non_finite_state_raises():
     with pytest.raises(NonFiniteStateError):
         sim.run(20, blockSize=10)
     sim.release()
+
+
+@pytest.mark.parametrize("which", ["chain-1190", "water-23558"])
+def test_moves_inside_step_graphs_evaluate_the_trial_state(which, bench_box):
+    """Volume moves inside the step graphs are evaluated on the current lists when the
+    displacement check, with the move's allowance, still trusts them (the atoms' wraps and
+    origins scaled with them): each move's trial energy must be the oracle's potential of the
+    molecule-scaled state in the scaled box (5e-5), in a 2 x 2 x 2-cell box (every image searched)
+    and a 5^3 stencil box; an accepted move leaves the scaled box, a rejected one the old."""
+    if which == "chain-1190":
+        system, pos, grid = chain1190()
+    else:
+        system, pos, grid = bench_box
+    sim = GpuSimulation(system, bench_options(grid, seed=13, pressure=1.0, barostatInterval=25))
+    sim.setState(pos)
+    sim.initialise()
+    sim.minimise(maxIterations=30, forceTolerance=1000.0)
+    sim.run(100, blockSize=25)
+    alpha = oracle.alpha_from_tolerance(0.9, 5e-4)
+    outcomes = []
+    for _ in range(6):
+        before = sim.readState()
+        attempts = sim.diagnostics()["barostat_attempts"]
+        sim.run(25, blockSize=25)
+        assert sim.diagnostics()["barostat_attempts"] == attempts + 1
+        move = sim.lastVolumeMove()
+        after_box = np.asarray(sim.readState()["boxVectors"])
+        ls = move["length_scale"]
+        scaled_system = dict(system)
+        scaled_system["boxVectors"] = np.asarray(before["boxVectors"], dtype=np.float64) * ls
+        o = oracle.Oracle(scaled_system)
+        scaled = oracle.Oracle(system).scale_molecules(before["positions"].astype(np.float64), ls)
+        e, _ = o.potential(scaled.astype(np.float32).astype(np.float64), method="PME", alpha=alpha, grid=grid,
+                           order=4)
+        volume = float(np.prod(np.diag(np.asarray(scaled_system["boxVectors"]).reshape(3, 3))))
+        expect = e["total"] + o.dispersion(volume, 0.9)
+        assert move["new_potential"] == pytest.approx(expect, rel=5e-5), (which, move)
+        if move["accepted"]:
+            assert np.allclose(after_box, np.asarray(before["boxVectors"]) * ls, rtol=1e-15, atol=0)
+        else:
+            assert np.array_equal(after_box, np.asarray(before["boxVectors"]))
+        outcomes.append(bool(move["accepted"]))
+    sim.release()
