@@ -463,24 +463,26 @@ class ClockSampler:
 # The pair kernel's arithmetic ceiling, reported beside its memory roofline. The group-pair
 # kernel evaluates every pair within the cutoff once (the per-atom-row kernel twice, once from
 # each atom), and one evaluation of the force-only precision form issues, counted from the
-# kernels' source: 49 FP32 operations, 6 integer operations (three 64-bit fixed-point adds),
-# 3 SFU operations (rsqrt, ex2, rcp) and 3 float-to-int64 conversions. The ceiling is the larger
+# kernels' source: 49 FP32 operations (47 in the group-pair kernel, which folds the fixed-point
+# scale into the force's scalar factor once instead of scaling each component), 6 integer
+# operations (three 64-bit fixed-point adds), 3 SFU operations (rsqrt, ex2, rcp) and 3
+# float-to-int64 conversions. The ceiling is the larger
 # of the issue time (one instruction per lane per clock, 128 lanes per SM) and the
 # SFU-and-conversion time (16 lanes per SM per clock) on 148 SMs at the SM clock sampled during
 # the run. List walking, loads, out-of-cutoff entries, the partner's reduction and atomics and
 # the exception loop are not counted, so the kernel cannot reach it.
-PAIR_LANE_OPS = 49 + 6 + 3 + 3
 PAIR_XU_OPS = 3 + 3
 B200_SMS = 148
 
 
 def pair_arithmetic_ceiling(pairs, kernel_ms, sm_mhz, evaluations_per_pair=1):
     evaluations = evaluations_per_pair * int(pairs)
+    lane_ops = (47 if evaluations_per_pair == 1 else 49) + 6 + 3 + 3
     clock = float(sm_mhz) * 1e6
-    issue_s = evaluations * PAIR_LANE_OPS / (B200_SMS * 128 * clock)
+    issue_s = evaluations * lane_ops / (B200_SMS * 128 * clock)
     xu_s = evaluations * PAIR_XU_OPS / (B200_SMS * 16 * clock)
     ceiling_ms = max(issue_s, xu_s) * 1e3
-    return {"evaluations": evaluations, "lane_ops_per_evaluation": PAIR_LANE_OPS,
+    return {"evaluations": evaluations, "lane_ops_per_evaluation": lane_ops,
             "sfu_and_conversion_ops_per_evaluation": PAIR_XU_OPS, "sm_mhz": float(sm_mhz),
             "ceiling_ms": ceiling_ms, "frac": ceiling_ms / kernel_ms}
 
@@ -589,6 +591,8 @@ def prepare(system, pos, grid, seed, npt, args):
     opts = options_for(grid, seed=seed)
     if args.pair_list is not None:
         opts["pairList"] = args.pair_list
+    if args.nonbonded_lanes is not None:
+        opts["nonbondedLanes"] = args.nonbonded_lanes
     if npt:
         opts.update({"pressure": 1.0, "barostatInterval": BAROSTAT_INTERVAL})
     if args.rebuild_schedule:
@@ -699,6 +703,8 @@ def main():
     parser.add_argument("--pair-list", type=int, choices=[0, 1], default=None,
                         help="neighbour structure of the pair loop: 0 group-pair rows, 1 per-atom rows "
                              "(default: the engine's)")
+    parser.add_argument("--nonbonded-lanes", type=int, choices=[32, 64, 128], default=None,
+                        help="fix the group-pair kernel's lanes a row instead of autotuning them")
     parser.add_argument("--rebuild-schedule", action="store_true",
                         help="rebuild the lists on the reference's host schedule instead of on demand "
                              "(the same kernels; ncu profiles no kernel of a graph with conditional nodes)")
@@ -710,21 +716,18 @@ def main():
     if args.impl == "reference":
         run_reference(args, rank, world)
         return
-    if args.study == "learned-barostat":
+    if args.study is not None:
         if rank == 0:
-            print(json.dumps(learned_barostat_study(args.ps, seeds=tuple(args.seeds))), flush=True)
-        return
-    if args.study == "large-combined":
-        if rank == 0:
-            print(json.dumps(large_combined_study(args.steps)), flush=True)
-        return
-    if args.study == "trajectory":
-        if rank == 0:
-            print(json.dumps(trajectory_study()), flush=True)
-        return
-    if args.study == "render":
-        if rank == 0:
-            print(json.dumps(render_study()), flush=True)
+            studies = {"learned-barostat": lambda: learned_barostat_study(args.ps, seeds=tuple(args.seeds)),
+                       "large-combined": lambda: large_combined_study(args.steps),
+                       "trajectory": trajectory_study, "render": render_study}
+            # the clock record covers the whole study (nvidia-smi every 200 ms)
+            with ClockSampler(local) as clocks:
+                result = studies[args.study]()
+            summary = clocks.summary()
+            summary["window"] = "the whole study"
+            result["clocks"] = summary
+            print(json.dumps(result), flush=True)
         return
     # one GPU per process: make this rank's GPU device 0 before any CUDA initialisation
     if world > 1:
