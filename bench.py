@@ -92,53 +92,70 @@ def batch_workload(seed: int = 0, count: int = 64):
     return out
 
 
-def batched_block(steps: int, seed: int, single_steps: int = 200):
+def batched_block(steps: int, seed: int, single_steps: int = 200, rank: int = 0, world: int = 1,
+                  reduce_max=None):
     """Batched aggregate ns/day of the 64 uneven systems advanced together (one set of launches
     per step, CUDA-graph blocks of 100 steps): the sum over systems of each one's ns/day in the
-    batch. Beside it the plain path for the same work: the same 64 systems run one after
-    another on this GPU, each alone (aggregate = 64 x ns/day at the summed per-system step
+    batch. Beside it the plain path for the same work: the same systems run one after another
+    on the same GPU, each alone (aggregate = systems x ns/day at the summed per-system step
     time), and the ratio of the two, which is the summed single-system step time over the
-    batch's step time."""
+    batch's step time. On N GPUs the systems are partitioned whole across the ranks
+    (rainmd_b200.partition: no per-step collective); each rank advances its share as one batch,
+    and the slowest rank's step time sets both figures."""
+    from rainmd_b200.partition import partition_systems, system_cost
     from rainmd_b200.simulation import BatchSimulation, GpuSimulation
+
+    def slowest(x):
+        return reduce_max(x) if reduce_max is not None and world > 1 else x
 
     items = batch_workload(seed)
     systems = [s for s, _, _ in items]
     options = [options_for(g, seed=11 + k) for k, (_, _, g) in enumerate(items)]
     atoms = [s["topology"]["atomCount"] for s in systems]
-    batch = BatchSimulation(systems, options)
-    for k, (_, pos, _) in enumerate(items):
-        batch.setState(k, pos)
-    batch.initialise()
-    batch.minimise(maxIterations=100, forceTolerance=1000.0)
-    batch.run(500, blockSize=100)
-    batch.benchRun(100, 100, flushL2=True)
-    ms = batch.benchRun(steps, 100, flushL2=True)
-    batch_ns = len(systems) * ns_per_day(ms * 1e-3 / steps)
-    shapes = batch.kernelShapes()
-    batch.release()
-    single_ms = []
-    for k, (system, pos, _) in enumerate(items):
-        sim = GpuSimulation(system, options[k])
-        sim.setState(pos)
-        sim.initialise()
-        sim.minimise(maxIterations=100, forceTolerance=1000.0)
-        sim.run(200, blockSize=100)
-        single_ms.append(sim.benchRun(single_steps, 100, flushL2=True) / single_steps)
-        sim.release()
-    sequential_ms = float(sum(single_ms))
+    costs = [system_cost(a, float(np.prod(np.asarray(s["boxVectors"], dtype=np.float64)[[0, 4, 8]])), 0.9, g)
+             for a, s, (_, _, g) in zip(atoms, systems, items)]
+    parts = partition_systems(costs, world)
+    mine = parts[rank]
+    ms_per_step, single_ms, shapes = 0.0, [], None
+    if mine:
+        batch = BatchSimulation([systems[k] for k in mine], [options[k] for k in mine])
+        for b, k in enumerate(mine):
+            batch.setState(b, items[k][1])
+        batch.initialise()
+        batch.minimise(maxIterations=100, forceTolerance=1000.0)
+        batch.run(500, blockSize=100)
+        batch.benchRun(100, 100, flushL2=True)
+        ms_per_step = batch.benchRun(steps, 100, flushL2=True) / steps
+        shapes = batch.kernelShapes()
+        batch.release()
+        for k in mine:
+            sim = GpuSimulation(systems[k], options[k])
+            sim.setState(items[k][1])
+            sim.initialise()
+            sim.minimise(maxIterations=100, forceTolerance=1000.0)
+            sim.run(200, blockSize=100)
+            single_ms.append(sim.benchRun(single_steps, 100, flushL2=True) / single_steps)
+            sim.release()
+    batch_ms = slowest(ms_per_step)
+    sequential_ms = slowest(float(sum(single_ms)))
+    batch_ns = len(systems) * ns_per_day(batch_ms * 1e-3)
     sequential_ns = len(systems) * ns_per_day(sequential_ms * 1e-3)
-    return {"systems": len(systems), "atoms_total": int(sum(atoms)), "atoms_min": int(min(atoms)),
-            "atoms_max": int(max(atoms)), "steps": steps, "ms_per_step": ms / steps,
-            "aggregate_ns_per_day": batch_ns,
-            "sequential_single_ms_per_step_summed": sequential_ms,
-            "sequential_single_aggregate_ns_per_day": sequential_ns,
-            "ratio_vs_sequential_singles": batch_ns / sequential_ns,
-            "single_ns_per_day_min": ns_per_day(max(single_ms) * 1e-3),
-            "single_ns_per_day_max": ns_per_day(min(single_ms) * 1e-3),
-            "single_steps": single_steps,
-            "kernel_shapes": {k: shapes[k] for k in ("neighbourGroupAtoms", "nonbondedLanes",
-                                                     "spreadAtomsPerBlock")},
-            "seed": seed}
+    loads = [sum(costs[k] for k in p) for p in parts]
+    out = {"systems": len(systems), "atoms_total": int(sum(atoms)), "atoms_min": int(min(atoms)),
+           "atoms_max": int(max(atoms)), "steps": steps, "ms_per_step": batch_ms,
+           "aggregate_ns_per_day": batch_ns,
+           "sequential_single_ms_per_step_summed": sequential_ms,
+           "sequential_single_aggregate_ns_per_day": sequential_ns,
+           "ratio_vs_sequential_singles": batch_ns / sequential_ns,
+           "single_steps": single_steps, "seed": seed,
+           "partition": {"ranks": world, "systems_per_rank": [len(p) for p in parts],
+                         "cost_max_over_mean": max(loads) / (sum(loads) / world)}}
+    if world == 1:
+        out["single_ns_per_day_min"] = ns_per_day(max(single_ms) * 1e-3)
+        out["single_ns_per_day_max"] = ns_per_day(min(single_ms) * 1e-3)
+    if shapes is not None:
+        out["kernel_shapes"] = {k: shapes[k] for k in ("neighbourGroupAtoms", "nonbondedLanes", "spreadAtomsPerBlock")}
+    return out
 
 
 def blocking_se(series):
@@ -808,7 +825,8 @@ def main():
                         "list_builds_timed": builds2, "volume_moves_timed": moves2,
                         "workload": describe(args.workload, grid, not npt)}
         extra["config0"] = config0_line(args, barrier)
-    batched = None if args.no_batched else batched_block(args.batch_steps, seed=rank)
+    batched = None if args.no_batched else batched_block(args.batch_steps, seed=0, rank=rank, world=world,
+                                                          reduce_max=reduce_max)
     if rank != 0:
         if world > 1:
             dist.destroy_process_group()
