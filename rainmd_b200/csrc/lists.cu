@@ -889,7 +889,7 @@ void launch_rebuild(const LaunchCtx &ctx, cudaStream_t stream) {
   LaunchCtxView v{ctx.posq,      ctx.atom_type, ctx.spos,      ctx.wrap,      ctx.sorted_orig,
                   ctx.sorted_type, ctx.rank,   ctx.group_order, ctx.slot_info, ctx.order_pos,
                   ctx.pair_list != 1 ? ctx.group_box : nullptr, ctx.cell_gstart};
-  k_cells_sort<<<ctx.n_cells_total, 128, 0, stream>>>(ctx.cell_sys, ctx.sys, ctx.cell_start,
+  k_cells_sort<<<ctx.n_cells_total, 256, 0, stream>>>(ctx.cell_sys, ctx.sys, ctx.cell_start,
                                                       ctx.cell_count, ctx.cell_atoms, v, only);
   const int blocks = (ctx.n_groups_total + NBR_WARPS - 1) / NBR_WARPS;
   if (ctx.pair_list != 1) {  // group-pair rows (the cell scan counted 4-atom groups)

@@ -344,16 +344,16 @@ __global__ void __launch_bounds__(128, ENERGY ? 4 : 5) k_group_pairs(
   const int warp = task / split, part = task - warp * split;  // the group slot, this warp's share
   const int lane = threadIdx.x & 31;
   if (warp >= n_groups) return;
-  const int size = gsize[warp];
+  // the group's records, loaded together before the first branch on them
+  const int size = gsize[warp], sys_index = group_sys[warp], first = gfirst[warp], count = gnbr_count[warp];
   if (size == 0) return;  // an unused slot (the whole warp leaves)
-  const DevSys &s = sys[group_sys[warp]];
+  const DevSys &s = sys[sys_index];
   const float2 *ljtab = (lj_in_smem ? lj_shared : lj) + s.lj_base;
   // the group's atoms, the same for every lane (an absent atom is masked by every entry): their
   // records in this warp's shared memory, their original indices in registers
   __shared__ float4 group_pos[4][G];
   __shared__ int group_lj[4][G];
   const int wib = threadIdx.x >> 5;
-  const int first = gfirst[warp];
   int ia[G];
 #pragma unroll
   for (int a = 0; a < G; ++a) {
@@ -368,7 +368,6 @@ __global__ void __launch_bounds__(128, ENERGY ? 4 : 5) k_group_pairs(
   const float alpha = s.alpha;
   const float gauss_k = 2.0f * alpha * 0.5641895835477563f;  // 2a/sqrt(pi)
   const float cut2 = s.cutoff2;
-  const int count = gnbr_count[warp];
   const int *row = gnbr + s.gnbr_base + (long long)(warp - s.group_base) * s.nbr_capacity;
   // per group atom: force x, y, z (and energies lj, coulomb, virial) in fixed point
   long long acc[G][ENERGY ? 6 : 3];
