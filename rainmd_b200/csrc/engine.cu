@@ -460,6 +460,14 @@ void Engine::plan_system(HostSystem &h, const rmd_system &s) {
   }
 }
 
+static FastDiv make_fast_div(uint32_t d) {
+  if (d == 0 || d >= (1u << 31)) throw Error(RMD_ERR_INVALID, "divisor out of range");
+  uint32_t shift = 0;
+  while ((1ull << shift) < d) ++shift;
+  const unsigned long long magic = (((1ull << 32) * ((1ull << shift) - d)) / d) + 1;
+  return FastDiv{(uint32_t)magic, shift};
+}
+
 static void fft_axis_plan(int n, FftAxis &ax, int tw_base) {
   ax.n = n;
   ax.nstages = 0;
@@ -469,6 +477,14 @@ static void fft_axis_plan(int n, FftAxis &ax, int tw_base) {
   while (r % 2 == 0) { ax.radix[ax.nstages++] = 2; r /= 2; }
   while (r % 3 == 0) { ax.radix[ax.nstages++] = 3; r /= 3; }
   while (r % 5 == 0) { ax.radix[ax.nstages++] = 5; r /= 5; }
+  int span = 1;
+  for (int st = 0; st < ax.nstages; ++st) {
+    ax.per_line[st] = make_fast_div((uint32_t)(n / ax.radix[st]));
+    ax.span[st] = make_fast_div((uint32_t)span);
+    span *= ax.radix[st];
+  }
+  ax.n_div = make_fast_div((uint32_t)n);
+  ax.half_div = make_fast_div((uint32_t)(n / 2 + 1));
 }
 
 constexpr int FFT_SMEM_HOST = 2048;

@@ -9,11 +9,22 @@
 namespace rmd {
 
 // One FFT axis of one system: length, Stockham radices and its twiddle table offset.
+// Division by a divisor fixed per plan, without a hardware divide: for 1 <= d < 2^31 and
+// 0 <= x < 2^31, x / d = (umulhi(x, magic) + x) >> shift with shift = ceil(log2 d) and
+// magic = floor(2^32 (2^shift - d) / d) + 1 (T. Granlund and P. L. Montgomery, "Division by
+// invariant integers using multiplication", PLDI 1994; the sum cannot overflow since
+// umulhi(x, magic) < x < 2^31).
+struct FastDiv {
+  uint32_t magic, shift;
+};
 struct FftAxis {
   int n;
   int nstages;
   int radix[12];
   int tw_base;
+  FastDiv per_line[12];  // stage s: n / radix[s] butterflies a line
+  FastDiv span[12];      // stage s: the product of the earlier radices
+  FastDiv n_div, half_div;  // n and n / 2 + 1
 };
 struct FftPlan {
   FftAxis axis[3];

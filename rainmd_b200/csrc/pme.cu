@@ -81,17 +81,22 @@ __device__ __forceinline__ void dft_small(float2 *v, bool inv) {
   }
 }
 
+__device__ __forceinline__ int fast_div(int x, FastDiv f) {
+  return (int)((__umulhi((uint32_t)x, f.magic) + (uint32_t)x) >> f.shift);
+}
+
 template <int R>
 __device__ __forceinline__ void stockham_stage(const float2 *__restrict__ in, float2 *__restrict__ out,
                                                int lines, int N, int ld, int Ns, const float2 *tw,
-                                               bool inv) {
+                                               bool inv, FastDiv per_line_div, FastDiv span_div) {
   const int per_line = N / R;
   const int stride_tw = N / (Ns * R);
   for (int idx = threadIdx.x; idx < lines * per_line; idx += blockDim.x) {
-    const int line = idx / per_line, j = idx - line * per_line;
+    const int line = fast_div(idx, per_line_div), j = idx - line * per_line;
     const float2 *src = in + line * ld;
     float2 v[R];
-    const int k = j % Ns;
+    const int jq = fast_div(j, span_div);
+    const int k = j - jq * Ns;
 #pragma unroll
     for (int r = 0; r < R; ++r) v[r] = src[j + r * per_line];
 #pragma unroll
@@ -101,7 +106,7 @@ __device__ __forceinline__ void stockham_stage(const float2 *__restrict__ in, fl
       v[r] = cmul(v[r], w);
     }
     dft_small<R>(v, inv);
-    float2 *dst = out + line * ld + (j / Ns) * Ns * R + k;
+    float2 *dst = out + line * ld + jq * Ns * R + k;
 #pragma unroll
     for (int r = 0; r < R; ++r) dst[r * Ns] = v[r];
   }
@@ -117,10 +122,11 @@ __device__ float2 *fft_stages(float2 *a, float2 *b, int lines, int N, int ld, co
   for (int st = 0; st < ax.nstages; ++st) {
     const int R = ax.radix[st];
     __syncthreads();
-    if (R == 4) stockham_stage<4>(a, b, lines, N, ld, Ns, tw, inv);
-    else if (R == 2) stockham_stage<2>(a, b, lines, N, ld, Ns, tw, inv);
-    else if (R == 3) stockham_stage<3>(a, b, lines, N, ld, Ns, tw, inv);
-    else stockham_stage<5>(a, b, lines, N, ld, Ns, tw, inv);
+    const FastDiv pl = ax.per_line[st], sp = ax.span[st];
+    if (R == 4) stockham_stage<4>(a, b, lines, N, ld, Ns, tw, inv, pl, sp);
+    else if (R == 2) stockham_stage<2>(a, b, lines, N, ld, Ns, tw, inv, pl, sp);
+    else if (R == 3) stockham_stage<3>(a, b, lines, N, ld, Ns, tw, inv, pl, sp);
+    else stockham_stage<5>(a, b, lines, N, ld, Ns, tw, inv, pl, sp);
     Ns *= R;
     float2 *t = a;
     a = b;
@@ -209,7 +215,7 @@ __global__ void __launch_bounds__(256) k_fft_z_r2c(const FftTask *__restrict__ t
   const int M = t.count;
   unsigned long long *g = fixed_grid + s.grid_base;
   for (int idx = threadIdx.x; idx < M * N; idx += blockDim.x) {
-    const int p = idx / N, k = idx - p * N;
+    const int p = fast_div(idx, pl.axis[2].n_div), k = idx - p * N;
     const int l = 2 * (t.first + p);
     unsigned long long *ra = g + (long long)l * N + k;
     const bool two = l + 1 < nlines;
@@ -223,7 +229,7 @@ __global__ void __launch_bounds__(256) k_fft_z_r2c(const FftTask *__restrict__ t
   float2 *r = fft_lines(bufa, bufb, M, N, N, pl.axis[2], twiddles + pl.axis[2].tw_base, false);
   float2 *h = half + s.half_base;
   for (int idx = threadIdx.x; idx < M * nzh; idx += blockDim.x) {
-    const int p = idx / nzh, k = idx - p * nzh;
+    const int p = fast_div(idx, pl.axis[2].half_div), k = idx - p * nzh;
     const int l = 2 * (t.first + p);
     const float2 z = r[p * N + k];
     const float2 zc = r[p * N + (N - k) % N];
@@ -252,7 +258,7 @@ __global__ void __launch_bounds__(256) k_fft_z_c2r(const FftTask *__restrict__ t
   const int M = t.count;
   const float2 *h = half + s.half_base;
   for (int idx = threadIdx.x; idx < M * N; idx += blockDim.x) {
-    const int p = idx / N, k = idx - p * N;
+    const int p = fast_div(idx, pl.axis[2].n_div), k = idx - p * N;
     const int l = 2 * (t.first + p);
     const bool has_b = l + 1 < nlines;
     float2 a, b;
@@ -274,7 +280,7 @@ __global__ void __launch_bounds__(256) k_fft_z_c2r(const FftTask *__restrict__ t
   float2 *r = fft_lines(bufa, bufb, M, N, N, pl.axis[2], twiddles + pl.axis[2].tw_base, true);
   float *g = real_grid + s.grid_base;
   for (int idx = threadIdx.x; idx < M * N; idx += blockDim.x) {
-    const int p = idx / N, k = idx - p * N;
+    const int p = fast_div(idx, pl.axis[2].n_div), k = idx - p * N;
     const int l = 2 * (t.first + p);
     const float2 z = r[idx];
     g[(long long)l * N + k] = z.x;
@@ -643,7 +649,7 @@ __global__ void __launch_bounds__(256) k_fft_plane(const FftTask *__restrict__ t
   const int ldy = ny + 1, ldx = nx + 1;  // padded lines (bank-conflict-free transposes)
   float2 *h = half + s.half_base + kz;  // element (x, y) at h[(x * ny + y) * nzh]
   for (int idx = threadIdx.x; idx < nx * ny; idx += blockDim.x) {
-    const int x = idx / ny, y = idx - x * ny;
+    const int x = fast_div(idx, pl.axis[1].n_div), y = idx - x * ny;
     bufa[x * ldy + y] = h[(long long)idx * nzh];
   }
   const float *modz = stage_plane_tables(tab, pl, twiddles, moduli + s.moduli_base, nx, ny);
@@ -651,7 +657,7 @@ __global__ void __launch_bounds__(256) k_fft_plane(const FftTask *__restrict__ t
   float2 *r = fft_stages(bufa, bufb, nx, ny, ldy, pl.axis[1], tab.tw_y, false);
   float2 *o = (r == bufa) ? bufb : bufa;
   for (int idx = threadIdx.x; idx < nx * ny; idx += blockDim.x) {
-    const int x = idx / ny, y = idx - x * ny;
+    const int x = fast_div(idx, pl.axis[1].n_div), y = idx - x * ny;
     o[y * ldx + x] = r[x * ldy + y];
   }
   // forward x: ny lines of nx
@@ -662,7 +668,7 @@ __global__ void __launch_bounds__(256) k_fft_plane(const FftTask *__restrict__ t
   const float two_pref = (float)(2.0 * ONE_4PI_EPS0 / (2.0 * M_PI * volume));
   double energy = 0.0, virial = 0.0;
   for (int idx = threadIdx.x; idx < nx * ny; idx += blockDim.x) {
-    const int y = idx / nx, mx = idx - y * nx;
+    const int y = fast_div(idx, pl.axis[0].n_div), mx = idx - y * nx;
     convolve_point<ENERGY>(r[y * ldx + mx], mx, y, kz, nx, ny, nz, s, tab.mod_x, tab.mod_y, modz, factor,
                            two_pref, energy, virial);
   }
@@ -671,13 +677,13 @@ __global__ void __launch_bounds__(256) k_fft_plane(const FftTask *__restrict__ t
   r = fft_stages(r, o, ny, nx, ldx, pl.axis[0], tab.tw_x, true);
   o = (r == bufa) ? bufb : bufa;
   for (int idx = threadIdx.x; idx < nx * ny; idx += blockDim.x) {
-    const int x = idx / ny, y = idx - x * ny;
+    const int x = fast_div(idx, pl.axis[1].n_div), y = idx - x * ny;
     o[x * ldy + y] = r[y * ldx + x];
   }
   // inverse y
   r = fft_stages(o, r, nx, ny, ldy, pl.axis[1], tab.tw_y, true);
   for (int idx = threadIdx.x; idx < nx * ny; idx += blockDim.x) {
-    const int x = idx / ny, y = idx - x * ny;
+    const int x = fast_div(idx, pl.axis[1].n_div), y = idx - x * ny;
     h[(long long)idx * nzh] = r[x * ldy + y];
   }
   if (ENERGY) block_energy(energy, virial, e_pme, e_pme_vir, blockIdx.x);
@@ -716,7 +722,7 @@ __global__ void __cluster_dims__(PLANE_CLUSTER, 1, 1) __launch_bounds__(256)
   const int y0 = min(ny, rank * cols_per), nc = min(ny, y0 + cols_per) - y0;
   float2 *h = half + s.half_base + kz;  // element (x, y) at h[(x * ny + y) * nzh]
   for (int idx = threadIdx.x; idx < nr * ny; idx += blockDim.x) {
-    const int xl = idx / ny, y = idx - xl * ny;
+    const int xl = fast_div(idx, pl.axis[1].n_div), y = idx - xl * ny;
     ra[xl * ldy + y] = h[((long long)(x0 + xl) * ny + y) * nzh];
   }
   const float *modz = stage_plane_tables(tab, pl, twiddles, moduli + s.moduli_base, nx, ny);
@@ -725,7 +731,7 @@ __global__ void __cluster_dims__(PLANE_CLUSTER, 1, 1) __launch_bounds__(256)
   const float2 *rows = fft_stages(ra, rb, nr, ny, ldy, pl.axis[1], tab.tw_y, false);
   cluster.sync();
   for (int idx = threadIdx.x; idx < nc * nx; idx += blockDim.x) {
-    const int yl = idx / nx, x = idx - yl * nx;
+    const int yl = fast_div(idx, pl.axis[0].n_div), x = idx - yl * nx;
     const int owner = x / rows_per;
     const float2 *src = cluster.map_shared_rank(rows, owner);
     ca[yl * ldx + x] = src[(x - owner * rows_per) * ldy + y0 + yl];
@@ -738,14 +744,14 @@ __global__ void __cluster_dims__(PLANE_CLUSTER, 1, 1) __launch_bounds__(256)
   const float two_pref = (float)(2.0 * ONE_4PI_EPS0 / (2.0 * M_PI * volume));
   double energy = 0.0, virial = 0.0;
   for (int idx = threadIdx.x; idx < nc * nx; idx += blockDim.x) {
-    const int yl = idx / nx, mx = idx - yl * nx;
+    const int yl = fast_div(idx, pl.axis[0].n_div), mx = idx - yl * nx;
     convolve_point<ENERGY>(c[yl * ldx + mx], mx, y0 + yl, kz, nx, ny, nz, s, tab.mod_x, tab.mod_y, modz, factor,
                            two_pref, energy, virial);
   }
   const float2 *cols = fft_stages(c, c == ca ? cb : ca, nc, nx, ldx, pl.axis[0], tab.tw_x, true);
   cluster.sync();
   for (int idx = threadIdx.x; idx < nr * ny; idx += blockDim.x) {
-    const int xl = idx / ny, y = idx - xl * ny;
+    const int xl = fast_div(idx, pl.axis[1].n_div), y = idx - xl * ny;
     const int owner = y / cols_per;
     const float2 *src = cluster.map_shared_rank(cols, owner);
     ra[xl * ldy + y] = src[(y - owner * cols_per) * ldx + x0 + xl];
@@ -754,7 +760,7 @@ __global__ void __cluster_dims__(PLANE_CLUSTER, 1, 1) __launch_bounds__(256)
   // inverse y over this block's rows
   const float2 *r = fft_stages(ra, rb, nr, ny, ldy, pl.axis[1], tab.tw_y, true);
   for (int idx = threadIdx.x; idx < nr * ny; idx += blockDim.x) {
-    const int xl = idx / ny, y = idx - xl * ny;
+    const int xl = fast_div(idx, pl.axis[1].n_div), y = idx - xl * ny;
     h[((long long)(x0 + xl) * ny + y) * nzh] = r[xl * ldy + y];
   }
   if (ENERGY) block_energy(energy, virial, e_pme, e_pme_vir, blockIdx.x);
