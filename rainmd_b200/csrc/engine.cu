@@ -576,7 +576,7 @@ void Engine::upload_all(const std::vector<const rmd_system *> &src) {
   lj.upload(h_lj);
   noise.alloc(3 * (size_t)N);
   noise.zero();
-  force.alloc(3 * (size_t)N);
+  force.alloc(3 * (size_t)N + 1);  // rounded up to even: k_rebuild_decide clears it two words at a time
   force.zero();
   saved_force.alloc(3 * (size_t)N);
   saved_force.zero();
@@ -1268,6 +1268,7 @@ LaunchCtx Engine::ctx() const {
   c.exc_partner = exc_partner.p;
   c.exc_param = exc_param.p;
   c.force = force.p;
+  c.force_cleared = false;
   c.e_lj = e_lj.p;
   c.e_coul = e_coul.p;
   c.e_vir = e_vir.p;
@@ -1450,9 +1451,11 @@ void Engine::record_forces(int rebuild, bool energy) {
     launch_rebuild(c, stream);
     recorded += 1 + rebuild_launches(c);
   } else if (rebuild == REBUILD_IF_STALE) {
-    record_conditional_rebuild(c);
+    record_conditional_rebuild(c);  // its decision kernel also clears the force array
   }
-  launch_nonbonded(c, energy, nb_lanes, stream);
+  LaunchCtx nb = c;
+  nb.force_cleared = rebuild == REBUILD_IF_STALE;
+  launch_nonbonded(nb, energy, nb_lanes, stream);
   launch_bonded(c, energy, stream);
   if (pme_on) {
     CUDA_OK(cudaStreamWaitEvent(stream, ev_join, 0));
@@ -1480,7 +1483,8 @@ void Engine::record_conditional_rebuild(const LaunchCtx &c) {
     throw Error(RMD_ERR_CUDA, "a conditional rebuild can only be recorded into a captured graph");
   cudaGraphConditionalHandle handle;
   CUDA_OK(cudaGraphConditionalHandleCreate(&handle, graph, 0, 0));
-  launch_rebuild_decide(handle, disp.p, list_allow.p, sys.p, S, stale.p, list_builds.p, stream);
+  launch_rebuild_decide(handle, disp.p, list_allow.p, sys.p, S, stale.p, list_builds.p,
+                        c.pair_list != 1 ? force.p : nullptr, N, stream);
   recorded += 1;
   CUDA_OK(cudaStreamGetCaptureInfo(stream, &status, nullptr, &graph, &deps, &ndeps));
   cudaGraphNodeParams params = {};

@@ -113,6 +113,7 @@ struct LaunchCtx {
   int *order_pos;          // per slot: its position in group_order
   float4 *group_box;       // per group slot: bounding box lo, hi of its atoms' wrapped positions
   unsigned long long *e_acc;  // per-atom integer energy sums of the group-pair kernel (3 N)
+  bool force_cleared;  // the force array was zeroed since the last evaluation (launch_nonbonded skips its clear)
   // cell-ordered copies written at each rebuild and kept current by the integrator:
   // spos[slot] = position minus the atom's wrap shift (w = charge), the original index,
   // the LJ type; rank[atom] = slot and wrap[atom] = that shift
@@ -179,8 +180,10 @@ int rebuild_launches(const LaunchCtx &c);  // kernels launch_rebuild issues (wit
 // Rebuild on demand (lists.cu): flag the systems that have moved past half their skin since
 // their last build and set `handle` (an IF node's condition) when any has; and the reset every
 // rebuild starts with (of the flagged systems, or of all when `only` is null).
+// `clear_force` (if not null): the 3 N-word force array, zeroed by the same launch.
 void launch_rebuild_decide(cudaGraphConditionalHandle handle, const unsigned *disp, const float *allow,
-                           const DevSys *sys, int S, int *stale, unsigned long long *rebuilds, cudaStream_t stream);
+                           const DevSys *sys, int S, int *stale, unsigned long long *rebuilds,
+                           unsigned long long *clear_force, int n_atoms, cudaStream_t stream);
 void launch_rebuild_reset(int *required, int *required_max, unsigned *disp, float *allow, int *rebuilt, int S,
                           unsigned long long *builds, const int *only, cudaStream_t stream);
 // group slots a system needs for a given group size (its search groups never exceed this)

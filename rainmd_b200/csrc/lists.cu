@@ -14,6 +14,8 @@
 //     hits in candidate order, so every row's order equals the sequential one.
 #include <climits>
 
+#include <algorithm>
+
 #include "common.cuh"
 #include "kernels.h"
 
@@ -820,7 +822,14 @@ __global__ void __launch_bounds__(32 * GROUP_ROW_WARPS)
 // not trigger one: the host's block check reports it.
 __global__ void k_rebuild_decide(cudaGraphConditionalHandle handle, const unsigned *__restrict__ disp,
                                  const float *__restrict__ allow, const DevSys *__restrict__ sys, int S,
-                                 int *__restrict__ stale, unsigned long long *__restrict__ rebuilds) {
+                                 int *__restrict__ stale, unsigned long long *__restrict__ rebuilds,
+                                 ulonglong2 *__restrict__ clear, long long clear_pairs) {
+  // the force array the group-pair kernel accumulates into, cleared by the whole grid (the
+  // decision itself is block 0's), which saves the step graph a memset node
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < clear_pairs;
+       k += (long long)gridDim.x * blockDim.x)
+    clear[k] = make_ulonglong2(0ull, 0ull);
+  if (blockIdx.x != 0) return;
   int need = 0;
   for (int s = threadIdx.x; s < S; s += blockDim.x) {
     const float skin = sys[s].list_cutoff - sys[s].cutoff;
@@ -859,8 +868,14 @@ __global__ void k_rebuild_reset(int *__restrict__ required, int *__restrict__ re
 }
 
 void launch_rebuild_decide(cudaGraphConditionalHandle handle, const unsigned *disp, const float *allow,
-                           const DevSys *sys, int S, int *stale, unsigned long long *rebuilds, cudaStream_t stream) {
-  k_rebuild_decide<<<1, 256, 0, stream>>>(handle, disp, allow, sys, S, stale, rebuilds);
+                           const DevSys *sys, int S, int *stale, unsigned long long *rebuilds,
+                           unsigned long long *clear_force, int n_atoms, cudaStream_t stream) {
+  // 3 N words of fixed-point force, two a thread (the array is 16-byte aligned and 3 N is
+  // rounded up to even in its allocation)
+  const long long pairs = clear_force ? (3LL * n_atoms + 1) / 2 : 0;
+  const int blocks = (int)std::max(1LL, std::min(1184LL, (pairs + 255) / 256));
+  k_rebuild_decide<<<blocks, 256, 0, stream>>>(handle, disp, allow, sys, S, stale, rebuilds,
+                                                reinterpret_cast<ulonglong2 *>(clear_force), pairs);
 }
 
 void launch_rebuild_reset(int *required, int *required_max, unsigned *disp, float *allow, int *rebuilt, int S,

@@ -555,7 +555,8 @@ __global__ void k_group_pair_energies(const unsigned long long *__restrict__ e_a
 static void launch_group_pairs(const LaunchCtx &c, bool energy, int lanes, cudaStream_t stream) {
   const int split = lanes >= 128 ? 4 : lanes >= 64 ? 2 : 1;  // lanes per group row: warps sharing it x 32
   // (errors of these calls surface in the caller's cudaGetLastError, as the launches' do)
-  (void)cudaMemsetAsync(c.force, 0, sizeof(unsigned long long) * 3 * (size_t)c.n_atoms, stream);
+  if (!c.force_cleared)
+    (void)cudaMemsetAsync(c.force, 0, sizeof(unsigned long long) * 3 * (size_t)c.n_atoms, stream);
   if (energy) (void)cudaMemsetAsync(c.e_acc, 0, sizeof(unsigned long long) * 3 * (size_t)c.n_atoms, stream);
   const int threads = 128;
   const int blocks = (int)(((long long)c.n_groups_total * split * 32 + threads - 1) / threads);
