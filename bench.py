@@ -70,10 +70,19 @@ def smooth_at_least(n: int) -> int:
         n += 1
 
 
-def options_for(grid, seed):
+# Neighbour-list skin (nm). 0.25 nm for the water boxes: on the 23,558-atom NPT box a sweep of
+# 0.10 / 0.15 / 0.20 / 0.25 / 0.30 nm gave 0.118 / 0.115 / 0.112 / 0.111 / 0.111 ms a step (fewer
+# rebuilds against longer rows); --skin overrides it. The small boxes of config 0 and the batch
+# (2.3-4.9 nm) keep 0.15 nm, below the 0.9 (L/2 - rc) cap of the reference's skinFor
+# (cells.js:67-91) on the smallest of them.
+LIST_SKIN = 0.25
+SMALL_BOX_SKIN = 0.15
+
+
+def options_for(grid, seed, skin=None):
     return {"timestep": TIMESTEP_PS, "temperature": 300.0, "friction": 1.0, "seed": seed,
             "pmeOrder": 4, "grid": grid, "ewaldTolerance": 5e-4, "waterSolver": 1,
-            "skin": 0.15, "rebuildInterval": 10, "adaptiveRebuild": True,
+            "skin": LIST_SKIN if skin is None else skin, "rebuildInterval": 10, "adaptiveRebuild": True,
             "dispersionCorrection": True}
 
 
@@ -110,7 +119,7 @@ def batched_block(steps: int, seed: int, single_steps: int = 200, rank: int = 0,
 
     items = batch_workload(seed)
     systems = [s for s, _, _ in items]
-    options = [options_for(g, seed=11 + k) for k, (_, _, g) in enumerate(items)]
+    options = [options_for(g, seed=11 + k, skin=SMALL_BOX_SKIN) for k, (_, _, g) in enumerate(items)]
     atoms = [s["topology"]["atomCount"] for s in systems]
     costs = [system_cost(a, float(np.prod(np.asarray(s["boxVectors"], dtype=np.float64)[[0, 4, 8]])), 0.9, g)
              for a, s, (_, _, g) in zip(atoms, systems, items)]
@@ -596,16 +605,17 @@ def config_block(args, atoms, grid, world):
     return {"workload": describe(args.workload, grid, args.ensemble == "npt"),
             "atoms": atoms, "replicas": world, "parallelism": f"replicas{world}",
             "l2": "flushed (256 MB written) before every timed block",
-            "lists": "reference host schedule" if args.rebuild_schedule else "rebuilt on demand"}
+            "lists": "reference host schedule" if args.rebuild_schedule else "rebuilt on demand",
+            "skin_nm": LIST_SKIN}
 
 
-def prepare(system, pos, grid, seed, npt, args):
+def prepare(system, pos, grid, seed, npt, args, skin=None):
     """A simulation of `system` minimised and equilibrated (untimed), with its block length:
     NPT runs in blocks of the barostat interval (a move at the start of each block, as the
     reference's run() attempts one at block boundaries), NVT in blocks of 100 steps."""
     from rainmd_b200.simulation import GpuSimulation
 
-    opts = options_for(grid, seed=seed)
+    opts = options_for(grid, seed=seed, skin=skin)
     if args.pair_list is not None:
         opts["pairList"] = args.pair_list
     if args.nonbonded_lanes is not None:
@@ -674,7 +684,7 @@ def config0_line(args, barrier):
     cores. The reference reports 133 ns/day for this system on Apple M-series WebGPU."""
     system, pos, grid = workload("chain-1190", seed=1)
     n = system["topology"]["atomCount"]
-    sim, block = prepare(system, pos, grid, seed=7, npt=True, args=args)
+    sim, block = prepare(system, pos, grid, seed=7, npt=True, args=args, skin=SMALL_BOX_SKIN)
     steps = max(args.steps, 100)
     device_ms, launches, builds, moves = timed(sim, steps, args.warmup, block, barrier)
     seconds, h2d, d2h, _ = end_to_end(sim, n, steps, block, barrier, True)
@@ -694,6 +704,7 @@ def config0_line(args, barrier):
 
 
 def main():
+    global LIST_SKIN
     parser = argparse.ArgumentParser()
     parser.add_argument("--gpus", type=int, default=1)
     parser.add_argument("--steps", type=int, default=2000)
@@ -720,12 +731,16 @@ def main():
     parser.add_argument("--pair-list", type=int, choices=[0, 1], default=None,
                         help="neighbour structure of the pair loop: 0 group-pair rows, 1 per-atom rows "
                              "(default: the engine's)")
+    parser.add_argument("--skin", type=float, default=None,
+                        help=f"neighbour-list skin in nm (default {LIST_SKIN})")
     parser.add_argument("--nonbonded-lanes", type=int, choices=[32, 64, 128], default=None,
                         help="fix the group-pair kernel's lanes a row instead of autotuning them")
     parser.add_argument("--rebuild-schedule", action="store_true",
                         help="rebuild the lists on the reference's host schedule instead of on demand "
                              "(the same kernels; ncu profiles no kernel of a graph with conditional nodes)")
     args = parser.parse_args()
+    if args.skin is not None:
+        LIST_SKIN = float(args.skin)
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -1,6 +1,6 @@
 """Parity on the benchmark's own configuration, through the C ABI.
 
-The benchmark runs the 23,558-atom TIP3P box (rc 0.9 nm, skin 0.15 nm, PME order 4 on 64^3)
+The benchmark runs the 23,558-atom TIP3P box (rc 0.9 nm, skin 0.25 nm, PME order 4 on 64^3)
 with autotuned launch shapes and lists rebuilt on demand inside the step graph. Here:
   - the cell and neighbour lists the device holds after on-demand rebuilds mid-run equal, bit
     for bit, the f32 restatement of the reference's cell assignment and search
@@ -33,10 +33,14 @@ BOLTZMANN = 0.008314462618      # shared/units.js:50
 BAR = 0.06022140857             # kJ/mol/nm^3 per bar, shared/units.js:53
 
 
-def bench_options(grid, seed=7, **extra):
+BENCH_SKIN = 0.25      # bench.py LIST_SKIN: the water boxes
+SMALL_BOX_SKIN = 0.15  # bench.py SMALL_BOX_SKIN: the 1,190-atom system and the batch
+
+
+def bench_options(grid, seed=7, skin=BENCH_SKIN, **extra):
     """The benchmark's options (bench.py options_for)."""
     o = {"timestep": 0.002, "temperature": 300.0, "friction": 1.0, "seed": seed, "pmeOrder": 4,
-         "grid": grid, "ewaldTolerance": 5e-4, "waterSolver": 1, "skin": 0.15, "rebuildInterval": 10,
+         "grid": grid, "ewaldTolerance": 5e-4, "waterSolver": 1, "skin": skin, "rebuildInterval": 10,
          "adaptiveRebuild": True, "dispersionCorrection": True}
     o.update(extra)
     return o
@@ -196,10 +200,10 @@ def test_benchmark_lists_bit_exact_after_on_demand_rebuilds(bench_box, form, gro
     assert d["list_builds"] - builds0 >= 3  # rebuilt on demand inside the graphs
     if group is not None:
         assert sim.kernelShapes()["neighbourGroupAtoms"] == group
-    pairs = assert_lists_match_oracle(sim, system)
+    pairs = assert_lists_match_oracle(sim, system, skin=BENCH_SKIN)
     assert pairs > 23558 * 400
     if form == 2:
-        assert assert_group_rows_cover(sim, system) >= pairs // 2
+        assert assert_group_rows_cover(sim, system, skin=BENCH_SKIN) >= pairs // 2
     sim.release()
 
 
@@ -221,7 +225,8 @@ def test_batch_lists_bit_exact_per_system(bench_box):
     rebuilds equal the oracle's for that system alone."""
     items = [chain1190(), water(2854), bench_box]
     systems = [s for s, _, _ in items]
-    batch = BatchSimulation(systems, [bench_options(g, seed=5 + k, pairList=2) for k, (_, _, g) in enumerate(items)])
+    batch = BatchSimulation(systems, [bench_options(g, seed=5 + k, skin=SMALL_BOX_SKIN, pairList=2)
+                                      for k, (_, _, g) in enumerate(items)])
     for k, (_, p, _) in enumerate(items):
         batch.setState(k, p)
     batch.initialise()
@@ -244,8 +249,8 @@ def test_cell_plan_is_the_engines(bench_box):
     sim.initialise()
     d = sim.diagnostics()
     plan = planSystem(system, options)
-    expect = oracle.plan_cell_list(23558, system["boxVectors"], 0.9, skin=0.15)
-    assert d["skin"] == plan["skin"] == 0.15
+    expect = oracle.plan_cell_list(23558, system["boxVectors"], 0.9, skin=BENCH_SKIN)
+    assert d["skin"] == plan["skin"] == BENCH_SKIN
     assert list(d["cell_counts"]) == plan["counts"] == expect["counts"]
     assert d["neighbour_capacity"] == plan["capacity"] == (expect["maxNeighbours"] + 3) // 4 * 4
     assert d["pme_alpha"] == plan["alpha"] and list(d["pme_grid"]) == plan["grid"] == grid
@@ -412,7 +417,8 @@ def test_moves_inside_step_graphs_evaluate_the_trial_state(which, bench_box):
         system, pos, grid = chain1190()
     else:
         system, pos, grid = bench_box
-    sim = GpuSimulation(system, bench_options(grid, seed=13, pressure=1.0, barostatInterval=25))
+    skin = SMALL_BOX_SKIN if which == "chain-1190" else BENCH_SKIN
+    sim = GpuSimulation(system, bench_options(grid, seed=13, skin=skin, pressure=1.0, barostatInterval=25))
     sim.setState(pos)
     sim.initialise()
     sim.minimise(maxIterations=30, forceTolerance=1000.0)
