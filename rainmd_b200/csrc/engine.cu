@@ -530,12 +530,11 @@ void Engine::build(int count, const rmd_system *systems, const rmd_options *opti
   // its DMA lands; cudaMemset, which is asynchronous) go. A non-blocking stream would let a
   // kernel read a buffer before such an upload had finished.
   CUDA_OK(cudaStreamCreateWithFlags(&stream, cudaStreamDefault));
-  // the reciprocal branch is a chain of small latency-bound kernels next to one large pair
-  // kernel: at higher priority its blocks take SM slots as they free instead of after the
-  // pair kernel's last wave
-  int lowest = 0, highest = 0;
-  CUDA_OK(cudaDeviceGetStreamPriorityRange(&lowest, &highest));
-  CUDA_OK(cudaStreamCreateWithPriority(&side, cudaStreamDefault, highest));
+  // The reciprocal branch's stream. Step graphs are instantiated without per-node priorities,
+  // so its kernels run at the graph's launch priority; measured on one B200 (23,558 atoms),
+  // giving them the highest priority (cudaGraphInstantiateFlagUseNodePriority) slowed the NVT
+  // step from 0.101 to 0.104 ms, and the pair branch the higher one changed nothing.
+  CUDA_OK(cudaStreamCreateWithFlags(&side, cudaStreamDefault));
   CUDA_OK(cudaStreamCreateWithFlags(&cond, cudaStreamNonBlocking));
   on_demand = true;
   for (auto &h : hs) on_demand = on_demand && h.on_demand;
