@@ -184,7 +184,7 @@ struct Engine {
   // the reciprocal-space branch of a force evaluation runs on `side`, forked from and joined
   // back to `stream` with events (inside a captured graph these become parallel branches)
   cudaStream_t side = nullptr;
-  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_clear = nullptr;
   // the stream a conditional rebuild body is captured on (record_forces)
   cudaStream_t cond = nullptr;
   bool on_demand = true;  // lists rebuilt when the device finds them stale (all systems agree)
@@ -283,6 +283,7 @@ struct Engine {
     for (auto &kv : graphs) cudaGraphExecDestroy(kv.second);
     if (ev_fork) cudaEventDestroy(ev_fork);
     if (ev_join) cudaEventDestroy(ev_join);
+    if (ev_clear) cudaEventDestroy(ev_clear);
     if (side) cudaStreamDestroy(side);
     if (cond) cudaStreamDestroy(cond);
     if (stream) cudaStreamDestroy(stream);
@@ -540,6 +541,7 @@ void Engine::build(int count, const rmd_system *systems, const rmd_options *opti
   for (auto &h : hs) on_demand = on_demand && h.on_demand;
   CUDA_OK(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
   CUDA_OK(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
+  CUDA_OK(cudaEventCreateWithFlags(&ev_clear, cudaEventDisableTiming));
   upload_all(src);
 }
 
@@ -1435,14 +1437,17 @@ BaroArgs Engine::bargs() const {
 void Engine::record_forces(int rebuild, bool energy) {
   const LaunchCtx c = ctx();
   // The reciprocal-space chain up to the convolved grid only reads positions, so it runs
-  // concurrently with the list rebuild and the pair and bonded kernels; the gather, which
-  // adds into the force array the pair kernel stores (and reads the cell order the rebuild
-  // writes), waits for both branches.
+  // concurrently with the list rebuild and the pair and bonded kernels. The gather adds into
+  // the force array (and reads the cell order the rebuild writes). With group-pair rows every
+  // force is an integer atomic add, so the gather joins that branch as soon as the array is
+  // cleared and the rebuild is done, beside the pair kernel; the per-atom-row pair kernel
+  // stores its atoms' forces, so there the gather waits for both branches.
+  const bool gather_beside = pme_on && c.pair_list != 1;
   if (pme_on) {
     CUDA_OK(cudaEventRecord(ev_fork, stream));
     CUDA_OK(cudaStreamWaitEvent(side, ev_fork, 0));
     launch_pme_grid(c, energy, side);
-    CUDA_OK(cudaEventRecord(ev_join, side));
+    if (!gather_beside) CUDA_OK(cudaEventRecord(ev_join, side));
   }
   if (rebuild == REBUILD_FORCED) {
     launch_rebuild_reset(required.p, required_max.p, disp.p, list_allow.p, list_rebuilt.p, S, list_builds.p + 1,
@@ -1454,11 +1459,21 @@ void Engine::record_forces(int rebuild, bool energy) {
   }
   LaunchCtx nb = c;
   nb.force_cleared = rebuild == REBUILD_IF_STALE;
+  if (gather_beside) {
+    if (!nb.force_cleared) {
+      CUDA_OK(cudaMemsetAsync(force.p, 0, sizeof(unsigned long long) * 3 * (size_t)N, stream));
+      nb.force_cleared = true;
+    }
+    CUDA_OK(cudaEventRecord(ev_clear, stream));
+    CUDA_OK(cudaStreamWaitEvent(side, ev_clear, 0));
+    launch_pme_gather(c, side);
+    CUDA_OK(cudaEventRecord(ev_join, side));
+  }
   launch_nonbonded(nb, energy, nb_lanes, stream);
   launch_bonded(c, energy, stream);
   if (pme_on) {
     CUDA_OK(cudaStreamWaitEvent(stream, ev_join, 0));
-    launch_pme_gather(c, stream);
+    if (!gather_beside) launch_pme_gather(c, stream);
   }
   recorded += nonbonded_launches(c, energy) + (n_bonds + n_angles + n_tors + n_rest > 0 ? 1 : 0) + pme_launches(c);
   if (energy) {
