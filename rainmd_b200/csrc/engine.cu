@@ -319,7 +319,7 @@ struct Engine {
   // kernel-shape autotuner: which shapes were left to it, and what it measured
   bool tune_group = false, tune_lanes = false, tune_spread = false;
   double tune_ms[9] = {-1, -1, -1, -1, -1, -1, -1, -1, -1};
-  void autotune();
+  bool autotune();  // true when it launched timing work (the force array then holds its sums)
   void drop_graphs();
   int check_capacity();  // returns max required; grows if needed
   bool capacity_grew = false;  // the last check_capacity grew the lists (and rebuilt them, forces only)
@@ -1645,8 +1645,8 @@ std::map<std::string, std::array<int, 3>> g_tuned;
 // Each candidate is timed with CUDA events on the engine's stream over a few launches on the
 // engine's own current state, the fastest is kept, and the choice is cached by workload
 // shape (atoms, systems, cells, PME grids and order, accumulation mode).
-void Engine::autotune() {
-  if (!(tune_group || tune_lanes || tune_spread)) return;
+bool Engine::autotune() {
+  if (!(tune_group || tune_lanes || tune_spread)) return false;
   // captured step graphs hold the shapes they were recorded with: they stay valid (and are
   // replayed without re-capture by the next run) unless the tuned shapes change
   const std::array<int, 3> before = {group_atoms, nb_lanes, spread_atoms};
@@ -1664,7 +1664,7 @@ void Engine::autotune() {
       if (tune_lanes) nb_lanes = it->second[1];
       if (tune_spread) spread_atoms = it->second[2];
       keep_or_drop_graphs();
-      return;
+      return false;
     }
   }
   cudaEvent_t a, b;
@@ -1729,6 +1729,7 @@ void Engine::autotune() {
     g_tuned[key] = {group_atoms, nb_lanes, spread_atoms};
   }
   keep_or_drop_graphs();
+  return true;
 }
 
 void Engine::initialise() {
@@ -1736,10 +1737,12 @@ void Engine::initialise() {
   sync();
   for (auto &h : hs) h.steps_since_rebuild = 0;
   check_capacity();
-  autotune();
-  // the forces (accumulated into by the timed pair-loop launches) from a clean evaluation
-  evaluate(false, false);
-  sync();
+  // the forces from a clean evaluation when the autotuner's timed pair-loop launches added into
+  // them (every launch shape gives the same forces, so a cached choice keeps the first ones)
+  if (autotune()) {
+    evaluate(false, false);
+    sync();
+  }
   // kinetic energies of the current velocities, for energy() before any step
   launch_integrate(iargs(0), INT_CLOSE_KINETIC, stream);
   kernel_launches += 1;
