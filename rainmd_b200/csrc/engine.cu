@@ -6,6 +6,7 @@
 // reference's shared/ modules and cited where they appear. The step itself is a CUDA graph
 // per block of steps: one replay launches every kernel of every step of every system.
 #include <algorithm>
+#include <cstddef>
 #include <array>
 #include <climits>
 #include <cmath>
@@ -280,6 +281,7 @@ struct Engine {
   long long kernel_launches = 0;                     // kernels launched so far (graphs and direct)
 
   ~Engine() {
+    if (pinned) cudaFreeHost(pinned);
     for (auto &kv : graphs) cudaGraphExecDestroy(kv.second);
     if (ev_fork) cudaEventDestroy(ev_fork);
     if (ev_join) cudaEventDestroy(ev_join);
@@ -334,6 +336,20 @@ struct Engine {
   void check_block(int steps);
   void energy(int s, rmd_energy_report *out);
   void sync() { CUDA_OK(cudaStreamSynchronize(stream)); }
+  // Page-locked staging for the state copies of setState and readState: every copy of a call
+  // is one asynchronous transfer on the engine stream, and the call waits once.
+  void *pinned = nullptr;
+  size_t pinned_bytes = 0;
+  char *staging(size_t bytes) {
+    if (bytes > pinned_bytes) {
+      if (pinned) CUDA_OK(cudaFreeHost(pinned));
+      pinned = nullptr;
+      pinned_bytes = 0;
+      CUDA_OK(cudaMallocHost(&pinned, bytes));
+      pinned_bytes = bytes;
+    }
+    return static_cast<char *>(pinned);
+  }
   void update_box_from_host(int s);
   void attempt_volume_change();
   double scale_volume(int s, double ls);
@@ -1559,22 +1575,29 @@ void Engine::set_state(int s, const double *pos, const double *vel_in, int64_t s
   for (int k = 0; k < 3 * h.n; ++k) span = std::max(span, std::fabs(pos[k]));
   h.tol_floor = std::isfinite(h.min_constraint) ? 4.0 * span * std::ldexp(1.0, -24) / h.min_constraint : 0.0;
   h.tolerance = std::max(h.requested_tol, h.tol_floor);
-  std::vector<float4> p(h.n), v(h.n);
+  sync();  // the staging buffer may still feed an earlier call's copies
+  char *stage = staging(sizeof(float4) * 2 * (size_t)h.n + 16);
+  float4 *p = reinterpret_cast<float4 *>(stage), *v = p + h.n;
   for (int i = 0; i < h.n; ++i) {
     p[i] = make_float4((float)pos[3 * i], (float)pos[3 * i + 1], (float)pos[3 * i + 2], (float)h.charges[i]);
     v[i] = make_float4(vel_in ? (float)vel_in[3 * i] : 0.f, vel_in ? (float)vel_in[3 * i + 1] : 0.f,
                        vel_in ? (float)vel_in[3 * i + 2] : 0.f, h.masses[i] > 0 ? (float)(1.0 / h.masses[i]) : 0.f);
   }
-  CUDA_OK(cudaMemcpy(posq.p + h.atom_start, p.data(), sizeof(float4) * h.n, cudaMemcpyHostToDevice));
-  CUDA_OK(cudaMemcpy(vel.p + h.atom_start, v.data(), sizeof(float4) * h.n, cudaMemcpyHostToDevice));
-  long long sb = step;
-  CUDA_OK(cudaMemcpy(step_base.p + s, &sb, sizeof sb, cudaMemcpyHostToDevice));
-  DevInteg di;
-  CUDA_OK(cudaMemcpy(&di, integ.p + s, sizeof di, cudaMemcpyDeviceToHost));
-  di.tolerance = (float)h.tolerance;
-  di.supplied_noise = supplied;
-  CUDA_OK(cudaMemcpy(integ.p + s, &di, sizeof di, cudaMemcpyHostToDevice));
-  CUDA_OK(cudaMemset(diag.p + 4 * s, 0, sizeof(int) * 4));
+  long long *sb = reinterpret_cast<long long *>(v + h.n);
+  float *tol = reinterpret_cast<float *>(sb + 1);
+  int *sup = reinterpret_cast<int *>(tol + 1);
+  *sb = step;
+  *tol = (float)h.tolerance;
+  *sup = supplied;
+  CUDA_OK(cudaMemcpyAsync(posq.p + h.atom_start, p, sizeof(float4) * h.n, cudaMemcpyHostToDevice, stream));
+  CUDA_OK(cudaMemcpyAsync(vel.p + h.atom_start, v, sizeof(float4) * h.n, cudaMemcpyHostToDevice, stream));
+  CUDA_OK(cudaMemcpyAsync(step_base.p + s, sb, sizeof(long long), cudaMemcpyHostToDevice, stream));
+  // the integrator's tolerance and noise source of this system (two fields of its DevInteg)
+  char *di = reinterpret_cast<char *>(integ.p + s);
+  CUDA_OK(cudaMemcpyAsync(di + offsetof(DevInteg, tolerance), tol, sizeof(float), cudaMemcpyHostToDevice, stream));
+  CUDA_OK(cudaMemcpyAsync(di + offsetof(DevInteg, supplied_noise), sup, sizeof(int), cudaMemcpyHostToDevice, stream));
+  CUDA_OK(cudaMemsetAsync(diag.p + 4 * s, 0, sizeof(int) * 4, stream));
+  sync();
   h.step = step;
   h.steps_since_rebuild = 1LL << 40;
   h.kinetic_sampled_in_step = false;
@@ -2439,41 +2462,41 @@ rmd_status rmd_read_state_at(rmd_sim *sim, int32_t s, float *positions, float *v
   return guarded(sim, [&]() {
     auto &e = sim->engine;
     const auto &h = e.hs[s];
+    // every requested array in one round of asynchronous copies into page-locked staging
     e.sync();
-    if (positions || velocities) {
-      std::vector<float4> buf(h.n);
+    const size_t n = (size_t)h.n;
+    char *stage = e.staging(sizeof(float4) * 2 * n + sizeof(long long) * 3 * n + sizeof(rmd::DevSysD));
+    float4 *p = reinterpret_cast<float4 *>(stage), *v = p + n;
+    long long *f = reinterpret_cast<long long *>(v + n);
+    rmd::DevSysD *d = reinterpret_cast<rmd::DevSysD *>(f + 3 * n);
+    if (positions)
+      CUDA_OK(cudaMemcpyAsync(p, e.posq.p + h.atom_start, sizeof(float4) * n, cudaMemcpyDeviceToHost, e.stream));
+    if (velocities)
+      CUDA_OK(cudaMemcpyAsync(v, e.vel.p + h.atom_start, sizeof(float4) * n, cudaMemcpyDeviceToHost, e.stream));
+    if (forces)
+      for (int c = 0; c < 3; ++c)
+        CUDA_OK(cudaMemcpyAsync(f + c * n, e.force.p + (size_t)c * e.N + h.atom_start, sizeof(long long) * n,
+                                cudaMemcpyDeviceToHost, e.stream));
+    if (box_vectors || volume)
+      CUDA_OK(cudaMemcpyAsync(d, e.sysd.p + s, sizeof(rmd::DevSysD), cudaMemcpyDeviceToHost, e.stream));
+    e.sync();
+    for (size_t i = 0; i < n; ++i) {
       if (positions) {
-        CUDA_OK(cudaMemcpy(buf.data(), e.posq.p + h.atom_start, sizeof(float4) * h.n, cudaMemcpyDeviceToHost));
-        for (int i = 0; i < h.n; ++i) {
-          positions[3 * i] = buf[i].x;
-          positions[3 * i + 1] = buf[i].y;
-          positions[3 * i + 2] = buf[i].z;
-        }
+        positions[3 * i] = p[i].x;
+        positions[3 * i + 1] = p[i].y;
+        positions[3 * i + 2] = p[i].z;
       }
       if (velocities) {
-        CUDA_OK(cudaMemcpy(buf.data(), e.vel.p + h.atom_start, sizeof(float4) * h.n, cudaMemcpyDeviceToHost));
-        for (int i = 0; i < h.n; ++i) {
-          velocities[3 * i] = buf[i].x;
-          velocities[3 * i + 1] = buf[i].y;
-          velocities[3 * i + 2] = buf[i].z;
-        }
+        velocities[3 * i] = v[i].x;
+        velocities[3 * i + 1] = v[i].y;
+        velocities[3 * i + 2] = v[i].z;
       }
+      if (forces)
+        for (int c = 0; c < 3; ++c) forces[3 * i + c] = (float)((double)f[c * n + i] / rmd::FORCE_SCALE);
     }
-    if (forces) {
-      std::vector<long long> f(h.n);
-      for (int c = 0; c < 3; ++c) {
-        CUDA_OK(cudaMemcpy(f.data(), e.force.p + (size_t)c * e.N + h.atom_start, sizeof(long long) * h.n,
-                           cudaMemcpyDeviceToHost));
-        for (int i = 0; i < h.n; ++i) forces[3 * i + c] = (float)((double)f[i] / rmd::FORCE_SCALE);
-      }
-    }
-    if (box_vectors || volume) {
-      rmd::DevSysD d;
-      CUDA_OK(cudaMemcpy(&d, e.sysd.p + s, sizeof d, cudaMemcpyDeviceToHost));
-      if (box_vectors)
-        for (int k = 0; k < 9; ++k) box_vectors[k] = d.box[k];
-      if (volume) *volume = d.volume;
-    }
+    if (box_vectors)
+      for (int k = 0; k < 9; ++k) box_vectors[k] = d->box[k];
+    if (volume) *volume = d->volume;
   });
 }
 
